@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of the IM-SRG(2) commutator engine on B200.
+
+Workload (one step): the FP64 commutator C = [Omega, H] of two seeded random
+operators in the (M_L,M_S)-blocked layout of an N=20 electron, R=20 shell
+quantum dot (420 spin-orbitals, 61,947,679 stored entries = 495.6 MB per
+operator), with the particle-hole (Pandya) channel on: E0, one- and two-body
+parts through 110/220/111/121/221/122/222.  H is Hermitian, Omega
+anti-Hermitian, entries iid N(0, 0.1^2), then (anti)symmetrised.
+
+value: whole-job throughput in TFLOP/s, counting the FP64 work of the
+reference algorithm per commutator (qd_imsrg_b200.flops), inputs resident
+in HBM.  e2e: the same metric through the public API with host buffers
+(upload of both operators, commutator, download of the result) every step.
+
+--gpus N (under torchrun): N independent replicas, one per GPU, no data-path
+collective (weak scaling); the timed region is bracketed by barriers and the
+max over ranks is reported.
+
+--impl reference: the CPU restatement of the reference (oracle/, with
+OpenBLAS dgemm) on the host cores; each step is a bounded block sample of
+the same commutator (a stride-S block subset, rotating over steps).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s to converged E_gs (N=20,R=20, |dE|<=1e-6): chosen form vs FP64 GPU; TFLOP/s"
+NBODY, EMAX = 20, 20
+SEED_H, SEED_OMEGA = 1, 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nbody", type=int, default=NBODY)
+    ap.add_argument("--emax", type=int, default=EMAX)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--ref-stride", type=int, default=8)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------
+# nvidia-smi clock sampler (started before, stopped after the timed region)
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = str(local_rank)
+        if vis:
+            parts = [p.strip() for p in vis.split(",") if p.strip()]
+            if local_rank < len(parts) and parts[local_rank].isdigit():
+                idx = parts[local_rank]
+        self.idx = idx
+        self.proc = None
+        self.path = os.path.join("/tmp", "qd_clocks_%d_%d.csv" % (os.getpid(), local_rank))
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.idx, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------------------
+def measured_dgemm_tflops(torch, device) -> float:
+    """cuBLAS DGEMM throughput (8192^3, best of 3) as the FP64 tensor-pipe peak."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(device)
+    best = 1e30
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_peak: float) -> dict:
+    """Roofline of the stage with the largest device time."""
+    name, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    per_launch_s = (ms / max(cnt, 1)) / 1e3
+    if name == "ladder_gemm":
+        return {"kernel": "k_grouped_gemm (ladders of commutator_222)", "bound": "tensor",
+                "achieved": flops["ladder"] / per_launch_s / 1e12, "peak": dgemm_peak, "unit": "TFLOP/s",
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; tcgen05 has no f64 kind)",
+                "algorithmic_per_launch": flops["ladder"]}
+    if name == "pandya_gemm":
+        # one r x r x nb product per cross-coupled block (the reference does two)
+        return {"kernel": "k_grouped_gemm (Pandya products)", "bound": "tensor",
+                "achieved": flops["pandya"] / 2 / per_launch_s / 1e12, "peak": dgemm_peak, "unit": "TFLOP/s",
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                "algorithmic_per_launch": flops["pandya"] / 2}
+    if name == "c122":
+        byts = 3.0 * 8 * neq2b  # read A, B two-body, write C two-body
+        return {"kernel": "k_122 (commutator_122)", "bound": "hbm", "achieved": byts / per_launch_s / 1e9,
+                "peak": hbm_peak, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                "algorithmic_per_launch": byts}
+    byts = 3.0 * 8 * neq2b
+    return {"kernel": name, "bound": "hbm", "achieved": byts / per_launch_s / 1e9, "peak": hbm_peak,
+            "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs", "algorithmic_per_launch": byts}
+
+
+def hbm_peak_gbs() -> float:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def cpu_baseline_full(a: np.ndarray, b: np.ndarray, flops_total: float) -> dict:
+    """The oracle on the host cores: one complete [Omega,H] (N=20,R=20, Pandya
+    channel on), phases of the block sampler run back to back."""
+    import oracle
+
+    O = oracle.Layout(NBODY, EMAX)
+    A, B, Cop = oracle.Op(O, -1, a), oracle.Op(O, 1, b), oracle.Op(O, 1)
+    S = oracle.Sampler(A)
+    stride = 4
+    t0 = time.perf_counter()
+    for ph in range(stride):
+        S.run(A, B, Cop, stride, ph)
+    dt = time.perf_counter() - t0
+    return {"value": flops_total / dt / 1e12, "unit": "TFLOP/s", "cores": oracle.get_threads(), "kind": "port",
+            "seconds": dt, "blas": os.path.basename(oracle.BLAS) if oracle.BLAS else "oracle loop dgemm",
+            "sample": "one complete [Omega,H] at N=20,R=20 with the Pandya channel, same inputs "
+                      "(oracle restatement, OpenMP over blocks, OpenBLAS dgemm)"}
+
+
+# --------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    """Reference arm: the CPU restatement on the host cores, block-sampled."""
+    if rank != 0:
+        return 0
+    import oracle
+    import qd_imsrg_b200 as qd
+    from qd_imsrg_b200.flops import commutator_flops
+
+    P = qd.Layout(args.nbody, args.emax, device=qd.HOST_ONLY)
+    a = qd.random_operator(P, -1, SEED_OMEGA)
+    b = qd.random_operator(P, 1, SEED_H)
+    fl = sample_flops(P, args.ref_stride)
+    O = oracle.Layout(args.nbody, args.emax)
+    A, B, Cop = oracle.Op(O, -1, a), oracle.Op(O, 1, b), oracle.Op(O, 1)
+    S = oracle.Sampler(A)
+    stride = args.ref_stride
+    # phase 0 fills the cross-coupled matrices; warm-up starts there
+    for w in range(args.warmup):
+        S.run(A, B, Cop, stride, w % stride)
+    done, t = 0.0, 0.0
+    for k in range(args.steps):
+        ph = (args.warmup + k) % stride
+        if ph != 0 and k == 0:
+            S.run(A, B, Cop, stride, 0)  # cross-coupled matrices for this run
+        t0 = time.perf_counter()
+        S.run(A, B, Cop, stride, ph)
+        t += time.perf_counter() - t0
+        done += fl[ph]
+    val = done / t / 1e12
+    total = commutator_flops(P)["total"]
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Philox operators)",
+            "config": {"workload": "FP64 [Omega,H] N=%d R=%d, Pandya on; reference arm: CPU restatement"
+                                   % (args.nbody, args.emax), "block_stride": stride,
+                       "flops_per_commutator": total},
+            "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": oracle.get_threads(), "kind": "port",
+                             "sample": "per step the two-body work of every %d-th (M_L,M_S) block and "
+                                       "cross-coupled block (phase rotating; phase 0 adds E0 and the "
+                                       "one-body parts), throughput = reference-algorithm FLOPs of the "
+                                       "sample / time" % stride},
+            "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def sample_flops(P, stride):
+    """Reference-algorithm FLOPs done by each phase of the block sampler."""
+    from qd_imsrg_b200.flops import commutator_flops_parts
+
+    parts = commutator_flops_parts(P)
+    out = []
+    for ph in range(stride):
+        f = parts["block"][ph::stride].sum() + parts["cc"][ph::stride].sum()
+        if ph == 0:
+            f += parts["onebody"]
+        out.append(float(f))
+    return out
+
+
+# --------------------------------------------------------------------------
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+
+    import qd_imsrg_b200 as qd
+    from qd_imsrg_b200.flops import commutator_flops
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    P = qd.Layout(args.nbody, args.emax, device=local)
+    stream = torch.cuda.Stream(device=device)
+    P.set_stream(stream.cuda_stream)
+    fl = commutator_flops(P)
+    neq = P.neq
+    n, mp = P.nbody, P.msp - P.nbody
+    neq2b = neq - (1 + n * n + mp * mp + mp * n)
+
+    a = qd.random_operator(P, -1, SEED_OMEGA)
+    b = qd.random_operator(P, 1, SEED_H)
+    A, B, C = qd.FullHam(P, -1, a), qd.FullHam(P, 1, b), qd.FullHam(P, 1)
+
+    for _ in range(args.warmup):
+        qd.commutator(A, B, C, pandya=True)
+    P.synchronize()
+    dgemm_peak = measured_dgemm_tflops(torch, device)
+
+    clocks = ClockSampler(local)
+    launches0 = P.launches()
+    P.profile(True)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        qd.commutator(A, B, C, pandya=True)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    barrier(world)
+    prof = P.profile_read()
+    P.profile(False)
+    launches = P.launches() - launches0
+    sec = e0.elapsed_time(e1) / 1e3
+    sec = max_over_ranks(sec, world, device)
+    value = world * args.steps * fl["total"] / sec / 1e12
+
+    # end to end through the public API with pinned host buffers
+    ha = torch.from_numpy(a).pin_memory().numpy()
+    hb = torch.from_numpy(b).pin_memory().numpy()
+    hc = torch.empty(neq, dtype=torch.float64).pin_memory().numpy()
+    import ctypes as _C
+
+    from qd_imsrg_b200 import _native
+
+    lib = _native.lib()
+    barrier(world)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        A.upload(ha)
+        B.upload(hb)
+        qd.commutator(A, B, C, pandya=True)
+        _native.check(lib.qd_op_download(C.h, hc.ctypes.data_as(_C.POINTER(_C.c_double)), neq))
+    e2e_sec = (time.perf_counter() - t0) / args.e2e_steps
+    e2e_sec = max_over_ranks(e2e_sec, world, device)
+    e2e = {"value": world * fl["total"] / e2e_sec / 1e12, "unit": "TFLOP/s",
+           "h2d_bytes_per_step": 2 * 8 * neq, "d2h_bytes_per_step": 8 * neq, "ms_per_step": 1e3 * e2e_sec}
+
+    roof = stage_roofline(prof, fl, neq2b, dgemm_peak, hbm_peak_gbs())
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["traffic"] = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.nbody == NBODY and args.emax == EMAX:
+        cpu = cpu_baseline_full(a, b, fl["total"])
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox operators)",
+            "config": {"workload": "FP64 commutator [Omega,H], N=%d R=%d (%d spin-orbitals), random "
+                                   "(anti)Hermitian operators, Pandya channel on" % (n, P.emax, P.msp),
+                       "n_electrons": n, "shells": P.emax, "neq_per_operator": neq,
+                       "flops_per_step": fl["total"], "flops_breakdown": fl,
+                       "l2": "inputs larger than L2 (two 495.6 MB operators read per step)",
+                       "parallelism": "replicas x%d" % world},
+            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+            "stages_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()},
+            "dgemm_peak_tflops": dgemm_peak,
+        }
+        print(json.dumps(line), flush=True)
+    # release device objects before the torch stream they run on goes away
+    for o in (A, B, C):
+        o.close()
+    P.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

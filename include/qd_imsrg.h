@@ -1,0 +1,194 @@
+/*
+ * qd_imsrg.h -- C ABI of the B200-native IM-SRG(2) commutator engine.
+ *
+ * Drop-in boundary for the commutator / BCH hot path of nparz/qd_IMSRG.
+ * Each entry point below names the reference subroutine it replaces
+ * (file:line inside the reference project).  The Fortran host keeps
+ * Hartree-Fock, TBME generation and EOM; it hands the normal-ordered
+ * Hamiltonian to this library in the reference's own flat "vectorize" order
+ * (src/ME_general.f90:1871-1989) and calls the commutator / BCH / Magnus
+ * routines on device-resident operators.  INTEGRATION.md shows the
+ * iso_c_binding interface module a Fortran caller would add.
+ *
+ * Conventions
+ *   - Every function returns an int status: QD_OK (0) or a QD_ERR_* code;
+ *     qd_last_error() gives a message for the calling thread.  (The
+ *     reference has no error returns; it STOPs.)
+ *   - Operators live in device memory owned by the library, one flat FP64
+ *     array per operator in vectorize order: E0, fhh(n,n), fpp(m-n,m-n),
+ *     fph(m-n,n), then per (M_L,M_S) block Vhhhh, Vpppp, Vpphh, Vphph,
+ *     Vppph, Vphhh, each column-major.  herm (+1 Hermitian, -1
+ *     anti-Hermitian) is a field of the operator, as full_ham%herm.
+ *   - All work of one layout runs in order on that layout's CUDA stream.
+ *     Calls on one layout are not reentrant.  Scalar results (energies,
+ *     norms) synchronise the stream before returning.
+ *   - Single-particle indices are in the reference's "states order"
+ *     (arrange_states, src/ME_general.f90:688-716); holes must be states
+ *     1..N (convertF, src/ME_general.f90:1517-1525).
+ */
+#ifndef QD_IMSRG_H
+#define QD_IMSRG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QD_OK 0
+#define QD_ERR_ARG 1        /* bad argument (null handle, size mismatch, ...) */
+#define QD_ERR_LAYOUT 2     /* layout cannot be built (holes not states 1..N) */
+#define QD_ERR_CUDA 3       /* a CUDA call failed                              */
+#define QD_ERR_OOM 4        /* device allocation failed                        */
+#define QD_ERR_NAN 5        /* non-finite value detected                       */
+#define QD_ERR_NOCONV 6     /* flow did not converge within the step limit     */
+#define QD_ERR_NODEVICE 7   /* no CUDA device / extension unusable             */
+#define QD_ERR_STATE 8      /* call order violated (e.g. no cross-coupled data) */
+
+typedef struct qd_layout qd_layout; /* basis + (M_L,M_S) block layout           */
+typedef struct qd_op qd_op;         /* one operator: type(full_ham) on device    */
+typedef struct qd_cc qd_cc;         /* one type(cc_mat): Pandya X(r,nb) matrices */
+
+const char* qd_last_error(void);
+const char* qd_version(void);
+
+/* ---- layout: arrange_states + reindex + build_cross_coupled --------------
+ * Replaces src/ME_general.f90:688-716 (arrange_states), :956-1116
+ * (reindex), :363-448 (build_cross_coupled) and :1755-1778
+ * (get_num_elements).  eig: m single-particle energies in states order
+ * (m = emax*(emax+1)), or NULL for oscillator energies 2n+|ml|+1; pairs are
+ * classed hole/particle by eig <= eF exactly as reindex does.
+ * device >= 0 selects a CUDA device, -1 keeps the current device, and
+ * QD_HOST_ONLY builds the host-side tables only (no CUDA calls; operators
+ * cannot be created on such a layout, but qd_layout_* queries and
+ * qd_random_operator work).  */
+#define QD_HOST_ONLY (-2)
+int qd_layout_create(int nbody, int emax, const double* eig, int device, qd_layout** out);
+int qd_layout_destroy(qd_layout* L);
+int qd_layout_info(const qd_layout* L, int* nbody, int* msp, int* nblock, int64_t* neq, int* ncc);
+/* per block q (0-based): nhh, nph, npp, ML, MS  (5 ints per block)          */
+int qd_layout_blocks(const qd_layout* L, int* dims5);
+/* per block: vectorize offsets of Vhhhh,Vpppp,Vpphh,Vphph,Vppph,Vphhh      */
+int qd_layout_offsets(const qd_layout* L, int64_t* off6);
+/* pair list of block q (0-based), kind 0=hh 1=ph 2=pp; 1-based states,
+ * (count x 2) row-major; returns the count in *count                        */
+int qd_layout_pairs(const qd_layout* L, int q, int kind, int* out, int* count);
+/* CUDA stream (cudaStream_t) used for this layout; NULL = library-owned    */
+int qd_layout_set_stream(qd_layout* L, void* stream);
+int qd_layout_synchronize(qd_layout* L);
+/* device bytes currently held by the layout's work arena                    */
+int qd_layout_workspace_bytes(const qd_layout* L, int64_t* bytes);
+/* Optional per-stage timing with CUDA events on the layout's stream (the
+ * reference only has omp_get_wtime around whole runs, magnus_IMSRG.f90:30,159).
+ * enable != 0 starts (and resets) it.  qd_layout_profile_read synchronises
+ * and returns accumulated milliseconds and launch counts per stage:
+ * 0 E0 (110+220), 1 commutator_111, 2 commutator_121, 3 commutator_221,
+ * 4 commutator_122, 5 calc_cc, 6 ladder GEMMs (matrix_mult222),
+ * 7 Pandya GEMMs (construct_cc_ints), 8 particle-hole gather, 9 BCH glue.  */
+#define QD_NSTAGE 10
+int qd_layout_profile(qd_layout* L, int enable);
+int qd_layout_profile_read(qd_layout* L, double* ms, int64_t* counts, int nstage);
+/* number of kernels this library has launched for the layout so far        */
+int qd_layout_launches(const qd_layout* L, int64_t* n);
+
+/* ---- operators: allocate_everything / vectorize / repackage ---------------
+ * Replaces src/IMSRG_tools.f90:465-537 (allocate_everything: zero-filled,
+ * herm = herm), src/ME_general.f90:1871-1989 (vectorize) and :1992-2109
+ * (repackage).                                                               */
+int qd_op_create(qd_layout* L, int herm, qd_op** out);
+int qd_op_destroy(qd_op* op);
+int qd_op_upload(qd_op* op, const double* host_vec, int64_t neq);
+int qd_op_download(const qd_op* op, double* host_vec, int64_t neq);
+/* device <-> device in vectorize order (pointers into device memory)        */
+int qd_op_upload_device(qd_op* op, const double* dev_vec, int64_t neq);
+int qd_op_set_herm(qd_op* op, int herm);
+int qd_op_get_herm(const qd_op* op, int* herm);
+/* raw device pointer of the operator's array (for interop, e.g. torch)     */
+int qd_op_device_ptr(qd_op* op, double** dptr);
+/* Seeded random operator in vectorize order, written to a host buffer:
+ * entries iid N(0, sigma^2) (Philox-4x32-10 counter RNG, Box-Muller),
+ * diagonal-class blocks (fhh,fpp,Vhhhh,Vpppp,Vphph) made (X + herm X^T)/2,
+ * E0 = 0; conserve != 0 zeroes one-body entries that change (ml,ms).
+ * No counterpart in the reference (synthetic input generator).              */
+int qd_random_operator(const qd_layout* L, int herm, uint64_t seed, double sigma, int conserve,
+                       double* host_vec, int64_t neq);
+
+/* ---- algebra (src/ME_general.f90:592-686, :2112-2138) ---------------------- */
+int qd_add_arrays(const qd_op* r1, double s1, const qd_op* r2, double s2, qd_op* r3); /* r3=s1*r1+s2*r2 */
+int qd_copy_arrays(const qd_op* r1, qd_op* r2);                                        /* r2 = r1      */
+int qd_set_to_zero(qd_op* r1);
+/* mat_2_norm: as the reference, the one-body parts only (its block loop is
+ * empty): sqrt(sum fph^2 + sum fpp^2 + sum fhh^2)                            */
+int qd_mat_2_norm(const qd_op* r, double* out);
+
+/* ---- commutators (src/commutators.f90) ------------------------------------- */
+int qd_commutator_110(const qd_op* r1, const qd_op* r2, double* c);  /* :12-33   */
+int qd_commutator_220(const qd_op* r1, const qd_op* r2, double* c);  /* :36-70   */
+int qd_commutator_111(const qd_op* r1, const qd_op* r2, qd_op* r3);  /* :137-195, overwrites 1-body */
+int qd_commutator_121(const qd_op* r1, const qd_op* r2, qd_op* r3);  /* :73-134, accumulates 1-body */
+int qd_commutator_221(const qd_op* r1, const qd_op* r2, qd_op* r3, qd_op* w1, qd_op* w2); /* :198-352 */
+int qd_commutator_122(const qd_op* r1, const qd_op* r2, qd_op* r3);  /* :355-676, overwrites 2-body */
+/* :679-985 with matrix_mult222 :987-1132 and construct_cc_ints
+ * (src/ME_general.f90:923-952); accumulates 2-body.  HCC belongs to r2,
+ * ETACC to r1.  A qd_cc that calc_cc never filled holds X = 0, so its
+ * particle-hole terms vanish (as in run_magnus).  w1 is accepted for
+ * interface parity and is not used.                                          */
+int qd_commutator_222(const qd_op* r1, const qd_op* r2, qd_op* r3, qd_op* w1, const qd_cc* HCC,
+                      const qd_cc* ETACC);
+
+/* Whole [A,B] -> C in the reference's order (E0 = 110+220; 111; 121; 221;
+ * 122; 222).  flags: QD_PANDYA = fill both operators' cross-coupled
+ * matrices first (as dGam, src/gs_IMSRG.f90:243-250); without it the
+ * particle-hole channel is skipped (X = 0, as run_magnus).                  */
+#define QD_PANDYA 1u
+int qd_commutator(const qd_op* A, const qd_op* B, qd_op* C, unsigned flags);
+
+/* ---- cross-coupled (Pandya) matrices ----------------------------------------
+ * calc_cc src/commutators.f90:1135-1159, copy_cc src/IMSRG_tools.f90:437-461 */
+int qd_cc_create(qd_layout* L, double herm, qd_cc** out);  /* X = 0 */
+int qd_cc_destroy(qd_cc* cc);
+int qd_cc_set_herm(qd_cc* cc, double herm);
+int qd_calc_cc(const qd_op* H, qd_cc* HCC);
+int qd_cc_download(const qd_cc* cc, double* host, int64_t n, int64_t* needed);
+
+/* ---- generator, energies ---------------------------------------------------- */
+int qd_build_white(qd_op* gen, const qd_op* H);  /* src/IMSRG_tools.f90:377-434 */
+int qd_mbpt2(const qd_op* H, double* out);        /* src/HFQDmod.f90:325-362   */
+/* HF_E2, src/HFQDmod.f90:292-323: E0 = sum_{i<=N} eig(i) - sum Vhhhh(j,j);
+ * sets H's E0 as the reference does (eig as given to qd_layout_create)       */
+int qd_hf_e2(qd_op* H, double* out);
+
+/* ---- BCH / Magnus (src/magnus_IMSRG.f90) ----------------------------------- */
+/* BCH_EXPAND :253-318: HS = sum_k ad_G^k(H) cof(k) with the reference's
+ * truncated cof table and exit test |INT2|*cof/|INT1| < 1e-5 (one-body norm).
+ * INT1, INT2, AD, w1, w2 are caller workspaces (contents unspecified on
+ * return); HCC/OCC as in the reference (never filled -> no ph channel) unless
+ * flags has QD_PANDYA, which refills them from AD and G before each 222.
+ * *nterms receives the number of commutators evaluated.                      */
+int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op* INT2, qd_op* AD,
+                  qd_op* w1, qd_op* w2, qd_cc* HCC, qd_cc* OCC, unsigned flags, int* nterms);
+/* MAGNUS_EXPAND :321-369: the reference returns after DG = ETA.              */
+int qd_magnus_expand(qd_op* DG, const qd_op* G, const qd_op* ETA);
+/* euler_step :372-384: G = G + stp*DG; s = s + stp                          */
+int qd_euler_step(qd_op* G, const qd_op* DG, double* s, double stp);
+
+/* s_evolve with build_white, :194-248 (TDA diagnostics omitted).  HAM is the
+ * normal-ordered HF Hamiltonian, HS receives the evolved Hamiltonian.
+ * trace (may be NULL): up to max_iter rows of 7 doubles per flow iteration:
+ * iteration, s, E0, nrm1, nrm2, crit, BCH terms (negated for a rejected
+ * step).  *rows = rows written.  Returns QD_ERR_NOCONV past max_iter.      */
+typedef struct qd_flow_result {
+  double E0;        /* HS%E0 at convergence                  */
+  double s;         /* final flow parameter                  */
+  int iterations;   /* accepted steps                        */
+  int rejected;     /* rejected steps                        */
+  int commutators;  /* total BCH commutators evaluated       */
+  int rows;         /* trace rows written                    */
+} qd_flow_result;
+int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, double* trace,
+                   qd_flow_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QD_IMSRG_H */

@@ -1,0 +1,305 @@
+"""qd_imsrg_b200 -- B200-native IM-SRG(2) commutator / BCH engine.
+
+Python front end of the C ABI (include/qd_imsrg.h).  Names and argument
+meanings follow the reference Fortran subroutines so that host code reads
+like the reference:
+
+  reference (nparz/qd_IMSRG)                      here
+  type(full_ham)  ME_general.f90:43-62            FullHam (device operator)
+  type(cc_mat)    ME_general.f90:19-24            CCMat
+  reindex / build_cross_coupled                   Layout
+  commutator_110/220/111/121/221/122/222          commutator_110 ... commutator_222
+  calc_cc, build_white, add_arrays, copy_arrays,  same names
+  set_to_zero, mat_2_norm, MBPT2, HF_E2
+  BCH_EXPAND, MAGNUS_EXPAND, euler_step,          bch_expand, magnus_expand,
+  s_evolve                                        euler_step, magnus_flow
+
+Operators stay resident in device memory in the reference's (M_L,M_S)-blocked
+layout; host arrays are exchanged in the reference's vectorize order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native
+from ._native import QD_PANDYA, FlowResult, QDError, check, lib
+
+__all__ = [
+    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA",
+    "commutator_110", "commutator_220", "commutator_111", "commutator_121", "commutator_221",
+    "commutator_122", "commutator_222", "commutator", "calc_cc", "build_white", "add_arrays",
+    "copy_arrays", "set_to_zero", "mat_2_norm", "mbpt2", "hf_e2", "bch_expand", "magnus_expand",
+    "euler_step", "magnus_flow", "random_operator",
+]
+
+_dp = C.POINTER(C.c_double)
+HOST_ONLY = -2
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Layout:
+    """Basis of N holes in emax major shells, blocked as reindex does.
+
+    eig: optional single-particle energies in states order (default:
+    oscillator energies 2n+|ml|+1), used to class pairs as hole/particle.
+    device: CUDA device (-1 = current); HOST_ONLY builds only the host tables.
+    """
+
+    def __init__(self, nbody: int, emax: int, eig=None, device: int = -1):
+        self.h = C.c_void_p()
+        e = None
+        if eig is not None:
+            self._eig = np.ascontiguousarray(eig, dtype=np.float64)
+            e = _d(self._eig)
+        check(lib().qd_layout_create(int(nbody), int(emax), e, int(device), C.byref(self.h)))
+        nb, msp, nblk, ncc = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        neq = C.c_int64()
+        check(lib().qd_layout_info(self.h, C.byref(nb), C.byref(msp), C.byref(nblk), C.byref(neq), C.byref(ncc)))
+        self.nbody, self.msp, self.nblock, self.neq, self.ncc = nb.value, msp.value, nblk.value, neq.value, ncc.value
+        self.emax = int(emax)
+        dims = np.zeros((self.nblock, 5), np.int32)
+        check(lib().qd_layout_blocks(self.h, dims.ctypes.data_as(C.POINTER(C.c_int))))
+        self.dims = dims
+        offs = np.zeros((self.nblock, 6), np.int64)
+        check(lib().qd_layout_offsets(self.h, offs.ctypes.data_as(C.POINTER(C.c_int64))))
+        self.offs = offs
+
+    def pairs(self, q: int, kind: int) -> np.ndarray:
+        """1-based (i,j) pairs of block q (0-based); kind 0=hh, 1=ph, 2=pp."""
+        cnt = C.c_int()
+        check(lib().qd_layout_pairs(self.h, int(q), int(kind), None, C.byref(cnt)))
+        out = np.zeros((max(cnt.value, 1), 2), np.int32)
+        check(lib().qd_layout_pairs(self.h, int(q), int(kind), out.ctypes.data_as(C.POINTER(C.c_int)),
+                                    C.byref(cnt)))
+        return out[: cnt.value]
+
+    def synchronize(self) -> None:
+        check(lib().qd_layout_synchronize(self.h))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib().qd_layout_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def profile(self, enable: bool = True) -> None:
+        """Start (and reset) or stop per-stage CUDA-event timing."""
+        check(lib().qd_layout_profile(self.h, int(enable)))
+
+    def profile_read(self) -> dict:
+        """{stage: (milliseconds, launches)} accumulated since profile(True)."""
+        ms = np.zeros(_native.QD_NSTAGE, np.float64)
+        cnt = np.zeros(_native.QD_NSTAGE, np.int64)
+        check(lib().qd_layout_profile_read(self.h, _d(ms), cnt.ctypes.data_as(C.POINTER(C.c_int64)),
+                                           _native.QD_NSTAGE))
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(_native.STAGES)}
+
+    def launches(self) -> int:
+        """Kernels launched by the library for this layout so far."""
+        n = C.c_int64()
+        check(lib().qd_layout_launches(self.h, C.byref(n)))
+        return n.value
+
+    def workspace_bytes(self) -> int:
+        b = C.c_int64()
+        check(lib().qd_layout_workspace_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None) and self.h.value:
+            lib().qd_layout_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def random_operator(layout: Layout, herm: int, seed: int, sigma: float = 0.1, conserve: bool = True) -> np.ndarray:
+    """Seeded synthetic operator (host vector, vectorize order)."""
+    v = np.empty(layout.neq, np.float64)
+    check(lib().qd_random_operator(layout.h, int(herm), C.c_uint64(seed), float(sigma), int(conserve), _d(v),
+                                   layout.neq))
+    return v
+
+
+class FullHam:
+    """A device-resident operator (type(full_ham)); herm = +1 or -1."""
+
+    def __init__(self, layout: Layout, herm: int = 1, vec=None):
+        self.layout = layout
+        self.h = C.c_void_p()
+        check(lib().qd_op_create(layout.h, int(herm), C.byref(self.h)))
+        if vec is not None:
+            self.upload(vec)
+
+    def upload(self, vec) -> None:
+        v = np.ascontiguousarray(vec, dtype=np.float64)
+        check(lib().qd_op_upload(self.h, _d(v), v.size))
+
+    def download(self) -> np.ndarray:
+        v = np.empty(self.layout.neq, np.float64)
+        check(lib().qd_op_download(self.h, _d(v), v.size))
+        return v
+
+    @property
+    def herm(self) -> int:
+        h = C.c_int()
+        check(lib().qd_op_get_herm(self.h, C.byref(h)))
+        return h.value
+
+    @herm.setter
+    def herm(self, h: int) -> None:
+        check(lib().qd_op_set_herm(self.h, int(h)))
+
+    def device_ptr(self) -> int:
+        p = _dp()
+        check(lib().qd_op_device_ptr(self.h, C.byref(p)))
+        return C.cast(p, C.c_void_p).value
+
+    @property
+    def E0(self) -> float:
+        return float(self.download()[0])
+
+    def close(self) -> None:
+        if getattr(self, "h", None) and self.h.value:
+            lib().qd_op_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CCMat:
+    """Cross-coupled (Pandya) X(r,nb) matrices of one operator (type(cc_mat))."""
+
+    def __init__(self, layout: Layout, herm: float = 1.0):
+        self.layout = layout
+        self.h = C.c_void_p()
+        check(lib().qd_cc_create(layout.h, float(herm), C.byref(self.h)))
+
+    def set_herm(self, h: float) -> None:
+        check(lib().qd_cc_set_herm(self.h, float(h)))
+
+    def download(self) -> np.ndarray:
+        need = C.c_int64()
+        check(lib().qd_cc_download(self.h, None, 0, C.byref(need)))
+        out = np.empty(need.value, np.float64)
+        check(lib().qd_cc_download(self.h, _d(out), need.value, C.byref(need)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None) and self.h.value:
+            lib().qd_cc_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _scalar(fn, *args) -> float:
+    out = C.c_double()
+    check(fn(*args, C.byref(out)))
+    return out.value
+
+
+def commutator_110(r1: FullHam, r2: FullHam) -> float:
+    return _scalar(lib().qd_commutator_110, r1.h, r2.h)
+
+
+def commutator_220(r1: FullHam, r2: FullHam) -> float:
+    return _scalar(lib().qd_commutator_220, r1.h, r2.h)
+
+
+def commutator_111(r1, r2, r3) -> None:
+    check(lib().qd_commutator_111(r1.h, r2.h, r3.h))
+
+
+def commutator_121(r1, r2, r3) -> None:
+    check(lib().qd_commutator_121(r1.h, r2.h, r3.h))
+
+
+def commutator_221(r1, r2, r3, w1, w2) -> None:
+    check(lib().qd_commutator_221(r1.h, r2.h, r3.h, w1.h, w2.h))
+
+
+def commutator_122(r1, r2, r3) -> None:
+    check(lib().qd_commutator_122(r1.h, r2.h, r3.h))
+
+
+def commutator_222(r1, r2, r3, w1, HCC: CCMat, ETACC: CCMat) -> None:
+    check(lib().qd_commutator_222(r1.h, r2.h, r3.h, w1.h if w1 is not None else None, HCC.h, ETACC.h))
+
+
+def commutator(A: FullHam, B: FullHam, Cop: FullHam, pandya: bool = True) -> None:
+    """C = [A,B] in the reference's call order; pandya fills both operators'
+    cross-coupled matrices first (as dGam), otherwise the particle-hole
+    channel is absent (as run_magnus)."""
+    check(lib().qd_commutator(A.h, B.h, Cop.h, QD_PANDYA if pandya else 0))
+
+
+def calc_cc(H: FullHam, HCC: CCMat) -> None:
+    check(lib().qd_calc_cc(H.h, HCC.h))
+
+
+def build_white(gen: FullHam, H: FullHam) -> None:
+    check(lib().qd_build_white(gen.h, H.h))
+
+
+def add_arrays(r1, s1, r2, s2, r3) -> None:
+    check(lib().qd_add_arrays(r1.h, float(s1), r2.h, float(s2), r3.h))
+
+
+def copy_arrays(r1, r2) -> None:
+    check(lib().qd_copy_arrays(r1.h, r2.h))
+
+
+def set_to_zero(r1) -> None:
+    check(lib().qd_set_to_zero(r1.h))
+
+
+def mat_2_norm(r) -> float:
+    return _scalar(lib().qd_mat_2_norm, r.h)
+
+
+def mbpt2(r) -> float:
+    return _scalar(lib().qd_mbpt2, r.h)
+
+
+def hf_e2(r) -> float:
+    return _scalar(lib().qd_hf_e2, r.h)
+
+
+def bch_expand(HS, G, H, INT1, INT2, AD, w1, w2, HCC: CCMat, OCC: CCMat, pandya: bool = False) -> int:
+    n = C.c_int()
+    check(lib().qd_bch_expand(HS.h, G.h, H.h, INT1.h, INT2.h, AD.h, w1.h, w2.h, HCC.h, OCC.h,
+                              QD_PANDYA if pandya else 0, C.byref(n)))
+    return n.value
+
+
+def magnus_expand(DG, G, ETA) -> None:
+    check(lib().qd_magnus_expand(DG.h, G.h, ETA.h))
+
+
+def euler_step(G, DG, s: float, stp: float) -> float:
+    sv = C.c_double(s)
+    check(lib().qd_euler_step(G.h, DG.h, C.byref(sv), float(stp)))
+    return sv.value
+
+
+def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int = 500):
+    """s_evolve(build_white): returns (trace[rows,7], FlowResult)."""
+    trace = np.zeros((max_iter, 7), np.float64)
+    res = FlowResult()
+    check(lib().qd_magnus_flow(HAM.h, HS.h, QD_PANDYA if pandya else 0, int(max_iter), _d(trace), C.byref(res)))
+    return trace[: res.rows], res

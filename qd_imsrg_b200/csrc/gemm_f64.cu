@@ -1,0 +1,564 @@
+// gemm_f64.cu -- grouped FP64 block GEMM on the DMMA tensor pipe.
+//
+// All dense contractions of one commutator stage (the ladders of
+// matrix_mult222, the intermediates of commutator_221, the one-body products
+// of commutator_111 and the Pandya products of construct_cc_ints) run as ONE
+// launch over a task list that covers every (M_L,M_S) block of uneven size.
+//
+// Problem = one output sub-block C (M x N, column-major, ldc) and a list of
+// K-segments  acc += alpha_s * op(A_s) op(B_s); the segments are concatenated
+// along K so every output tile is accumulated in registers and written once.
+// Epilogue modes:
+//   ACC       C += V
+//   SET       C  = V
+//   ACC_PAIR  C += V + sigma V^T      (M == N; the CTA computes the tile pair
+//   SET_PAIR  C  = V + sigma V^T       (I,J),(J,I) so V^T is at hand)
+// The pair modes carry the "hA*W^T - hB*W" transpose-adds of the reference
+// (src/commutators.f90:1002-1127, :154-169) without a second GEMM.
+//
+// Tile 64x64x16, 4 warps (2x2), each warp 32x32 = 4x4 DMMA m8n8k4 fragments;
+// 3-stage cp.async (8-byte, zero-fill) pipeline; FP64 accumulate.
+// tcgen05 has no f64 kind, so mma.sync DMMA is the FP64 tensor path here.
+#include <algorithm>
+#include <cstring>
+
+#include "dev_common.cuh"
+
+namespace qd {
+
+constexpr int BM = 64, BN = 64, BK = 16, LDS = 68, NSTAGE = 3, TLD = 65;
+constexpr int GEMM_THREADS = 128;
+constexpr int SMEM_PIPE = 2 * NSTAGE * BK * LDS;  // doubles
+constexpr int SMEM_TILE = BN * TLD;               // doubles
+constexpr size_t GEMM_SMEM = sizeof(double) * (SMEM_PIPE + SMEM_TILE);
+constexpr int NBUF = 7;
+
+struct Bufs {
+  const double* p[NBUF];
+};
+
+__device__ __forceinline__ void cp_async8(double* s, const double* g, bool pred) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(sz));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ bool seg_active(const GSeg& s, unsigned mA, unsigned mB) {
+  auto dead = [&](int src, int dep) {
+    if (dep < 0) return false;
+    unsigned m = src == 0 ? mA : (src == 1 ? mB : 0u);
+    return ((m >> dep) & 1u) != 0;
+  };
+  return !dead(s.srcA, s.depA) && !dead(s.srcB, s.depB);
+}
+
+// Load the (row0, col0) tile's k-slab [k0, k0+BK) of segment s into stage buffers.
+__device__ __forceinline__ void load_stage(const GSeg& s, const Bufs& bufs, int M, int N, int row0, int col0,
+                                           int k0, double* sA, double* sB) {
+  const int tid = threadIdx.x;
+  const double* A = bufs.p[s.srcA] + s.offA;
+  const double* B = bufs.p[s.srcB] + s.offB;
+#pragma unroll
+  for (int it = 0; it < (BM * BK) / GEMM_THREADS; ++it) {
+    int idx = tid + it * GEMM_THREADS;
+    int mm, kk;
+    if (!s.tA) {
+      mm = idx & (BM - 1);
+      kk = idx >> 6;
+    } else {
+      kk = idx & (BK - 1);
+      mm = idx >> 4;
+    }
+    int gm = row0 + mm, gk = k0 + kk;
+    bool ok = gm < M && gk < s.K;
+    const double* src = ok ? (s.tA ? A + gk + (i64)gm * s.lda : A + gm + (i64)gk * s.lda) : A;
+    cp_async8(sA + kk * LDS + mm, src, ok);
+  }
+#pragma unroll
+  for (int it = 0; it < (BN * BK) / GEMM_THREADS; ++it) {
+    int idx = tid + it * GEMM_THREADS;
+    int nn, kk;
+    if (!s.tB) {
+      kk = idx & (BK - 1);
+      nn = idx >> 4;
+    } else {
+      nn = idx & (BN - 1);
+      kk = idx >> 6;
+    }
+    int gn = col0 + nn, gk = k0 + kk;
+    bool ok = gn < N && gk < s.K;
+    const double* src = ok ? (s.tB ? B + gn + (i64)gk * s.ldb : B + gk + (i64)gn * s.ldb) : B;
+    cp_async8(sB + kk * LDS + nn, src, ok);
+  }
+}
+
+struct SegCursor {
+  int seg[8];
+  int ktiles[8];
+  int nact;
+  int total;
+};
+
+// Accumulate the tile (row0, col0) of problem P into acc[4][4][2].
+__device__ void tile_mainloop(const GProb& P, const GSeg* __restrict__ segs, const SegCursor& cur, const Bufs& bufs,
+                              double hv0, double hv1, int row0, int col0, double* smem, double acc[4][4][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  if (cur.total == 0) return;
+  double* sA = smem;
+  double* sB = smem + NSTAGE * BK * LDS;
+
+  // stage g -> (segment, k0)
+  auto locate = [&](int g, int& si, int& k0) {
+    int a = 0;
+    for (;;) {
+      if (g < cur.ktiles[a]) break;
+      g -= cur.ktiles[a];
+      ++a;
+    }
+    si = cur.seg[a];
+    k0 = g * BK;
+  };
+  // prologue
+#pragma unroll
+  for (int st = 0; st < NSTAGE - 1; ++st) {
+    if (st < cur.total) {
+      int si, k0;
+      locate(st, si, k0);
+      GSeg s = segs[si];
+      load_stage(s, bufs, P.M, P.N, row0, col0, k0, sA + st * BK * LDS, sB + st * BK * LDS);
+    }
+    cp_commit();
+  }
+  for (int g = 0; g < cur.total; ++g) {
+    int gl = g + NSTAGE - 1;
+    if (gl < cur.total) {
+      int si, k0;
+      locate(gl, si, k0);
+      GSeg s = segs[si];
+      int b = gl % NSTAGE;
+      load_stage(s, bufs, P.M, P.N, row0, col0, k0, sA + b * BK * LDS, sB + b * BK * LDS);
+    }
+    cp_commit();
+    cp_wait<NSTAGE - 1>();
+    __syncthreads();
+    int si, k0;
+    locate(g, si, k0);
+    const GSeg& s = segs[si];
+    double alpha = s.c * (s.pa ? hv0 : 1.0) * (s.pb ? hv1 : 1.0);
+    const double* a_s = sA + (g % NSTAGE) * BK * LDS;
+    const double* b_s = sB + (g % NSTAGE) * BK * LDS;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double af[4], bf[4];
+      const int kr = kk + (lane & 3);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) af[i] = alpha * a_s[kr * LDS + wm * 32 + i * 8 + (lane >> 2)];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bf[j] = b_s[kr * LDS + wn * 32 + j * 8 + (lane >> 2)];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+    __syncthreads();
+  }
+  cp_wait<0>();
+  __syncthreads();
+}
+
+// accumulator fragments -> smem tile T[col*TLD + row]
+__device__ __forceinline__ void stash(double* T, const double acc[4][4][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int r = wm * 32 + i * 8 + (lane >> 2);
+      int c = wn * 32 + j * 8 + 2 * (lane & 3);
+      T[c * TLD + r] = acc[i][j][0];
+      T[(c + 1) * TLD + r] = acc[i][j][1];
+    }
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __restrict__ tasks,
+                                                               const GProb* __restrict__ probs,
+                                                               const GSeg* __restrict__ segs, Bufs bufs, double hv0,
+                                                               double hv1, unsigned maskA, unsigned maskB) {
+  extern __shared__ double smem[];
+  const GTask t = tasks[blockIdx.x];
+  const GProb P = probs[t.prob];
+  double* out = const_cast<double*>(bufs.p[P.outbuf]) + P.offC;
+
+  SegCursor cur;
+  cur.nact = 0;
+  cur.total = 0;
+  for (int k = 0; k < P.nseg && cur.nact < 8; ++k) {
+    const GSeg& s = segs[P.seg0 + k];
+    if (!seg_active(s, maskA, maskB) || s.K <= 0) continue;
+    cur.seg[cur.nact] = P.seg0 + k;
+    cur.ktiles[cur.nact] = (s.K + BK - 1) / BK;
+    cur.total += cur.ktiles[cur.nact];
+    ++cur.nact;
+  }
+  const bool pair = P.mode == GM_ACC_PAIR || P.mode == GM_SET_PAIR;
+  const bool acc_mode = P.mode == GM_ACC || P.mode == GM_ACC_PAIR;
+  double* T1 = smem + SMEM_PIPE;  // first tile stash (pair mode)
+  double* T2 = smem;              // aliases the pipeline buffers after the main loop
+  double acc[4][4][2];
+
+  const int r0 = t.ti * BM, c0 = t.tj * BN;
+  tile_mainloop(P, segs, cur, bufs, hv0, hv1, r0, c0, smem, acc);
+
+  if (!pair) {
+    stash(T2, acc);
+    __syncthreads();
+    const int mr = min(BM, P.M - r0), nc = min(BN, P.N - c0);
+    for (int idx = threadIdx.x; idx < BM * BN; idx += GEMM_THREADS) {
+      int r = idx & (BM - 1), c = idx >> 6;
+      if (r < mr && c < nc) {
+        double* p = out + (r0 + r) + (i64)(c0 + c) * P.ldc;
+        double v = T2[c * TLD + r];
+        *p = acc_mode ? *p + v : v;
+      }
+    }
+    return;
+  }
+  const double sigma = P.sc * (P.spa ? hv0 : 1.0) * (P.spb ? hv1 : 1.0);
+  if (t.ti == t.tj) {
+    stash(T1, acc);
+    __syncthreads();
+    const int mr = min(BM, P.M - r0);
+    for (int idx = threadIdx.x; idx < BM * BN; idx += GEMM_THREADS) {
+      int r = idx & (BM - 1), c = idx >> 6;
+      if (r < mr && c < mr) {
+        double* p = out + (r0 + r) + (i64)(r0 + c) * P.ldc;
+        double v = T1[c * TLD + r] + sigma * T1[r * TLD + c];
+        *p = acc_mode ? *p + v : v;
+      }
+    }
+    return;
+  }
+  // off-diagonal tile pair: V(I,J) -> T1, then V(J,I) -> T2
+  stash(T1, acc);
+  __syncthreads();
+  tile_mainloop(P, segs, cur, bufs, hv0, hv1, c0, r0, smem, acc);
+  stash(T2, acc);
+  __syncthreads();
+  const int mI = min(BM, P.M - r0), mJ = min(BM, P.M - c0);
+  // C(I,J) (rows r0.., cols c0..) = T1 + sigma * T2^T
+  for (int idx = threadIdx.x; idx < BM * BN; idx += GEMM_THREADS) {
+    int r = idx & (BM - 1), c = idx >> 6;
+    if (r < mI && c < mJ) {
+      double* p = out + (r0 + r) + (i64)(c0 + c) * P.ldc;
+      double v = T1[c * TLD + r] + sigma * T2[r * TLD + c];
+      *p = acc_mode ? *p + v : v;
+    }
+  }
+  // C(J,I) (rows c0.., cols r0..) = T2 + sigma * T1^T
+  for (int idx = threadIdx.x; idx < BM * BN; idx += GEMM_THREADS) {
+    int r = idx & (BM - 1), c = idx >> 6;
+    if (r < mJ && c < mI) {
+      double* p = out + (c0 + r) + (i64)(r0 + c) * P.ldc;
+      double v = T2[c * TLD + r] + sigma * T1[r * TLD + c];
+      *p = acc_mode ? *p + v : v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: program construction and launch
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Builder {
+  GemmProgram& P;
+  int cur = -1;
+  explicit Builder(GemmProgram& p) : P(p) {}
+  void prob(int M, int N, i64 offC, int ldc, int mode, int outbuf, double sc = 0.0, int spa = 0, int spb = 0) {
+    GProb g;
+    std::memset(&g, 0, sizeof(g));
+    g.M = M;
+    g.N = N;
+    g.ldc = ldc;
+    g.offC = offC;
+    g.mode = mode;
+    g.outbuf = outbuf;
+    g.seg0 = (int)P.segs.size();
+    g.nseg = 0;
+    g.sc = sc;
+    g.spa = (signed char)spa;
+    g.spb = (signed char)spb;
+    P.probs.push_back(g);
+    cur = (int)P.probs.size() - 1;
+  }
+  // acc += c * hv0^pa * hv1^pb * op(A) op(B)
+  void seg(int srcA, i64 offA, int lda, bool tA, int depA, int srcB, i64 offB, int ldb, bool tB, int depB, int K,
+           double c, int pa = 0, int pb = 0) {
+    if (K <= 0) return;
+    GSeg s;
+    std::memset(&s, 0, sizeof(s));
+    s.offA = offA;
+    s.offB = offB;
+    s.lda = std::max(1, lda);
+    s.ldb = std::max(1, ldb);
+    s.K = K;
+    s.srcA = (signed char)srcA;
+    s.srcB = (signed char)srcB;
+    s.tA = tA;
+    s.tB = tB;
+    s.depA = (signed char)depA;
+    s.depB = (signed char)depB;
+    s.pa = (signed char)pa;
+    s.pb = (signed char)pb;
+    s.c = c;
+    P.segs.push_back(s);
+    P.probs[cur].nseg++;
+  }
+  void drop_if_empty() {
+    if (cur >= 0 && P.probs[cur].nseg == 0) {
+      P.probs.pop_back();
+      cur = -1;
+    }
+  }
+};
+
+// operand buffer ids
+enum { BA = 0, BB = 1, BXA = 2, BXB = 3, BO0 = 4, BO1 = 5, BZ = 6 };
+const bool N_ = false, T_ = true;
+
+}  // namespace
+
+int build_programs(qd_layout* L) {
+  if (L->programs_built) return QD_OK;
+  const int n = L->n, mp = L->mp;
+  // ---- matrix_mult222 ladders (ACC into C) ----
+  {
+    GemmProgram& P = L->prog_ladder;
+    Builder b(P);
+    for (int q = 0; q < L->nblock; ++q) {
+      const int nh = L->blk[q].x, nb = L->blk[q].y, np = L->blk[q].z;
+      const i64* o = &L->boff[6 * q];
+      const i64 hhhh = o[0], pppp = o[1], pphh = o[2], phph = o[3], ppph = o[4], phhh = o[5];
+      if (nh > 0) {  // V = -hB Bpphh^T Apphh - Ahhhh Bhhhh ; C += V + s V^T
+        b.prob(nh, nh, hhhh, nh, GM_ACC_PAIR, BO0, -1.0, 1, 1);
+        if (np > 0) b.seg(BB, pphh, np, T_, P_PPHH, BA, pphh, np, N_, P_PPHH, np, -1.0, 0, 1);
+        b.seg(BA, hhhh, nh, N_, P_HHHH, BB, hhhh, nh, N_, P_HHHH, nh, -1.0);
+        b.drop_if_empty();
+      }
+      if (np > 0) {  // V = -hB Apphh Bpphh^T - Bpppp Apppp
+        b.prob(np, np, pppp, np, GM_ACC_PAIR, BO0, -1.0, 1, 1);
+        if (nh > 0) b.seg(BA, pphh, np, N_, P_PPHH, BB, pphh, np, T_, P_PPHH, nh, -1.0, 0, 1);
+        b.seg(BB, pppp, np, N_, P_PPPP, BA, pppp, np, N_, P_PPPP, np, -1.0);
+        b.drop_if_empty();
+      }
+      if (nb > 0) {  // V = -hB (Aphhh Bphhh^T + Bppph^T Appph)
+        b.prob(nb, nb, phph, nb, GM_ACC_PAIR, BO0, -1.0, 1, 1);
+        if (nh > 0) b.seg(BA, phhh, nb, N_, P_PHHH, BB, phhh, nb, T_, P_PHHH, nh, -1.0, 0, 1);
+        if (np > 0) b.seg(BB, ppph, np, T_, P_PPPH, BA, ppph, np, N_, P_PPPH, np, -1.0, 0, 1);
+        b.drop_if_empty();
+      }
+      if (np > 0 && nh > 0) {  // Apppp Bpphh - Bpppp Apphh - Apphh Bhhhh + Bpphh Ahhhh
+        b.prob(np, nh, pphh, np, GM_ACC, BO0);
+        b.seg(BA, pppp, np, N_, P_PPPP, BB, pphh, np, N_, P_PPHH, np, 1.0);
+        b.seg(BB, pppp, np, N_, P_PPPP, BA, pphh, np, N_, P_PPHH, np, -1.0);
+        b.seg(BA, pphh, np, N_, P_PPHH, BB, hhhh, nh, N_, P_HHHH, nh, -1.0);
+        b.seg(BB, pphh, np, N_, P_PPHH, BA, hhhh, nh, N_, P_HHHH, nh, 1.0);
+        b.drop_if_empty();
+      }
+      if (nb > 0 && nh > 0) {  // hA Appph^T Bpphh - hB Bppph^T Apphh - Aphhh Bhhhh + Bphhh Ahhhh
+        b.prob(nb, nh, phhh, nb, GM_ACC, BO0);
+        if (np > 0) {
+          b.seg(BA, ppph, np, T_, P_PPPH, BB, pphh, np, N_, P_PPHH, np, 1.0, 1, 0);
+          b.seg(BB, ppph, np, T_, P_PPPH, BA, pphh, np, N_, P_PPHH, np, -1.0, 0, 1);
+        }
+        b.seg(BA, phhh, nb, N_, P_PHHH, BB, hhhh, nh, N_, P_HHHH, nh, -1.0);
+        b.seg(BB, phhh, nb, N_, P_PHHH, BA, hhhh, nh, N_, P_HHHH, nh, 1.0);
+        b.drop_if_empty();
+      }
+      if (np > 0 && nb > 0) {  // -hB Apphh Bphhh^T + hA Bpphh Aphhh^T + Apppp Bppph - Bpppp Appph
+        b.prob(np, nb, ppph, np, GM_ACC, BO0);
+        if (nh > 0) {
+          b.seg(BA, pphh, np, N_, P_PPHH, BB, phhh, nb, T_, P_PHHH, nh, -1.0, 0, 1);
+          b.seg(BB, pphh, np, N_, P_PPHH, BA, phhh, nb, T_, P_PHHH, nh, 1.0, 1, 0);
+        }
+        b.seg(BA, pppp, np, N_, P_PPPP, BB, ppph, np, N_, P_PPPH, np, 1.0);
+        b.seg(BB, pppp, np, N_, P_PPPP, BA, ppph, np, N_, P_PPPH, np, -1.0);
+        b.drop_if_empty();
+      }
+    }
+  }
+  // ---- commutator_221 intermediates (SET into w1 = BO0, w2 = BO1) ----
+  {
+    GemmProgram& P = L->prog_221;
+    Builder b(P);
+    for (int q = 0; q < L->nblock; ++q) {
+      const int nh = L->blk[q].x, nb = L->blk[q].y, np = L->blk[q].z;
+      const i64* o = &L->boff[6 * q];
+      const i64 hhhh = o[0], pppp = o[1], pphh = o[2], phph = o[3], ppph = o[4], phhh = o[5];
+      if (np * nh != 0) {
+        b.prob(np, np, pppp, np, GM_SET, BO0);  // w1%Vpppp = Apphh Bpphh^T
+        b.seg(BA, pphh, np, N_, P_PPHH, BB, pphh, np, T_, P_PPHH, nh, 1.0);
+      }
+      if (np * nb != 0) {
+        b.prob(nb, nb, phph, nb, GM_SET, BO0);  // w1%Vphph = Bppph^T Appph
+        b.seg(BB, ppph, np, T_, P_PPPH, BA, ppph, np, N_, P_PPPH, np, 1.0);
+      }
+      if (nh * np != 0) {
+        b.prob(nh, nh, hhhh, nh, GM_SET, BO0);  // w1%Vhhhh = Bpphh^T Apphh
+        b.seg(BB, pphh, np, T_, P_PPHH, BA, pphh, np, N_, P_PPHH, np, 1.0);
+      }
+      if (nh * nb != 0) {
+        b.prob(nb, nb, phph, nb, GM_SET, BO1);  // w2%Vphph = Aphhh Bphhh^T
+        b.seg(BA, phhh, nb, N_, P_PHHH, BB, phhh, nb, T_, P_PHHH, nh, 1.0);
+      }
+      if (nh * nb * np != 0) {
+        b.prob(nb, nh, phhh, nb, GM_SET, BO0);  // w1%Vphhh = Bppph^T Apphh
+        b.seg(BB, ppph, np, T_, P_PPPH, BA, pphh, np, N_, P_PPHH, np, 1.0);
+        b.prob(nb, nh, phhh, nb, GM_SET, BO1);  // w2%Vphhh = Appph^T Bpphh
+        b.seg(BA, ppph, np, T_, P_PPPH, BB, pphh, np, N_, P_PPHH, np, 1.0);
+        b.prob(np, nb, ppph, np, GM_SET, BO0);  // w1%Vppph = Apphh Bphhh^T
+        b.seg(BA, pphh, np, N_, P_PPHH, BB, phhh, nb, T_, P_PHHH, nh, 1.0);
+        b.prob(np, nb, ppph, np, GM_SET, BO1);  // w2%Vppph = Bpphh Aphhh^T
+        b.seg(BB, pphh, np, N_, P_PPHH, BA, phhh, nb, T_, P_PHHH, nh, 1.0);
+      }
+    }
+  }
+  // ---- commutator_111 (SET into C's one-body part) ----
+  {
+    GemmProgram& P = L->prog_111;
+    Builder b(P);
+    if (n > 0) {  // V = Afhh Bfhh - hB Bfph^T Afph ; fhh = V + s V^T
+      b.prob(n, n, L->o_fhh, n, GM_SET_PAIR, BO0, -1.0, 1, 1);
+      b.seg(BA, L->o_fhh, n, N_, P_FHH, BB, L->o_fhh, n, N_, P_FHH, n, 1.0);
+      if (mp > 0) b.seg(BB, L->o_fph, mp, T_, P_FPH, BA, L->o_fph, mp, N_, P_FPH, mp, -1.0, 0, 1);
+    }
+    if (mp > 0) {  // V = hB Afph Bfph^T - Bfpp Afpp ; fpp = V + s V^T
+      b.prob(mp, mp, L->o_fpp, mp, GM_SET_PAIR, BO0, -1.0, 1, 1);
+      if (n > 0) b.seg(BA, L->o_fph, mp, N_, P_FPH, BB, L->o_fph, mp, T_, P_FPH, n, 1.0, 0, 1);
+      b.seg(BB, L->o_fpp, mp, N_, P_FPP, BA, L->o_fpp, mp, N_, P_FPP, mp, -1.0);
+    }
+    if (mp > 0 && n > 0) {  // fph = Afph Bfhh - Bfph Afhh + Afpp Bfph - Bfpp Afph
+      b.prob(mp, n, L->o_fph, mp, GM_SET, BO0);
+      b.seg(BA, L->o_fph, mp, N_, P_FPH, BB, L->o_fhh, n, N_, P_FHH, n, 1.0);
+      b.seg(BB, L->o_fph, mp, N_, P_FPH, BA, L->o_fhh, n, N_, P_FHH, n, -1.0);
+      b.seg(BA, L->o_fpp, mp, N_, P_FPP, BB, L->o_fph, mp, N_, P_FPH, mp, 1.0);
+      b.seg(BB, L->o_fpp, mp, N_, P_FPP, BA, L->o_fph, mp, N_, P_FPH, mp, -1.0);
+    }
+  }
+  // ---- construct_cc_ints as Z = XCC - YCC = hB P - hA P^T, P = X_A X_B^T ----
+  {
+    GemmProgram& P = L->prog_pandya;
+    Builder b(P);
+    for (int q = 0; q < L->ncc; ++q) {
+      const int r = L->ccdim[q].x, nb = L->ccdim[q].y;
+      if (r == 0) continue;
+      b.prob(r, r, L->cczoff[q], r, GM_SET_PAIR, BZ, -1.0, 1, 1);  // nb == 0 writes zeros
+      if (nb > 0) b.seg(BXA, L->ccxoff[q], r, N_, -1, BXB, L->ccxoff[q], r, T_, -1, nb, 1.0, 0, 1);
+    }
+  }
+  // upload
+  for (GemmProgram* P : {&L->prog_ladder, &L->prog_221, &L->prog_111, &L->prog_pandya}) {
+    size_t pb = std::max<size_t>(1, P->probs.size()) * sizeof(GProb);
+    size_t sb = std::max<size_t>(1, P->segs.size()) * sizeof(GSeg);
+    QD_CUDA(cudaMalloc(&P->d_probs, pb));
+    QD_CUDA(cudaMalloc(&P->d_segs, sb));
+    if (!P->probs.empty())
+      QD_CUDA(cudaMemcpy(P->d_probs, P->probs.data(), P->probs.size() * sizeof(GProb), cudaMemcpyHostToDevice));
+    if (!P->segs.empty())
+      QD_CUDA(cudaMemcpy(P->d_segs, P->segs.data(), P->segs.size() * sizeof(GSeg), cudaMemcpyHostToDevice));
+  }
+  QD_CUDA(cudaFuncSetAttribute(k_grouped_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
+  L->programs_built = true;
+  return QD_OK;
+}
+
+static bool seg_active_host(const GSeg& s, unsigned mA, unsigned mB) {
+  auto dead = [&](int src, int dep) {
+    if (dep < 0) return false;
+    unsigned m = src == 0 ? mA : (src == 1 ? mB : 0u);
+    return ((m >> dep) & 1u) != 0;
+  };
+  return !dead(s.srcA, s.depA) && !dead(s.srcB, s.depB);
+}
+
+// Task list for (maskA, maskB): every tile (tile pair in the pair modes) of
+// every problem that has an active segment (SET problems always: they must
+// write), longest first.
+static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTask** d_tasks, int* ntasks) {
+  auto key = std::make_pair(mA, mB);
+  auto it = P.tasks.find(key);
+  if (it != P.tasks.end()) {
+    *d_tasks = it->second.first;
+    *ntasks = it->second.second;
+    return QD_OK;
+  }
+  std::vector<std::pair<double, GTask>> v;
+  for (size_t pi = 0; pi < P.probs.size(); ++pi) {
+    const GProb& g = P.probs[pi];
+    double kt = 0.0;
+    for (int k = 0; k < g.nseg; ++k) {
+      const GSeg& s = P.segs[g.seg0 + k];
+      if (seg_active_host(s, mA, mB)) kt += (s.K + BK - 1) / BK;
+    }
+    bool set = g.mode == GM_SET || g.mode == GM_SET_PAIR;
+    if (kt == 0.0 && !set) continue;
+    int tm = (g.M + BM - 1) / BM, tn = (g.N + BN - 1) / BN;
+    bool pair = g.mode == GM_ACC_PAIR || g.mode == GM_SET_PAIR;
+    for (int i = 0; i < tm; ++i)
+      for (int j = pair ? i : 0; j < tn; ++j) {
+        GTask t;
+        t.prob = (int)pi;
+        t.ti = (short)i;
+        t.tj = (short)j;
+        double cost = (kt + 1.0) * ((pair && i != j) ? 2.0 : 1.0);
+        v.push_back({cost, t});
+      }
+  }
+  std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<GTask> h(v.size());
+  for (size_t i = 0; i < v.size(); ++i) h[i] = v[i].second;
+  GTask* d = nullptr;
+  if (!h.empty()) {
+    QD_CUDA(cudaMalloc(&d, h.size() * sizeof(GTask)));
+    QD_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(GTask), cudaMemcpyHostToDevice));
+  }
+  P.tasks[key] = std::make_pair(d, (int)h.size());
+  *d_tasks = d;
+  *ntasks = (int)h.size();
+  return QD_OK;
+}
+
+int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
+                unsigned maskB) {
+  int rc = build_programs(L);
+  if (rc) return rc;
+  GTask* d_tasks = nullptr;
+  int nt = 0;
+  if ((rc = get_tasks(L, P, maskA, maskB, &d_tasks, &nt))) return rc;
+  if (nt == 0) return QD_OK;
+  Bufs b;
+  for (int i = 0; i < NBUF; ++i) b.p[i] = bufs[i];
+  k_grouped_gemm<<<nt, GEMM_THREADS, GEMM_SMEM, L->stream>>>(d_tasks, P.d_probs, P.d_segs, b, hv0, hv1, maskA, maskB);
+  ++L->nlaunch;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+}  // namespace qd

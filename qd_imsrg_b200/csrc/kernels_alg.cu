@@ -1,0 +1,321 @@
+// kernels_alg.cu -- bandwidth-bound kernels of the commutator engine:
+// axpy (add_arrays), deterministic FP64 reductions (commutator_110/220 traces,
+// mat_2_norm, MBPT2, HF_E2), the White generator, the Pandya re-coupling
+// (calc_cc) and the particle-hole gather of commutator_222.
+#include "dev_common.cuh"
+
+namespace qd {
+
+// ---------------------------------------------------------------------------
+// add_arrays (src/ME_general.f90:592-618): c = sa*a + sb*b over the whole
+// vectorize array (E0 included).  double2-vectorised when all three pointers
+// share 16-byte alignment.
+// ---------------------------------------------------------------------------
+__global__ void k_axpy(const double* __restrict__ a, double sa, const double* __restrict__ b, double sb,
+                       double* __restrict__ c, i64 n) {
+  i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) c[i] = sa * a[i] + sb * b[i];
+}
+__global__ void k_axpy2(const double2* __restrict__ a, double sa, const double2* __restrict__ b, double sb,
+                        double2* __restrict__ c, i64 n2) {
+  i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
+    double2 x = a[i], y = b[i];
+    c[i] = make_double2(sa * x.x + sb * y.x, sa * x.y + sb * y.y);
+  }
+}
+
+int launch_axpy(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, i64 n) {
+  const int threads = 256, blocks = 148 * 8;
+  if ((((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15) == 0) {
+    k_axpy2<<<blocks, threads, 0, L->stream>>>((const double2*)a, sa, (const double2*)b, sb, (double2*)c, n / 2);
+    ++L->nlaunch;
+    if (n & 1) {
+      k_axpy<<<1, 32, 0, L->stream>>>(a + n - 1, sa, b + n - 1, sb, c + n - 1, 1);
+      ++L->nlaunch;
+    }
+  } else {
+    k_axpy<<<blocks, threads, 0, L->stream>>>(a, sa, b, sb, c, n);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic two-stage reductions.  Stage 1: RED_BLOCKS CTAs, fixed
+// element->thread assignment, fixed tree -> partial[b].  Stage 2: one CTA sums
+// the partials in a fixed order and writes scale*sum (+ add*out) to *out.
+// ---------------------------------------------------------------------------
+struct RedDotRange {  // sum a[i]*b[i] (or a[i]^2) over [o, o+n)
+  const double* a;
+  const double* b;
+  i64 o;
+  __device__ double operator()(i64 i) const {
+    double x = a[o + i];
+    return x * (b ? b[o + i] : x);
+  }
+};
+
+// element e of two-body part p -> (block, offset of the element in vectorize order)
+__device__ __forceinline__ void part_elem(const DevLayout& L, int p, i64 e, int& q, i64& pos, int& row, int& col) {
+  const i64* cum = L.pcum + (i64)p * L.nblock;
+  q = find_seg(cum, L.nblock, e);
+  i64 loc = e - __ldg(cum + q);
+  const int4 bd = __ldg(&L.blk[q]);
+  int part = P_HHHH + p;
+  int rows = part_rows(part, bd);
+  row = (int)(loc % rows);
+  col = (int)(loc / rows);
+  // the six block offsets are stored in part order (hhhh, pppp, pphh, phph, ppph, phhh)
+  pos = __ldg(L.boff + 6 * q + p) + loc;
+}
+
+struct RedDotPart {  // sum over all entries of one two-body part: a*b (or a^2)
+  DevLayout L;
+  const double* a;
+  const double* b;
+  int p;
+  __device__ double operator()(i64 e) const {
+    int q, row, col;
+    i64 pos;
+    part_elem(L, p, e, q, pos, row, col);
+    double x = a[pos];
+    return x * (b ? b[pos] : x);
+  }
+};
+
+// MBPT2 (src/HFQDmod.f90:325-362): Vpphh^2 / (fhh(h1,h1)+fhh(h2,h2)-(fpp(p1,p1)+fpp(p2,p2)))
+struct RedMBPT2 {
+  DevLayout L;
+  const double* h;
+  __device__ double operator()(i64 e) const {
+    int q, row, col;
+    i64 pos;
+    part_elem(L, P_PPHH - P_HHHH, e, q, pos, row, col);
+    int2 pp = block_pair(L, q, 2, row), hh = block_pair(L, q, 0, col);
+    const int n = L.n, mp = L.mp;
+    double f12 = h[L.o_fpp + (pp.x - n) + (i64)(pp.x - n) * mp] + h[L.o_fpp + (pp.y - n) + (i64)(pp.y - n) * mp];
+    double denom = h[L.o_fhh + hh.x + (i64)hh.x * n] + h[L.o_fhh + hh.y + (i64)hh.y * n] - f12;
+    double x = h[pos];
+    return x * x / denom;
+  }
+};
+
+// HF_E2 trace: sum over blocks of Vhhhh(j,j)
+struct RedHHTrace {
+  DevLayout L;
+  const double* h;
+  __device__ double operator()(i64 e) const {
+    int q, row, col;
+    i64 pos;
+    part_elem(L, P_HHHH - P_HHHH, e, q, pos, row, col);
+    return row == col ? h[pos] : 0.0;
+  }
+};
+
+template <class F>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce(F f, i64 n, double* __restrict__ partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  double s = 0.0;
+  i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) s += f(i);
+  s = block_sum<RED_THREADS>(s, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// out = scale * sum(partial) + add * (*out)
+__global__ void k_reduce_final(const double* __restrict__ partial, int np, double scale, double add,
+                               double* __restrict__ out) {
+  __shared__ double sh[RED_THREADS / 32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[i];
+  s = block_sum<RED_THREADS>(s, sh);
+  if (threadIdx.x == 0) *out = scale * s + (add != 0.0 ? add * (*out) : 0.0);
+}
+
+__global__ void k_sqrt(double* x) { *x = sqrt(*x); }
+
+int ensure_reduction(qd_layout* L) {
+  if (!L->d_red) {
+    QD_CUDA(cudaMalloc(&L->d_red, sizeof(double) * (RED_BLOCKS + 64)));
+    L->ws_bytes += sizeof(double) * (RED_BLOCKS + 64);
+  }
+  if (!L->h_red) QD_CUDA(cudaMallocHost(&L->h_red, sizeof(double) * 64));
+  return QD_OK;
+}
+
+template <class F>
+static int reduce_to(qd_layout* L, const F& f, i64 n, double scale, double add, double* dout) {
+  int rc = ensure_reduction(L);
+  if (rc) return rc;
+  if (n > 0) {
+    k_reduce<F><<<RED_BLOCKS, RED_THREADS, 0, L->stream>>>(f, n, L->d_red);
+    k_reduce_final<<<1, RED_THREADS, 0, L->stream>>>(L->d_red, RED_BLOCKS, scale, add, dout);
+    L->nlaunch += 2;
+  } else {
+    k_reduce_final<<<1, RED_THREADS, 0, L->stream>>>(L->d_red, 0, scale, add, dout);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// Device scalar slots in d_red beyond the partials
+double* red_slot(qd_layout* L, int k) { return L->d_red + RED_BLOCKS + k; }
+
+int reduce_dot_range(qd_layout* L, const double* a, const double* b, i64 o, i64 n, double scale, double add,
+                     double* dout) {
+  return reduce_to(L, RedDotRange{a, b, o}, n, scale, add, dout);
+}
+int reduce_dot_part(qd_layout* L, const double* a, const double* b, int part, double scale, double add, double* dout) {
+  int p = part - P_HHHH;
+  return reduce_to(L, RedDotPart{L->dev, a, b, p}, L->dev.pcnt[p], scale, add, dout);
+}
+int reduce_mbpt2(qd_layout* L, const double* h, double* dout) {
+  return reduce_to(L, RedMBPT2{L->dev, h}, L->dev.pcnt[P_PPHH - P_HHHH], 1.0, 0.0, dout);
+}
+int reduce_hhtrace(qd_layout* L, const double* h, double* dout) {
+  return reduce_to(L, RedHHTrace{L->dev, h}, L->dev.pcnt[0], 1.0, 0.0, dout);
+}
+// mat_2_norm: one-body parts only, sqrt taken on the device
+int reduce_norm1b(qd_layout* L, const double* a, double* dout) {
+  i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
+  int rc = reduce_to(L, RedDotRange{a, nullptr, L->o_fhh}, n1, 1.0, 0.0, dout);
+  if (rc) return rc;
+  k_sqrt<<<1, 1, 0, L->stream>>>(dout);
+  ++L->nlaunch;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// build_white (src/IMSRG_tools.f90:377-434)
+// ---------------------------------------------------------------------------
+__global__ void k_white_1b(DevLayout L, double* __restrict__ gen, const double* __restrict__ h, double herm) {
+  i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = L.n, mp = L.mp;
+  if (e >= (i64)mp * n) return;
+  int a = (int)(e % mp), i = (int)(e / mp);  // fph(a,i), a particle-local
+  int as = n + a;
+  double d = h[L.o_fpp + a + (i64)a * mp] - h[L.o_fhh + i + (i64)i * n] - dv_elem(L, h, herm, as, i, as, i);
+  gen[L.o_fph + e] = h[L.o_fph + e] / d;
+}
+
+__global__ void k_white_2b(DevLayout L, double* __restrict__ gen, const double* __restrict__ h, double herm) {
+  i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= L.pcnt[P_PPHH - P_HHHH]) return;
+  int q, row, col;
+  i64 pos;
+  part_elem(L, P_PPHH - P_HHHH, e, q, pos, row, col);
+  int2 p = block_pair(L, q, 2, row), hh = block_pair(L, q, 0, col);
+  const int n = L.n, mp = L.mp;
+  double efs = h[L.o_fpp + (p.x - n) + (i64)(p.x - n) * mp];
+  efs = efs + h[L.o_fpp + (p.y - n) + (i64)(p.y - n) * mp];
+  efs = efs - h[L.o_fhh + hh.x + (i64)hh.x * n];
+  efs = efs - h[L.o_fhh + hh.y + (i64)hh.y * n];
+  double Aph = dv_elem(L, h, herm, p.x, p.y, p.x, p.y) + dv_elem(L, h, herm, hh.x, hh.y, hh.x, hh.y) -
+               dv_elem(L, h, herm, p.x, hh.x, p.x, hh.x) - dv_elem(L, h, herm, p.x, hh.y, p.x, hh.y) -
+               dv_elem(L, h, herm, p.y, hh.x, p.y, hh.x) - dv_elem(L, h, herm, p.y, hh.y, p.y, hh.y);
+  gen[pos] = h[pos] / (efs + Aph);
+}
+
+int launch_white(qd_layout* L, double* gen, const double* h, int herm) {
+  i64 n1 = (i64)L->mp * L->n;
+  if (n1 > 0) {
+    k_white_1b<<<(unsigned)((n1 + 255) / 256), 256, 0, L->stream>>>(L->dev, gen, h, (double)herm);
+    ++L->nlaunch;
+  }
+  i64 n2 = L->dev.pcnt[P_PPHH - P_HHHH];
+  if (n2 > 0) {
+    k_white_2b<<<(unsigned)((n2 + 255) / 256), 256, 0, L->stream>>>(L->dev, gen, h, (double)herm);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// calc_cc (src/commutators.f90:1135-1159): X_q(r,nb) = v_elem(j,k,i,l,H)
+// with (i,j) the r-th row pair and (k,l) the nb-th (hole,particle) column pair.
+// ---------------------------------------------------------------------------
+__global__ void k_calc_cc(DevLayout L, const double* __restrict__ h, double herm, double* __restrict__ X,
+                          i64 xsize) {
+  i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= xsize) return;
+  int q = find_seg(L.ccxoff, L.ncc, e);
+  i64 loc = e - __ldg(L.ccxoff + q);
+  int2 d = __ldg(&L.ccdim[q]);
+  int r = (int)(loc % d.x), c = (int)(loc / d.x);
+  int2 ab = __ldg(&L.ccab[__ldg(&L.ccab_base[q]) + r]);
+  int2 kl = __ldg(&L.cchp[__ldg(&L.cchp_base[q]) + c]);
+  X[e] = dv_elem(L, h, herm, ab.y, kl.x, ab.x, kl.y);
+}
+
+int launch_calc_cc(qd_layout* L, const qd_op* H, double* X) {
+  if (L->xsize > 0) {
+    k_calc_cc<<<(unsigned)((L->xsize + 255) / 256), 256, 0, L->stream>>>(L->dev, H->d, (double)H->herm, X, L->xsize);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Particle-hole channel of commutator_222 (src/commutators.f90:716-980):
+// with legs (1,2|3,4) of the stored element and Z = XCC - YCC,
+//   C += Z[31](r31,r24) - Z[32](r32,r14) + Z[42](r42,r13) - Z[41](r41,r23).
+// Stored pairs are (a<b); the reference's particle-first naming of ph pairs
+// with pre = -1 is the same element by antisymmetry.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double zget(const DevLayout& L, const double* __restrict__ Z, int x, int y, int u, int v) {
+  int2 a = __ldg(&L.ccmap[x * L.m + y]);
+  int2 b = __ldg(&L.ccmap[u * L.m + v]);
+  int r = __ldg(&L.ccdim[a.x]).x;
+  return Z[__ldg(&L.cczoff[a.x]) + a.y + (i64)b.y * r];
+}
+
+__device__ __forceinline__ void decode2b(const DevLayout& L, i64 e, int& q, int& part, int& row, int& col) {
+  int s = find_seg(L.s2off, L.ns2, e);
+  int id = __ldg(L.s2id + s);
+  q = id >> 3;
+  part = P_HHHH + (id & 7);
+  i64 loc = e - __ldg(L.s2off + s);
+  int rows = part_rows(part, __ldg(&L.blk[q]));
+  row = (int)(loc % rows);
+  col = (int)(loc / rows);
+}
+
+__global__ void k_pandya_gather(DevLayout L, const double* __restrict__ Z, double* __restrict__ C) {
+  i64 e = L.o2 + (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= L.neq) return;
+  int q, part, row, col;
+  decode2b(L, e, q, part, row, col);
+  int cb, ck;
+  part_classes(part, cb, ck);
+  int2 br = block_pair(L, q, cb, row), kt = block_pair(L, q, ck, col);
+  const int b1 = br.x, b2 = br.y, k1 = kt.x, k2 = kt.y;
+  double X = zget(L, Z, k1, b1, b2, k2) - zget(L, Z, k1, b2, b1, k2) + zget(L, Z, k2, b2, b1, k1) -
+             zget(L, Z, k2, b1, b2, k1);
+  C[e] += X;
+}
+
+int launch_pandya_gather(qd_layout* L, const double* Z, double* C) {
+  i64 n2 = L->neq - L->dev.o2;
+  if (n2 > 0) {
+    k_pandya_gather<<<(unsigned)((n2 + 255) / 256), 256, 0, L->stream>>>(L->dev, Z, C);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+int ensure_z(qd_layout* L) {
+  if (!L->d_z && L->zsize > 0) {
+    QD_CUDA(cudaMalloc(&L->d_z, sizeof(double) * L->zsize));
+    L->ws_bytes += sizeof(double) * L->zsize;
+  }
+  return QD_OK;
+}
+
+}  // namespace qd

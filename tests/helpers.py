@@ -1,0 +1,84 @@
+"""Test helpers: comparison of vectorize-order operators part by part."""
+import numpy as np
+
+PART_NAMES = ["Vhhhh", "Vpppp", "Vpphh", "Vphph", "Vppph", "Vphhh"]
+
+
+def part_slices(layout):
+    """[(name, index array)] of the one-body and two-body parts of a layout
+    (oracle.Layout or qd_imsrg_b200.Layout; both expose dims/offs/nbody)."""
+    n = getattr(layout, "nbody", getattr(layout, "n", None))
+    m = getattr(layout, "msp", getattr(layout, "m", None))
+    mp = m - n
+    out = [("E0", np.array([0]))]
+    o = 1
+    out.append(("fhh", np.arange(o, o + n * n))); o += n * n
+    out.append(("fpp", np.arange(o, o + mp * mp))); o += mp * mp
+    out.append(("fph", np.arange(o, o + mp * n))); o += mp * n
+    idx = {k: [] for k in PART_NAMES}
+    for q in range(layout.nblock):
+        nh, nb, npp = (int(x) for x in layout.dims[q, :3])
+        sizes = [nh * nh, npp * npp, npp * nh, nb * nb, npp * nb, nb * nh]
+        for k, (name, sz) in enumerate(zip(PART_NAMES, sizes)):
+            if sz:
+                st = int(layout.offs[q, k])
+                idx[name].append(np.arange(st, st + sz))
+    for name in PART_NAMES:
+        out.append((name, np.concatenate(idx[name]) if idx[name] else np.zeros(0, np.int64)))
+    return out
+
+
+def compare_parts(layout, got, ref, rtol=1e-12, atol_floor=1e-300):
+    """Relative Frobenius error per part; returns {name: (rel, maxabs)} and
+    raises AssertionError listing parts above rtol."""
+    res, bad = {}, []
+    for name, ix in part_slices(layout):
+        if ix.size == 0:
+            continue
+        d = got[ix] - ref[ix]
+        nr = np.linalg.norm(ref[ix])
+        rel = np.linalg.norm(d) / max(nr, atol_floor)
+        mx = float(np.abs(d).max())
+        res[name] = (rel, mx)
+        if nr == 0.0:
+            if mx > 1e-13:
+                bad.append("%s: ref is zero, max|diff|=%.3e" % (name, mx))
+        elif rel > rtol:
+            bad.append("%s: rel %.3e max %.3e" % (name, rel, mx))
+    assert not bad, "; ".join(bad)
+    return res
+
+
+def numpy_random_op(L, herm, rng, conserve=True, sigma=0.1):
+    """Independent numpy generator of a test operator for an oracle.Layout:
+    N(0, sigma^2) entries, diagonal-class blocks (X + herm X^T)/2, E0 = 0."""
+    v = rng.normal(0.0, sigma, L.neq)
+    v[0] = 0.0
+    n, m = L.n, L.m
+    mp = m - n
+
+    def sym(o, k):
+        A = v[o:o + k * k].reshape(k, k, order="F")
+        v[o:o + k * k] = ((A + herm * A.T) / 2).reshape(-1, order="F")
+
+    sym(1, n)
+    sym(1 + n * n, mp)
+    if conserve:
+        g = L.qn[:, 1] * 10 + L.qn[:, 2]
+        o = 1
+        F = v[o:o + n * n].reshape(n, n, order="F").copy(); F[g[:n, None] != g[None, :n]] = 0
+        v[o:o + n * n] = F.reshape(-1, order="F"); o += n * n
+        F = v[o:o + mp * mp].reshape(mp, mp, order="F").copy(); F[g[n:, None] != g[None, n:]] = 0
+        v[o:o + mp * mp] = F.reshape(-1, order="F"); o += mp * mp
+        F = v[o:o + mp * n].reshape(mp, n, order="F").copy(); F[g[n:, None] != g[None, :n]] = 0
+        v[o:o + mp * n] = F.reshape(-1, order="F")
+    for q in range(L.nblock):
+        nh, nb, npp = (int(x) for x in L.dims[q, :3])
+        oh, opp, _, oph = (int(x) for x in L.offs[q, :4])
+        if nh:
+            sym(oh, nh)
+        if npp:
+            sym(opp, npp)
+        if nb:
+            sym(oph, nb)
+    return v
