@@ -11,6 +11,7 @@
 
 namespace qd {
 const char* last_error();
+void drop_122_plan(const qd_layout* L);
 }  // namespace qd
 
 using namespace qd;
@@ -329,6 +330,7 @@ int qd_layout_destroy(qd_layout* L) {
   cudaSetDevice(L->device);
   cudaStreamSynchronize(L->stream);
   drop_ws(L);
+  drop_122_plan(L);
   layout_free_device(L);
   delete L;
   return QD_OK;

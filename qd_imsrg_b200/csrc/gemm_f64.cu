@@ -63,104 +63,120 @@ __device__ __forceinline__ bool seg_active(const GSeg& s, unsigned mA, unsigned 
   return !dead(s.srcA, s.depA) && !dead(s.srcB, s.depB);
 }
 
-// Load the (row0, col0) tile's k-slab [k0, k0+BK) of segment s into stage buffers.
-__device__ __forceinline__ void load_stage(const GSeg& s, const Bufs& bufs, int M, int N, int row0, int col0,
-                                           int k0, double* sA, double* sB) {
+// Load the (row0, col0) tile's k-slab [k0, k0+BK) of segment s (operands at
+// A, B) into stage buffers sA[k][m], sB[k][n].  Each thread walks a fixed
+// column (or row) with a pointer stride; out-of-range elements are zero-filled.
+__device__ __forceinline__ void load_stage(const GSeg& s, const double* A, const double* B, int M, int N, int row0,
+                                           int col0, int k0, double* sA, double* sB) {
   const int tid = threadIdx.x;
-  const double* A = bufs.p[s.srcA] + s.offA;
-  const double* B = bufs.p[s.srcB] + s.offB;
+  constexpr int IT = (BM * BK) / GEMM_THREADS;  // 8
+  if (!s.tA) {  // A(m,k) at A[m + k*lda]: threads along m
+    const int mm = tid & (BM - 1), kk0 = tid >> 6;
+    const bool rok = row0 + mm < M;
+    const double* g = A + (row0 + mm) + (i64)(k0 + kk0) * s.lda;
+    const i64 step = (i64)2 * s.lda;
 #pragma unroll
-  for (int it = 0; it < (BM * BK) / GEMM_THREADS; ++it) {
-    int idx = tid + it * GEMM_THREADS;
-    int mm, kk;
-    if (!s.tA) {
-      mm = idx & (BM - 1);
-      kk = idx >> 6;
-    } else {
-      kk = idx & (BK - 1);
-      mm = idx >> 4;
+    for (int it = 0; it < IT; ++it) {
+      const int kk = kk0 + 2 * it;
+      const bool ok = rok && (k0 + kk < s.K);
+      cp_async8(sA + kk * LDS + mm, ok ? g : A, ok);
+      g += step;
     }
-    int gm = row0 + mm, gk = k0 + kk;
-    bool ok = gm < M && gk < s.K;
-    const double* src = ok ? (s.tA ? A + gk + (i64)gm * s.lda : A + gm + (i64)gk * s.lda) : A;
-    cp_async8(sA + kk * LDS + mm, src, ok);
+  } else {  // op(A)(m,k) = A[k + m*lda]: threads along k
+    const int kk = tid & (BK - 1), mm0 = tid >> 4;
+    const bool kok = k0 + kk < s.K;
+    const double* g = A + (k0 + kk) + (i64)(row0 + mm0) * s.lda;
+    const i64 step = (i64)8 * s.lda;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int mm = mm0 + 8 * it;
+      const bool ok = kok && (row0 + mm < M);
+      cp_async8(sA + kk * LDS + mm, ok ? g : A, ok);
+      g += step;
+    }
   }
+  if (!s.tB) {  // B(k,n) at B[k + n*ldb]: threads along k
+    const int kk = tid & (BK - 1), nn0 = tid >> 4;
+    const bool kok = k0 + kk < s.K;
+    const double* g = B + (k0 + kk) + (i64)(col0 + nn0) * s.ldb;
+    const i64 step = (i64)8 * s.ldb;
 #pragma unroll
-  for (int it = 0; it < (BN * BK) / GEMM_THREADS; ++it) {
-    int idx = tid + it * GEMM_THREADS;
-    int nn, kk;
-    if (!s.tB) {
-      kk = idx & (BK - 1);
-      nn = idx >> 4;
-    } else {
-      nn = idx & (BN - 1);
-      kk = idx >> 6;
+    for (int it = 0; it < IT; ++it) {
+      const int nn = nn0 + 8 * it;
+      const bool ok = kok && (col0 + nn < N);
+      cp_async8(sB + kk * LDS + nn, ok ? g : B, ok);
+      g += step;
     }
-    int gn = col0 + nn, gk = k0 + kk;
-    bool ok = gn < N && gk < s.K;
-    const double* src = ok ? (s.tB ? B + gn + (i64)gk * s.ldb : B + gk + (i64)gn * s.ldb) : B;
-    cp_async8(sB + kk * LDS + nn, src, ok);
+  } else {  // op(B)(k,n) = B[n + k*ldb]: threads along n
+    const int nn = tid & (BN - 1), kk0 = tid >> 6;
+    const bool nok = col0 + nn < N;
+    const double* g = B + (col0 + nn) + (i64)(k0 + kk0) * s.ldb;
+    const i64 step = (i64)2 * s.ldb;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int kk = kk0 + 2 * it;
+      const bool ok = nok && (k0 + kk < s.K);
+      cp_async8(sB + kk * LDS + nn, ok ? g : B, ok);
+      g += step;
+    }
   }
 }
 
-struct SegCursor {
-  int seg[8];
-  int ktiles[8];
+// Active segments of the CTA's problem, kept in shared memory.
+struct SegList {
+  GSeg seg[8];
+  const double* A[8];  // operand bases (buffer + offset)
+  const double* B[8];
+  double alpha[8];
   int nact;
-  int total;
+  int total;  // k-tiles over all active segments
 };
 
+// Advance a (segment, k0) cursor by one k-tile.
+__device__ __forceinline__ void cursor_next(const SegList& sl, int& si, int& k0) {
+  k0 += BK;
+  if (k0 >= sl.seg[si].K) {
+    ++si;
+    k0 = 0;
+  }
+}
+
 // Accumulate the tile (row0, col0) of problem P into acc[4][4][2].
-__device__ void tile_mainloop(const GProb& P, const GSeg* __restrict__ segs, const SegCursor& cur, const Bufs& bufs,
-                              double hv0, double hv1, int row0, int col0, double* smem, double acc[4][4][2]) {
+__device__ void tile_mainloop(const GProb& P, const SegList& sl, int row0, int col0, double* smem,
+                              double acc[4][4][2]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp & 1, wn = warp >> 1;
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  if (cur.total == 0) return;
+  const int total = sl.total;
+  if (total == 0) return;
   double* sA = smem;
   double* sB = smem + NSTAGE * BK * LDS;
-
-  // stage g -> (segment, k0)
-  auto locate = [&](int g, int& si, int& k0) {
-    int a = 0;
-    for (;;) {
-      if (g < cur.ktiles[a]) break;
-      g -= cur.ktiles[a];
-      ++a;
-    }
-    si = cur.seg[a];
-    k0 = g * BK;
-  };
-  // prologue
+  int ls = 0, lk = 0;  // load cursor
+  int cs = 0, ck = 0;  // compute cursor
 #pragma unroll
   for (int st = 0; st < NSTAGE - 1; ++st) {
-    if (st < cur.total) {
-      int si, k0;
-      locate(st, si, k0);
-      GSeg s = segs[si];
-      load_stage(s, bufs, P.M, P.N, row0, col0, k0, sA + st * BK * LDS, sB + st * BK * LDS);
+    if (st < total) {
+      load_stage(sl.seg[ls], sl.A[ls], sl.B[ls], P.M, P.N, row0, col0, lk, sA + st * BK * LDS,
+                 sB + st * BK * LDS);
+      cursor_next(sl, ls, lk);
     }
     cp_commit();
   }
-  for (int g = 0; g < cur.total; ++g) {
-    int gl = g + NSTAGE - 1;
-    if (gl < cur.total) {
-      int si, k0;
-      locate(gl, si, k0);
-      GSeg s = segs[si];
-      int b = gl % NSTAGE;
-      load_stage(s, bufs, P.M, P.N, row0, col0, k0, sA + b * BK * LDS, sB + b * BK * LDS);
+  for (int g = 0; g < total; ++g) {
+    const int gl = g + NSTAGE - 1;
+    if (gl < total) {
+      const int b = gl % NSTAGE;
+      load_stage(sl.seg[ls], sl.A[ls], sl.B[ls], P.M, P.N, row0, col0, lk, sA + b * BK * LDS,
+                 sB + b * BK * LDS);
+      cursor_next(sl, ls, lk);
     }
     cp_commit();
     cp_wait<NSTAGE - 1>();
     __syncthreads();
-    int si, k0;
-    locate(g, si, k0);
-    const GSeg& s = segs[si];
-    double alpha = s.c * (s.pa ? hv0 : 1.0) * (s.pb ? hv1 : 1.0);
+    const double alpha = sl.alpha[cs];
     const double* a_s = sA + (g % NSTAGE) * BK * LDS;
     const double* b_s = sB + (g % NSTAGE) * BK * LDS;
 #pragma unroll
@@ -168,14 +184,19 @@ __device__ void tile_mainloop(const GProb& P, const GSeg* __restrict__ segs, con
       double af[4], bf[4];
       const int kr = kk + (lane & 3);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) af[i] = alpha * a_s[kr * LDS + wm * 32 + i * 8 + (lane >> 2)];
+      for (int i = 0; i < 4; ++i) af[i] = a_s[kr * LDS + wm * 32 + i * 8 + (lane >> 2)];
 #pragma unroll
       for (int j = 0; j < 4; ++j) bf[j] = b_s[kr * LDS + wn * 32 + j * 8 + (lane >> 2)];
+      if (alpha != 1.0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] *= alpha;
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
+    cursor_next(sl, cs, ck);
     __syncthreads();
   }
   cp_wait<0>();
@@ -206,17 +227,23 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __re
   const GProb P = probs[t.prob];
   double* out = const_cast<double*>(bufs.p[P.outbuf]) + P.offC;
 
-  SegCursor cur;
-  cur.nact = 0;
-  cur.total = 0;
-  for (int k = 0; k < P.nseg && cur.nact < 8; ++k) {
-    const GSeg& s = segs[P.seg0 + k];
-    if (!seg_active(s, maskA, maskB) || s.K <= 0) continue;
-    cur.seg[cur.nact] = P.seg0 + k;
-    cur.ktiles[cur.nact] = (s.K + BK - 1) / BK;
-    cur.total += cur.ktiles[cur.nact];
-    ++cur.nact;
+  __shared__ SegList sl;
+  if (threadIdx.x == 0) {
+    int na = 0, tot = 0;
+    for (int k = 0; k < P.nseg && na < 8; ++k) {
+      const GSeg sg = segs[P.seg0 + k];
+      if (!seg_active(sg, maskA, maskB) || sg.K <= 0) continue;
+      sl.seg[na] = sg;
+      sl.A[na] = bufs.p[sg.srcA] + sg.offA;
+      sl.B[na] = bufs.p[sg.srcB] + sg.offB;
+      sl.alpha[na] = sg.c * (sg.pa ? hv0 : 1.0) * (sg.pb ? hv1 : 1.0);
+      tot += (sg.K + BK - 1) / BK;
+      ++na;
+    }
+    sl.nact = na;
+    sl.total = tot;
   }
+  __syncthreads();
   const bool pair = P.mode == GM_ACC_PAIR || P.mode == GM_SET_PAIR;
   const bool acc_mode = P.mode == GM_ACC || P.mode == GM_ACC_PAIR;
   double* T1 = smem + SMEM_PIPE;  // first tile stash (pair mode)
@@ -224,7 +251,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __re
   double acc[4][4][2];
 
   const int r0 = t.ti * BM, c0 = t.tj * BN;
-  tile_mainloop(P, segs, cur, bufs, hv0, hv1, r0, c0, smem, acc);
+  tile_mainloop(P, sl, r0, c0, smem, acc);
 
   if (!pair) {
     stash(T2, acc);
@@ -258,7 +285,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __re
   // off-diagonal tile pair: V(I,J) -> T1, then V(J,I) -> T2
   stash(T1, acc);
   __syncthreads();
-  tile_mainloop(P, segs, cur, bufs, hv0, hv1, c0, r0, smem, acc);
+  tile_mainloop(P, sl, c0, r0, smem, acc);
   stash(T2, acc);
   __syncthreads();
   const int mI = min(BM, P.M - r0), mJ = min(BM, P.M - c0);

@@ -9,19 +9,22 @@ namespace qd {
 // ---------------------------------------------------------------------------
 // add_arrays (src/ME_general.f90:592-618): c = sa*a + sb*b over the whole
 // vectorize array (E0 included).  double2-vectorised when all three pointers
-// share 16-byte alignment.
+// share 16-byte alignment.  Products and sum are rounded separately (no FMA
+// contraction), as in the reference's build, so the result is bit-identical.
 // ---------------------------------------------------------------------------
 __global__ void k_axpy(const double* __restrict__ a, double sa, const double* __restrict__ b, double sb,
                        double* __restrict__ c, i64 n) {
   i64 stride = (i64)gridDim.x * blockDim.x;
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) c[i] = sa * a[i] + sb * b[i];
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    c[i] = __dadd_rn(__dmul_rn(sa, a[i]), __dmul_rn(sb, b[i]));
 }
 __global__ void k_axpy2(const double2* __restrict__ a, double sa, const double2* __restrict__ b, double sb,
                         double2* __restrict__ c, i64 n2) {
   i64 stride = (i64)gridDim.x * blockDim.x;
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
     double2 x = a[i], y = b[i];
-    c[i] = make_double2(sa * x.x + sb * y.x, sa * x.y + sb * y.y);
+    c[i] = make_double2(__dadd_rn(__dmul_rn(sa, x.x), __dmul_rn(sb, y.x)),
+                       __dadd_rn(__dmul_rn(sa, x.y), __dmul_rn(sb, y.y)));
   }
 }
 

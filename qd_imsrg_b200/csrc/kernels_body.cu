@@ -115,94 +115,4 @@ int launch_221_trace(qd_layout* L, const qd_op* A, const qd_op* B, const qd_op* 
   return QD_OK;
 }
 
-// ---------------------------------------------------------------------------
-// commutator_122 (src/commutators.f90:355-676), overwriting every stored
-// two-body entry.  For the stored element <b1 b2|k1 k2> (b1<b2, k1<k2):
-//   C = sum_t [ F1(b1,t) V2(t b2|k1 k2) + F1(b2,t) V2(b1 t|k1 k2)
-//             - F1'(k1,t) V2(b1 b2|t k2) - F1'(k2,t) V2(b1 b2|k1 t) ] - (1<->2)
-// where, exactly as the reference reads them,
-//   t hole:     F(x,t) = f(x,t)            F'(x,t) = herm * f(x,t)
-//   t particle: F(x,t) = herm * f'(t,x)    F'(x,t) = f'(t,x)
-// (f, f' = the hole-loop and particle-loop reads of the reference).
-// V2(t b2|...) is non-zero only for t in the (ml,ms) group of b1, so each leg
-// sums over one group.  The reference's particle-first ph naming with
-// pre = -1 is the same element by antisymmetry.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double Fbra(const DevLayout& L, const double* __restrict__ op, double h, int x, int t) {
-  return t < L.n ? f_hole(L, op, x, t) : h * f_part(L, op, t, x);
-}
-__device__ __forceinline__ double Fket(const DevLayout& L, const double* __restrict__ op, double h, int x, int t) {
-  return t < L.n ? h * f_hole(L, op, x, t) : f_part(L, op, t, x);
-}
-
-__global__ void __launch_bounds__(256) k_122_simple(DevLayout L, const double* __restrict__ A, double hA,
-                                                    const double* __restrict__ B, double hB,
-                                                    double* __restrict__ C) {
-  i64 e = L.o2 + (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= L.neq) return;
-  int s = find_seg(L.s2off, L.ns2, e);
-  int id = __ldg(L.s2id + s);
-  int q = id >> 3, part = P_HHHH + (id & 7);
-  i64 loc = e - __ldg(L.s2off + s);
-  int rows = part_rows(part, __ldg(&L.blk[q]));
-  int row = (int)(loc % rows), col = (int)(loc / rows);
-  int cb, ck;
-  part_classes(part, cb, ck);
-  int2 br = block_pair(L, q, cb, row), kt = block_pair(L, q, ck, col);
-  const int b1 = br.x, b2 = br.y, k1 = kt.x, k2 = kt.y;
-  double acc = 0.0;
-  // bra leg 1
-  {
-    int g = __ldg(&L.gid[b1]);
-    for (int u = __ldg(&L.gstart[g]); u < __ldg(&L.gstart[g + 1]); ++u) {
-      int t = __ldg(&L.gmem[u]);
-      if (t == b2) continue;
-      acc += Fbra(L, A, hA, b1, t) * dv_elem(L, B, hB, t, b2, k1, k2) -
-             Fbra(L, B, hB, b1, t) * dv_elem(L, A, hA, t, b2, k1, k2);
-    }
-  }
-  // bra leg 2
-  {
-    int g = __ldg(&L.gid[b2]);
-    for (int u = __ldg(&L.gstart[g]); u < __ldg(&L.gstart[g + 1]); ++u) {
-      int t = __ldg(&L.gmem[u]);
-      if (t == b1) continue;
-      acc += Fbra(L, A, hA, b2, t) * dv_elem(L, B, hB, b1, t, k1, k2) -
-             Fbra(L, B, hB, b2, t) * dv_elem(L, A, hA, b1, t, k1, k2);
-    }
-  }
-  // ket leg 1
-  {
-    int g = __ldg(&L.gid[k1]);
-    for (int u = __ldg(&L.gstart[g]); u < __ldg(&L.gstart[g + 1]); ++u) {
-      int t = __ldg(&L.gmem[u]);
-      if (t == k2) continue;
-      acc -= Fket(L, A, hA, k1, t) * dv_elem(L, B, hB, b1, b2, t, k2) -
-             Fket(L, B, hB, k1, t) * dv_elem(L, A, hA, b1, b2, t, k2);
-    }
-  }
-  // ket leg 2
-  {
-    int g = __ldg(&L.gid[k2]);
-    for (int u = __ldg(&L.gstart[g]); u < __ldg(&L.gstart[g + 1]); ++u) {
-      int t = __ldg(&L.gmem[u]);
-      if (t == k1) continue;
-      acc -= Fket(L, A, hA, k2, t) * dv_elem(L, B, hB, b1, b2, k1, t) -
-             Fket(L, B, hB, k2, t) * dv_elem(L, A, hA, b1, b2, k1, t);
-    }
-  }
-  C[e] = acc;
-}
-
-int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
-  i64 n2 = L->neq - L->dev.o2;
-  if (n2 > 0) {
-    k_122_simple<<<(unsigned)((n2 + 255) / 256), 256, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d,
-                                                                      (double)B->herm, C);
-    ++L->nlaunch;
-  }
-  QD_CUDA(cudaGetLastError());
-  return QD_OK;
-}
-
 }  // namespace qd
