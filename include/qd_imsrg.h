@@ -121,6 +121,26 @@ int qd_set_to_zero(qd_op* r1);
  * empty): sqrt(sum fph^2 + sum fpp^2 + sum fhh^2)                            */
 int qd_mat_2_norm(const qd_op* r, double* out);
 
+/* Allocation-free one-body norm, for callers that must not allocate device
+ * memory while they run (a host that reserves its device-memory budget up
+ * front and forbids allocation inside its flow loop, or one whose memory is
+ * held by another allocator, where cudaMalloc may fail or synchronise the
+ * device).  No counterpart in the reference.
+ *   d_op   device array of one operator in vectorize order (e.g. from
+ *          qd_op_device_ptr); d_norm: device double receiving the norm;
+ *   stream cudaStream_t to run on (NULL: legacy default stream); the call is
+ *          asynchronous: the result is in d_norm once the stream reaches it.
+ * Nothing is allocated: the partial sums live in a static device array of
+ * QD_NOALLOC_MAX_PARTIALS doubles (32 KiB, held by every GPU that loads the
+ * library until exit).  Layouts with more than QD_NOALLOC_MAX_ENTRIES
+ * one-body entries are rejected with QD_ERR_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU race.                                                   */
+#define QD_NOALLOC_MAX_PARTIALS 4096
+#define QD_NOALLOC_MAX_ENTRIES (4096LL * 2048LL)
+int qd_mat_2_norm_noalloc(const qd_layout* L, const double* d_op, double* d_norm, void* stream);
+
 /* ---- commutators (src/commutators.f90) ------------------------------------- */
 int qd_commutator_110(const qd_op* r1, const qd_op* r2, double* c);  /* :12-33   */
 int qd_commutator_220(const qd_op* r1, const qd_op* r2, double* c);  /* :36-70   */
