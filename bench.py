@@ -197,6 +197,16 @@ def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_p
             "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs", "algorithmic_per_launch": byts}
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# engine's stages, from one ncu capture of the N=20, R=17 case (19,841,598
+# entries per operator, inputs above L2).  GEMM and gather traffic is operand
+# and output traffic, so it is scaled to the benchmarked basis by the number
+# of entries per operator.
+NCU_NEQ = 19841598
+NCU_TRAFFIC = {"ladder_gemm": 794.761728e6 + 162.643712e6, "pandya_gemm": 200.469760e6 + 676.389888e6,
+               "pandya_gather": 2126.409e6 + 154.573824e6}
+
+
 def hbm_peak_gbs() -> float:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -368,7 +378,10 @@ def main():
 
     roof = stage_roofline(prof, fl, neq2b, dgemm_peak, hbm_peak_gbs())
     roof["frac"] = roof["achieved"] / roof["peak"]
-    roof["traffic"] = None
+    stage = max(prof.items(), key=lambda kv: kv[1][0])[0]
+    roof["traffic"] = NCU_TRAFFIC[stage] * neq / NCU_NEQ if stage in NCU_TRAFFIC else None
+    roof["traffic_source"] = ("ncu dram bytes of the N=20 R=17 capture, scaled by entries per operator"
+                              if roof["traffic"] is not None else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.nbody == NBODY and args.emax == EMAX:

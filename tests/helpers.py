@@ -82,3 +82,26 @@ def numpy_random_op(L, herm, rng, conserve=True, sigma=0.1):
         if nb:
             sym(oph, nb)
     return v
+
+
+def synth_hamiltonian(L, rng, gap=2.0, vs=0.05, fs=0.05):
+    """A Hermitian test Hamiltonian on which the Magnus flow converges:
+    oscillator single-particle energies (holes lowered by `gap`) on the
+    one-body diagonal, off-diagonal one-body entries ~ N(0, fs^2), two-body
+    entries ~ N(0, vs^2), E0 = 0."""
+    v = numpy_random_op(L, 1, rng, conserve=True, sigma=vs)
+    n, m = L.n, L.m
+    mp = m - n
+    e = 2 * L.qn[:, 0] + np.abs(L.qn[:, 1]) + 1.0
+    o = 1
+    F = v[o:o + n * n].reshape(n, n, order="F") * (fs / vs)
+    F[np.diag_indices(n)] = e[:n] - gap
+    v[o:o + n * n] = F.reshape(-1, order="F")
+    o += n * n
+    F = v[o:o + mp * mp].reshape(mp, mp, order="F") * (fs / vs)
+    F[np.diag_indices(mp)] = e[n:]
+    v[o:o + mp * mp] = F.reshape(-1, order="F")
+    o += mp * mp
+    v[o:o + mp * n] *= fs / vs
+    v[0] = 0.0
+    return v
