@@ -161,6 +161,12 @@ int qd_commutator_222(const qd_op* r1, const qd_op* r2, qd_op* r3, qd_op* w1, co
  * matrices first (as dGam, src/gs_IMSRG.f90:243-250); without it the
  * particle-hole channel is skipped (X = 0, as run_magnus).                  */
 #define QD_PANDYA 1u
+/* For qd_bch_expand / qd_magnus_flow: take the BCH truncation norm and the
+ * eta norm of the step rejection over every stored one- and two-body entry.
+ * The reference's mat_2_norm sums the one-body parts only (its block loop is
+ * empty); on a Hartree-Fock Hamiltonian, whose ph Fock block vanishes, that
+ * makes the initial eta norm ~1e-16, so run_magnus rejects every step.      */
+#define QD_FULL_NORM 2u
 int qd_commutator(const qd_op* A, const qd_op* B, qd_op* C, unsigned flags);
 
 /* ---- cross-coupled (Pandya) matrices ----------------------------------------
@@ -177,6 +183,23 @@ int qd_mbpt2(const qd_op* H, double* out);        /* src/HFQDmod.f90:325-362   *
 /* HF_E2, src/HFQDmod.f90:292-323: E0 = sum_{i<=N} eig(i) - sum Vhhhh(j,j);
  * sets H's E0 as the reference does (eig as given to qd_layout_create)       */
 int qd_hf_e2(qd_op* H, double* out);
+
+/* ---- host-side inputs: Coulomb TBMEs and Hartree-Fock -----------------------
+ * The reference computes these on the host (generate_ME.f90, get_TBME.f90,
+ * src/HFQDmod.f90:9-254); they are the flow's input, not its hot path.       */
+/* Write ME.bin (records int32 n1,m1,n2,m2,n3,m3,n4,m4 + float64 Vdir at
+ * hbar-omega = 1, the stream read at src/HFQDmod.f90:97-127) for every
+ * m-conserving quadruple of spatial orbitals below emax shells, from v_int
+ * (src/ME_general.f90:2205-2276, real(16) arithmetic kept).  nthreads <= 0: 1.  */
+int qd_tbme_write(int emax, const char* path, int nthreads);
+/* construct_two_particle_HF_BASIS + HF_E2: HF single-particle energies (eig,
+ * m = emax*(emax+1), states order) and the normal-ordered HF Hamiltonian in
+ * vectorize order (vec, neq entries; E0 = E_HF).  mebin: ME.bin path, or NULL
+ * to compute the TBMEs in memory.  *iterations: HF iterations.              */
+int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double* eig, double* vec,
+                      int64_t neq, int* iterations);
+/* v_int(qi,qj,qk,ql,hw) with q = (n, ml, ms) (src/ME_general.f90:2205)       */
+double qd_v_int(const int* qi, const int* qj, const int* qk, const int* ql, double hw);
 
 /* ---- BCH / Magnus (src/magnus_IMSRG.f90) ----------------------------------- */
 /* BCH_EXPAND :253-318: HS = sum_k ad_G^k(H) cof(k) with the reference's

@@ -406,6 +406,15 @@ double mat_2_norm(Op& r) {
   return std::sqrt(od);
 }
 
+// The norm mat_2_norm's name intends: every stored one- and two-body entry
+// (E0 excluded).  Used only when a caller asks for it (flag 2 of the BCH and
+// flow drivers); the reference's own mat_2_norm is the one-body-only one.
+double mat_2_norm_full(Op& r) {
+  double od = 0.0;
+  for (i64 i = 1; i < r.L->neq; ++i) od += r.v[i] * r.v[i];
+  return std::sqrt(od);
+}
+
 // ---------------------------------------------------------------------------
 // Commutators
 // ---------------------------------------------------------------------------
@@ -1041,9 +1050,14 @@ struct Sampler {
 };
 
 // BCH_EXPAND, magnus_IMSRG.f90:253-318.  Returns the number of commutators.
-// pandya: 0 = as run_magnus (cross-coupled X never filled, Q1),
-//         1 = calc_cc on G and AD before every commutator_222.
-int BCH_EXPAND(Op& HS, Op& G, Op& H, Op& INT1, Op& INT2, Op& AD, Op& w1, Op& w2, CC& HCC, CC& OCC, int pandya) {
+// flags bit 0: calc_cc on G and AD before every commutator_222 (run_magnus
+//              never fills the cross-coupled X, so without it the ph channel
+//              is absent, as in the reference);
+// flags bit 1: truncation test with the one- plus two-body norm instead of
+//              the reference's one-body mat_2_norm.
+int BCH_EXPAND(Op& HS, Op& G, Op& H, Op& INT1, Op& INT2, Op& AD, Op& w1, Op& w2, CC& HCC, CC& OCC, int flags) {
+  const int pandya = flags & 1;
+  double (*nrm)(Op&) = (flags & 2) ? mat_2_norm_full : mat_2_norm;
   const double conv = 1e-5;
   const double cof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666, 0.0083333333333333333,
                           .001388888888888, 1.984126984e-4, 2.48015873e-5, 2.755731922e-6, 2.755731922e-7,
@@ -1079,7 +1093,7 @@ int BCH_EXPAND(Op& HS, Op& G, Op& H, Op& INT1, Op& INT2, Op& AD, Op& w1, Op& w2,
     commutator_222(G, AD, INT2, w1, HCC, OCC);
     ++count;
     add_arrays(INT1, 1.0, INT2, cof[i - 2], HS);
-    if (mat_2_norm(INT2) * cof[i - 2] / mat_2_norm(INT1) < convd) break;
+    if (nrm(INT2) * cof[i - 2] / nrm(INT1) < convd) break;
   }
   return count;
 }
@@ -1257,26 +1271,29 @@ void orc_add_arrays(void* r1, double s1, void* r2, double s2, void* r3) {
 void orc_copy_arrays(void* r1, void* r2) { copy_arrays(*(Op*)r1, *(Op*)r2); }
 void orc_set_to_zero(void* r1) { set_to_zero(*(Op*)r1); }
 double orc_mat_2_norm(void* r) { return mat_2_norm(*(Op*)r); }
+double orc_mat_2_norm_full(void* r) { return mat_2_norm_full(*(Op*)r); }
 double orc_mbpt2(void* r) { return MBPT2(*(Op*)r); }
 double orc_hf_e2(void* r) { return HF_E2(*(Op*)r); }
 
-int orc_bch_expand(void* HS, void* G, void* H, int pandya) {
+int orc_bch_expand(void* HS, void* G, void* H, int flags) {
   Op& h = *(Op*)H;
   const Layout* L = h.L;
   Op INT1(L, 1), INT2(L, 1), AD(L, 1), w1(L, 1), w2(L, 1);
   CC hcc(L), occ(L);
   hcc.herm = 1.0;
   occ.herm = -1.0;
-  return BCH_EXPAND(*(Op*)HS, *(Op*)G, h, INT1, INT2, AD, w1, w2, hcc, occ, pandya);
+  return BCH_EXPAND(*(Op*)HS, *(Op*)G, h, INT1, INT2, AD, w1, w2, hcc, occ, flags);
 }
 
 // s_evolve with build_white, magnus_IMSRG.f90:194-248 (TDA/spectrum
 // diagnostics omitted; they do not feed back into the flow).  HAM is the
 // normal-ordered HF Hamiltonian (herm=+1), HS receives the evolved one.
+// flags as BCH_EXPAND (bit 1 also switches the eta-norm of the step
+// rejection to the one- plus two-body norm).
 // trace: per accepted-or-rejected iteration, 7 doubles:
 //   iteration, s, E0, nrm1, nrm2, crit, bch_terms (negative when rejected)
 // Returns the number of trace rows written, or -1 if max_iter was reached.
-int orc_magnus_flow(void* HAMp, void* HSp, int pandya, int max_iter, double* trace, double* s_out) {
+int orc_magnus_flow(void* HAMp, void* HSp, int flags, int max_iter, double* trace, double* s_out) {
   const double conv_criteria = (double)1e-9f;  // Fortran real(4) literal 1e-9
   Op& HAM = *(Op*)HAMp;
   Op& HS = *(Op*)HSp;
@@ -1289,8 +1306,9 @@ int orc_magnus_flow(void* HAMp, void* HSp, int pandya, int max_iter, double* tra
   double s = 0.0, stp = (double)0.7f;  // "stp=.7" is a real(4) literal
   copy_arrays(HAM, HS);
   HS.herm = 1;
+  double (*nrm)(Op&) = (flags & 2) ? mat_2_norm_full : mat_2_norm;
   build_white(ETA, HS);
-  double nrm1 = mat_2_norm(ETA);
+  double nrm1 = nrm(ETA);
   double crit = std::fabs(MBPT2(HAM));
   int iteration = 0, rows = 0, loops = 0;
   while (crit > conv_criteria) {
@@ -1300,10 +1318,10 @@ int orc_magnus_flow(void* HAMp, void* HSp, int pandya, int max_iter, double* tra
     add_arrays(G, 1.0, DG, stp, G);
     s = s + stp;
     copy_arrays(HS, HS0);
-    int terms = BCH_EXPAND(HS, G, HAM, INT1, INT2, AD, w1, w2, HCC, OCC, pandya);
+    int terms = BCH_EXPAND(HS, G, HAM, INT1, INT2, AD, w1, w2, HCC, OCC, flags);
     copy_arrays(ETA, ETA0);
     build_white(ETA, HS);
-    double nrm2 = mat_2_norm(ETA);
+    double nrm2 = nrm(ETA);
     double* t = trace + 7 * rows;
     t[0] = iteration; t[1] = s; t[2] = HS.E0(); t[3] = nrm1; t[4] = nrm2; t[5] = crit; t[6] = terms;
     ++rows;

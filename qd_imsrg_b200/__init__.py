@@ -24,14 +24,14 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import QD_PANDYA, FlowResult, QDError, check, lib
+from ._native import QD_FULL_NORM, QD_PANDYA, FlowResult, QDError, check, lib
 
 __all__ = [
-    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA",
+    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA", "QD_FULL_NORM",
     "commutator_110", "commutator_220", "commutator_111", "commutator_121", "commutator_221",
     "commutator_122", "commutator_222", "commutator", "calc_cc", "build_white", "add_arrays",
     "copy_arrays", "set_to_zero", "mat_2_norm", "mbpt2", "hf_e2", "bch_expand", "magnus_expand",
-    "euler_step", "magnus_flow", "random_operator",
+    "euler_step", "magnus_flow", "random_operator", "tbme_write", "hf_hamiltonian", "v_int",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -280,10 +280,15 @@ def hf_e2(r) -> float:
     return _scalar(lib().qd_hf_e2, r.h)
 
 
-def bch_expand(HS, G, H, INT1, INT2, AD, w1, w2, HCC: CCMat, OCC: CCMat, pandya: bool = False) -> int:
+def _flags(pandya: bool, full_norm: bool) -> int:
+    return (QD_PANDYA if pandya else 0) | (QD_FULL_NORM if full_norm else 0)
+
+
+def bch_expand(HS, G, H, INT1, INT2, AD, w1, w2, HCC: CCMat, OCC: CCMat, pandya: bool = False,
+               full_norm: bool = False) -> int:
     n = C.c_int()
     check(lib().qd_bch_expand(HS.h, G.h, H.h, INT1.h, INT2.h, AD.h, w1.h, w2.h, HCC.h, OCC.h,
-                              QD_PANDYA if pandya else 0, C.byref(n)))
+                              _flags(pandya, full_norm), C.byref(n)))
     return n.value
 
 
@@ -297,9 +302,41 @@ def euler_step(G, DG, s: float, stp: float) -> float:
     return sv.value
 
 
-def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int = 500):
-    """s_evolve(build_white): returns (trace[rows,7], FlowResult)."""
+def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int = 500, full_norm: bool = False):
+    """s_evolve(build_white): returns (trace[rows,7], FlowResult).  pandya adds
+    the particle-hole channel (absent in run_magnus); full_norm uses the one-
+    plus two-body norm in the BCH truncation and the step rejection."""
     trace = np.zeros((max_iter, 7), np.float64)
     res = FlowResult()
-    check(lib().qd_magnus_flow(HAM.h, HS.h, QD_PANDYA if pandya else 0, int(max_iter), _d(trace), C.byref(res)))
+    check(lib().qd_magnus_flow(HAM.h, HS.h, _flags(pandya, full_norm), int(max_iter), _d(trace), C.byref(res)))
     return trace[: res.rows], res
+
+
+# ---- host-side inputs (the reference's HFQDmod / generate_ME) ----------------
+def tbme_write(emax: int, path: str, nthreads: int = 0) -> None:
+    """Write ME.bin (the reference's Coulomb TBME stream file) for emax shells."""
+    import os
+
+    check(lib().qd_tbme_write(int(emax), path.encode(), int(nthreads or (os.cpu_count() or 1))))
+
+
+def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, nthreads: int = 0):
+    """Hartree-Fock for N electrons in emax shells at hbar-omega = hw: returns
+    (vec, eig, iterations): the normal-ordered HF Hamiltonian in vectorize
+    order (vec[0] = E_HF) and the HF single-particle energies (states order),
+    ready for Layout(nbody, emax, eig) and FullHam(..., vec)."""
+    import os
+
+    L = Layout(nbody, emax, device=HOST_ONLY)
+    eig = np.zeros(emax * (emax + 1), np.float64)
+    vec = np.zeros(L.neq, np.float64)
+    it = C.c_int()
+    check(lib().qd_hf_hamiltonian(int(nbody), int(emax), float(hw), mebin.encode() if mebin else None,
+                                  int(nthreads or (os.cpu_count() or 1)), _d(eig), _d(vec), L.neq, C.byref(it)))
+    return vec, eig, it.value
+
+
+def v_int(qi, qj, qk, ql, hw: float = 1.0) -> float:
+    """Coulomb matrix element v_int of the reference, q = (n, ml, ms)."""
+    arrs = [(C.c_int * 3)(*[int(x) for x in q]) for q in (qi, qj, qk, ql)]
+    return float(lib().qd_v_int(*arrs, float(hw)))

@@ -17,8 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqdimsrg.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2,-fopenmp",
          "-Xptxas", "-warn-spills"]
+LIBS = ["-lquadmath", "-lgomp"]
 
 
 def sources():
@@ -50,7 +51,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [nvcc()] + ARCH + FLAGS
     if os.path.exists("/usr/bin/g++"):
         cmd += ["-ccbin", "/usr/bin/g++"]
-    cmd += ["-I", os.path.join(ROOT, "include"), "-shared", "-o", LIB + ".tmp"] + sources()
+    cmd += ["-I", os.path.join(ROOT, "include"), "-shared", "-o", LIB + ".tmp"] + sources() + LIBS
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.check_call(cmd)

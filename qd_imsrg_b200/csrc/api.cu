@@ -704,6 +704,7 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   TRY(use_device(L));
   TRY(build_programs(L));
   const bool pandya = (flags & QD_PANDYA) != 0;
+  auto norm = (flags & QD_FULL_NORM) ? reduce_norm_full : reduce_norm1b;
   CHECK(!pandya || (HCC && OCC), QD_ERR_ARG, "qd_bch_expand: QD_PANDYA needs HCC and OCC");
   const double conv = (double)1e-5f;  // "conv = 1e-5" is a real(4) literal in the reference
   INT2->herm = 1;
@@ -714,14 +715,14 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   for (int i = 2; i <= 12; ++i) {
     std::swap(INT2->d, AD->d);  // AD = previous term; INT2 becomes the output buffer
     std::swap(INT2->zero_mask, AD->zero_mask);
-    TRY(reduce_norm1b(L, HS->d, red_slot(L, 1)));  // |INT1| = |HS| before the update
+    TRY(norm(L, HS->d, red_slot(L, 1)));  // |INT1| = |HS| before the update
     if (pandya) {
       TRY(commutator_seq(L, G, AD, INT2, w1, w2, OCC, HCC, true));
     } else {
       TRY(commutator_seq(L, G, AD, INT2, w1, w2, nullptr, nullptr, false));
     }
     ++count;
-    TRY(reduce_norm1b(L, INT2->d, red_slot(L, 2)));
+    TRY(norm(L, INT2->d, red_slot(L, 2)));
     const double cof = kCof[i - 2];
     TRY(launch_axpy(L, HS->d, 1.0, INT2->d, cof, HS->d, L->neq));
     HS->zero_mask &= INT2->zero_mask;
@@ -788,9 +789,14 @@ int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, do
   double s = 0.0, stp = (double)0.7f;  // "stp=.7" is a real(4) literal
   FLOW(qd_copy_arrays(HAM, HS));
   HS->herm = 1;
+  auto eta_norm = [&](const qd_op* op, double* out) -> int {
+    if (!(flags & QD_FULL_NORM)) return qd_mat_2_norm(op, out);
+    TRY(reduce_norm_full(L, op->d, red_slot(L, 0)));
+    return scalar_out(L, red_slot(L, 0), out);
+  };
   FLOW(qd_build_white(ETA, HS));
   double nrm1, crit;
-  FLOW(qd_mat_2_norm(ETA, &nrm1));
+  FLOW(eta_norm(ETA, &nrm1));
   FLOW(qd_mbpt2(HAM, &crit));
   crit = std::fabs(crit);
   int iteration = 0, rows = 0, loops = 0, rejected = 0, comms = 0;
@@ -817,7 +823,7 @@ int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, do
     FLOW(qd_copy_arrays(ETA, ETA0));
     FLOW(qd_build_white(ETA, HS));
     double nrm2;
-    FLOW(qd_mat_2_norm(ETA, &nrm2));
+    FLOW(eta_norm(ETA, &nrm2));
     double E0;
     QD_CUDA(cudaMemcpyAsync(L->h_red + 8, HS->d, sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     QD_CUDA(cudaStreamSynchronize(L->stream));

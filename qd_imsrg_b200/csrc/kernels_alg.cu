@@ -181,6 +181,16 @@ int reduce_mbpt2(qd_layout* L, const double* h, double* dout) {
 int reduce_hhtrace(qd_layout* L, const double* h, double* dout) {
   return reduce_to(L, RedHHTrace{L->dev, h}, L->dev.pcnt[0], 1.0, 0.0, dout);
 }
+// one- plus two-body norm (every stored entry but E0), sqrt on the device
+int reduce_norm_full(qd_layout* L, const double* a, double* dout) {
+  int rc = reduce_to(L, RedDotRange{a, nullptr, L->o_fhh}, L->neq - L->o_fhh, 1.0, 0.0, dout);
+  if (rc) return rc;
+  k_sqrt<<<1, 1, 0, L->stream>>>(dout);
+  ++L->nlaunch;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
 // mat_2_norm: one-body parts only, sqrt taken on the device
 int reduce_norm1b(qd_layout* L, const double* a, double* dout) {
   i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;

@@ -195,6 +195,7 @@ int reduce_dot_part(qd_layout* L, const double* a, const double* b, int part, do
 int reduce_mbpt2(qd_layout* L, const double* h, double* dout);
 int reduce_hhtrace(qd_layout* L, const double* h, double* dout);
 int reduce_norm1b(qd_layout* L, const double* a, double* dout);
+int reduce_norm_full(qd_layout* L, const double* a, double* dout);
 double* red_slot(qd_layout* L, int k);
 int launch_white(qd_layout* L, double* gen, const double* h, int herm);
 int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
