@@ -195,9 +195,11 @@ int qd_tbme_write(int emax, const char* path, int nthreads);
 /* construct_two_particle_HF_BASIS + HF_E2: HF single-particle energies (eig,
  * m = emax*(emax+1), states order) and the normal-ordered HF Hamiltonian in
  * vectorize order (vec, neq entries; E0 = E_HF).  mebin: ME.bin path, or NULL
- * to compute the TBMEs in memory.  *iterations: HF iterations.              */
-int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double* eig, double* vec,
-                      int64_t neq, int* iterations);
+ * to compute the TBMEs in memory.  mix: fraction of the new density per
+ * iteration (1 = the reference's plain iteration, which oscillates for e.g.
+ * N=20 at hbar-omega=0.5; 0.5 damps it).  *iterations: HF iterations.      */
+int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double mix, double* eig,
+                      double* vec, int64_t neq, int* iterations);
 /* v_int(qi,qj,qk,ql,hw) with q = (n, ml, ms) (src/ME_general.f90:2205)       */
 double qd_v_int(const int* qi, const int* qj, const int* qk, const int* ql, double hw);
 

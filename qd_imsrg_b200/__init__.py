@@ -320,11 +320,12 @@ def tbme_write(emax: int, path: str, nthreads: int = 0) -> None:
     check(lib().qd_tbme_write(int(emax), path.encode(), int(nthreads or (os.cpu_count() or 1))))
 
 
-def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, nthreads: int = 0):
+def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, nthreads: int = 0, mix: float = 1.0):
     """Hartree-Fock for N electrons in emax shells at hbar-omega = hw: returns
     (vec, eig, iterations): the normal-ordered HF Hamiltonian in vectorize
     order (vec[0] = E_HF) and the HF single-particle energies (states order),
-    ready for Layout(nbody, emax, eig) and FullHam(..., vec)."""
+    ready for Layout(nbody, emax, eig) and FullHam(..., vec).  mix < 1 damps
+    the density update (1 = the reference's plain iteration)."""
     import os
 
     L = Layout(nbody, emax, device=HOST_ONLY)
@@ -332,7 +333,8 @@ def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, n
     vec = np.zeros(L.neq, np.float64)
     it = C.c_int()
     check(lib().qd_hf_hamiltonian(int(nbody), int(emax), float(hw), mebin.encode() if mebin else None,
-                                  int(nthreads or (os.cpu_count() or 1)), _d(eig), _d(vec), L.neq, C.byref(it)))
+                                  int(nthreads or (os.cpu_count() or 1)), float(mix), _d(eig), _d(vec), L.neq,
+                                  C.byref(it)))
     return vec, eig, it.value
 
 

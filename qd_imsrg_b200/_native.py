@@ -93,7 +93,8 @@ SIGNATURES = {
     "qd_euler_step": (C.c_int, [_vp, _vp, _dp, C.c_double]),
     "qd_magnus_flow": (C.c_int, [_vp, _vp, C.c_uint, C.c_int, _dp, C.POINTER(FlowResult)]),
     "qd_tbme_write": (C.c_int, [C.c_int, C.c_char_p, C.c_int]),
-    "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, _dp, _dp, _i64, _ip]),
+    "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, C.c_double, _dp, _dp, _i64,
+                                    _ip]),
     "qd_v_int": (C.c_double, [_ip, _ip, _ip, _ip, C.c_double]),
 }
 

@@ -25,7 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <unordered_map>
+#include <tuple>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -66,17 +66,26 @@ double gamma_hi(double x) {
 }
 
 struct VintCache {
-  std::unordered_map<unsigned long long, double> sm_int;
-  std::vector<q128> binc;  // bin_coef(n,k) at n*(BMAX+1)+k
-  std::vector<double> gam; // gamma(k/2) for k = 1..
+  std::vector<double> memo;  // sm_int by (gs1,gs2,gs3,gs4), NaN = not yet computed
+  int gsd = 0;               // gs values < gsd
+  std::vector<q128> binc;    // bin_coef(n,k) at n*(bmax+1)+k
+  std::vector<q128> fact;    // fac(n) = ((1*1)*2)*...*n, as fac() computes it
+  std::vector<double> gam;   // gamma(k/2), k >= 1
+  std::vector<double> half;  // 0.5d0**((G+1)*0.5), by G
   int bmax = 0;
   void build(int nb, int ng) {
     bmax = nb;
     binc.assign((size_t)(nb + 1) * (nb + 1), 0);
     for (int n = 0; n <= nb; ++n)
       for (int k = 0; k <= n; ++k) binc[(size_t)n * (nb + 1) + k] = bin_coef(n, k);
+    fact.assign(nb + 1, 0);
+    for (int n = 0; n <= nb; ++n) fact[n] = qfac(n);
     gam.assign(ng + 1, 0.0);
     for (int k = 1; k <= ng; ++k) gam[k] = gamma_hi(0.5 * k);
+    half.assign(ng + 1, 0.0);
+    for (int G = 0; G <= ng; ++G) half[G] = std::pow(0.5, ((double)G + 1.0) * 0.5);
+    gsd = nb / 2;
+    memo.assign((size_t)gsd * gsd * gsd * gsd, std::nan(""));
   }
   q128 bc(int n, int k) const { return binc[(size_t)n * (bmax + 1) + k]; }
   double g2(double x) const { return gam[(int)std::lround(2 * x)]; }  // gamma(x), x half-integer
@@ -96,12 +105,10 @@ double v_int(const int* qi, const int* qj, const int* qk, const int* ql, double 
           gs[1] = j2 + j3 + (std::abs(qj[1]) + qj[1]) / 2 + (std::abs(qk[1]) - qk[1]) / 2;
           gs[2] = j2 + j3 + (std::abs(qj[1]) - qj[1]) / 2 + (std::abs(qk[1]) + qk[1]) / 2;
           const double G = (double)(gs[0] + gs[1] + gs[2] + gs[3]);
-          const unsigned long long key = (unsigned long long)gs[0] | ((unsigned long long)gs[1] << 16) |
-                                         ((unsigned long long)gs[2] << 32) | ((unsigned long long)gs[3] << 48);
+          double& slot = C.memo[(((size_t)gs[0] * C.gsd + gs[1]) * C.gsd + gs[2]) * C.gsd + gs[3]];
           double sm_int;
-          auto it = C.sm_int.find(key);
-          if (it != C.sm_int.end()) {
-            sm_int = it->second;
+          if (!std::isnan(slot)) {
+            sm_int = slot;
           } else {
             sm_int = 0.0;
             for (int l1 = 0; l1 <= gs[0]; ++l1)
@@ -119,19 +126,19 @@ double v_int(const int* qi, const int* qj, const int* qk, const int* ql, double 
                   t = t * (q128)C.g2((G - LAM + 1.0) * 0.5);
                   sm_int = (double)((q128)sm_int + t);
                 }
-            C.sm_int.emplace(key, sm_int);
+            slot = sm_int;
           }
           const int s4 = ((j1 + j2 + j3 + j4) & 1) ? -1 : 1;
-          q128 den = qfac(j1);
-          den = den * qfac(j2);
-          den = den * qfac(j3);
-          den = den * qfac(j4);
+          q128 den = C.fact[j1];
+          den = den * C.fact[j2];
+          den = den * C.fact[j3];
+          den = den * C.fact[j4];
           q128 t = (q128)s4 / den;
           t = t * C.bc(qi[0] + std::abs(qi[1]), qi[0] - j1);
           t = t * C.bc(qj[0] + std::abs(qj[1]), qj[0] - j2);
           t = t * C.bc(qk[0] + std::abs(qk[1]), qk[0] - j3);
           t = t * C.bc(ql[0] + std::abs(ql[1]), ql[0] - j4);
-          t = t * (q128)std::pow(0.5, (G + 1.0) * 0.5);
+          t = t * (q128)C.half[(int)G];
           t = t * (q128)sm_int;
           sm = (double)((q128)sm + t);
         }
@@ -203,19 +210,29 @@ static int build_tbme(int emax, TBME& T, int nthreads) {
     for (int p = 0; p < (int)P.size(); ++p)
       for (int r = 0; r < (int)P.size(); ++r) {
         const int a = P[p].first, b = P[p].second, c = P[r].first, d = P[r].second;
-        // one representative per orbit {(p,r), (r,p), (ba,dc), (dc,ba)}: the
-        // lexicographically smallest, so every entry is written exactly once
+        // one representative per orbit of 8: {(p,r), (r,p), (ba,dc), (dc,ba)}
+        // and the same with every m_l negated (time reversal), the smallest
+        // (block, p, r) triple; every entry is then written exactly once
         const int pba = T.pair_idx[(size_t)b * N + a], pdc = T.pair_idx[(size_t)d * N + c];
-        const std::pair<int, int> me(p, r);
-        if (std::pair<int, int>(r, p) < me || std::pair<int, int>(pba, pdc) < me ||
-            std::pair<int, int>(pdc, pba) < me)
-          continue;
+        const int ta = S.index(S.n[a], -S.ml[a]), tb = S.index(S.n[b], -S.ml[b]);
+        const int tc = S.index(S.n[c], -S.ml[c]), td = S.index(S.n[d], -S.ml[d]);
+        const int Mt = T.pair_block[(size_t)ta * N + tb];
+        const int tab = T.pair_idx[(size_t)ta * N + tb], tcd = T.pair_idx[(size_t)tc * N + td];
+        const int tba = T.pair_idx[(size_t)tb * N + ta], tdc = T.pair_idx[(size_t)td * N + tc];
+        typedef std::tuple<int, int, int> K;
+        const K me((int)M, p, r);
+        const K orbit[7] = {K((int)M, r, p), K((int)M, pba, pdc), K((int)M, pdc, pba), K(Mt, tab, tcd),
+                            K(Mt, tcd, tab), K(Mt, tba, tdc), K(Mt, tdc, tba)};
+        bool canon = true;
+        for (const K& k : orbit) canon = canon && !(k < me);
+        if (!canon) continue;
         work.push_back({(int)M, p, r});
       }
   }
   int maxn = 0;
   for (int i = 0; i < N; ++i) maxn = std::max(maxn, S.n[i] + std::abs(S.ml[i]));
-  const int nb = 4 * (2 * emax + 4), ng = 4 * (4 * emax + 8);
+  // bin_coef arguments stay below ~3*emax, gs values below ~2*emax
+  const int nb = 4 * emax + 16, ng = 8 * emax + 32;
 #pragma omp parallel num_threads(nthreads)
   {
     VintCache C;
@@ -229,13 +246,25 @@ static int build_tbme(int emax, TBME& T, int nthreads) {
       int qc[3] = {S.n[c], S.ml[c], -1}, qd_[3] = {S.n[d], S.ml[d], -1};
       // <ab|V|cd>_direct = v_int(a,b,d,c) (get_ints, ME_general.f90:776-779)
       const double v = v_int(qa, qb, qd_, qc, 1.0, C);
-      const size_t n = P.size();
       const int pba = T.pair_idx[(size_t)b * N + a], pdc = T.pair_idx[(size_t)d * N + c];
+      const size_t n = P.size();
       double* D = T.D[q.M].data();
       D[(size_t)q.p * n + q.r] = v;
       D[(size_t)q.r * n + q.p] = v;
       D[(size_t)pba * n + pdc] = v;
       D[(size_t)pdc * n + pba] = v;
+      // time-reversed partners (all m_l negated), block -M
+      const int ta = S.index(S.n[a], -S.ml[a]), tb = S.index(S.n[b], -S.ml[b]);
+      const int tc = S.index(S.n[c], -S.ml[c]), td = S.index(S.n[d], -S.ml[d]);
+      const int Mt = T.pair_block[(size_t)ta * N + tb];
+      const size_t nt = T.pairs[Mt].size();
+      double* Dt = T.D[Mt].data();
+      const int tab = T.pair_idx[(size_t)ta * N + tb], tcd = T.pair_idx[(size_t)tc * N + td];
+      const int tba = T.pair_idx[(size_t)tb * N + ta], tdc = T.pair_idx[(size_t)td * N + tc];
+      Dt[(size_t)tab * nt + tcd] = v;
+      Dt[(size_t)tcd * nt + tab] = v;
+      Dt[(size_t)tba * nt + tdc] = v;
+      Dt[(size_t)tdc * nt + tba] = v;
     }
   }
   (void)maxn;
@@ -375,7 +404,10 @@ struct HFResult {
 };
 
 // HF iteration (HFQDmod.f90:186-237) on spin-orbitals in states order.
-static int run_hf(int nbody, int emax, double hw, const TBME& T, HFResult& R, int nthreads) {
+// mix: fraction of the new density taken each iteration (1 = the reference's
+// plain Roothaan iteration; below 1 damps the oscillation that large dots at
+// small hbar-omega show).
+static int run_hf(int nbody, int emax, double hw, const TBME& T, HFResult& R, int nthreads, double mix) {
   const int m = emax * (emax + 1);
   Spatial S(emax);
   std::vector<int> sn(m), sml(m), sms(m);
@@ -415,6 +447,7 @@ static int run_hf(int nbody, int emax, double hw, const TBME& T, HFResult& R, in
     }
   }
   std::vector<double> C((size_t)m * m, 0.0), eig(m, 0.0), eold(m, 0.0), den((size_t)m * m), Fm((size_t)m * m);
+  std::vector<double> den_old;
   for (int i = 0; i < m; ++i) C[(size_t)i * m + i] = 1.0;  // column-major: C[row + col*m]
   double crit = 1.0;
   int it = 0;
@@ -428,6 +461,9 @@ static int run_hf(int nbody, int emax, double hw, const TBME& T, HFResult& R, in
     for (int k = 0; k < nbody; ++k)
       for (int j = 0; j < m; ++j)
         for (int i = 0; i < m; ++i) den[(size_t)i + (size_t)j * m] += C[(size_t)i + (size_t)k * m] * C[(size_t)j + (size_t)k * m];
+    if (mix < 1.0 && !den_old.empty())
+      for (size_t e = 0; e < den.size(); ++e) den[e] = mix * den[e] + (1.0 - mix) * den_old[e];
+    den_old = den;
     // V(i,k) = sum_{j,l} den(l,j) <j i|V|l k>_AS  (construct_V, HFQDmod.f90:260-290)
 #pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
     for (int k = 0; k < m; ++k)
@@ -605,9 +641,9 @@ extern "C" int qd_tbme_write(int emax, const char* path, int nthreads) {
   return write_mebin(T, path);
 }
 
-extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double* eig_out,
-                                 double* vec_out, int64_t neq, int* iterations) {
-  if (nbody < 0 || emax < 1 || !eig_out || !vec_out) {
+extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double mix,
+                                 double* eig_out, double* vec_out, int64_t neq, int* iterations) {
+  if (nbody < 0 || emax < 1 || !eig_out || !vec_out || !(mix > 0.0 && mix <= 1.0)) {
     set_error("qd_hf_hamiltonian: bad arguments");
     return QD_ERR_ARG;
   }
@@ -616,7 +652,7 @@ extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* meb
   int rc = mebin ? read_mebin(mebin, emax, T) : build_tbme(emax, T, nt);
   if (rc) return rc;
   HFResult R;
-  if ((rc = run_hf(nbody, emax, hw, T, R, nt))) return rc;
+  if ((rc = run_hf(nbody, emax, hw, T, R, nt, mix))) return rc;
   qd_layout L;
   if ((rc = layout_build(&L, nbody, emax, R.eig.data()))) return rc;
   if (neq != L.neq) {
@@ -633,6 +669,8 @@ extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* meb
 
 extern "C" double qd_v_int(const int* qi, const int* qj, const int* qk, const int* ql, double hw) {
   VintCache C;
-  C.build(200, 400);
+  int big = 0;
+  for (const int* q : {qi, qj, qk, ql}) big = std::max(big, q[0] + std::abs(q[1]));
+  C.build(4 * big + 16, 8 * big + 32);
   return v_int(qi, qj, qk, ql, hw, C);
 }
