@@ -28,9 +28,11 @@ def part_slices(layout):
     return out
 
 
-def compare_parts(layout, got, ref, rtol=1e-12, atol_floor=1e-300):
+def compare_parts(layout, got, ref, rtol=1e-12, atol_floor=1e-300, atol=None):
     """Relative Frobenius error per part; returns {name: (rel, maxabs)} and
-    raises AssertionError listing parts above rtol."""
+    raises AssertionError listing parts above rtol.  With atol, a part whose
+    max |diff| is at most atol also passes (for parts that are analytically
+    zero and hold only rounding noise)."""
     res, bad = {}, []
     for name, ix in part_slices(layout):
         if ix.size == 0:
@@ -43,7 +45,7 @@ def compare_parts(layout, got, ref, rtol=1e-12, atol_floor=1e-300):
         if nr == 0.0:
             if mx > 1e-13:
                 bad.append("%s: ref is zero, max|diff|=%.3e" % (name, mx))
-        elif rel > rtol:
+        elif rel > rtol and not (atol is not None and mx <= atol):
             bad.append("%s: rel %.3e max %.3e" % (name, rel, mx))
     assert not bad, "; ".join(bad)
     return res
