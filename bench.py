@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--hw", type=float, default=0.5)
     ap.add_argument("--pandya", action="store_true", help="flow: add the particle-hole channel")
     ap.add_argument("--hf-mix", type=float, default=0.5, help="flow: HF density mixing (1 = plain iteration)")
+    ap.add_argument("--tbme", choices=["quad", "reference"], default="quad",
+                    help="flow: v_int in __float128 (quad) or in the reference's real(8) sums")
     return ap.parse_args()
 
 
@@ -315,7 +317,7 @@ def run_flow(args, world, rank, local):
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     t0 = time.perf_counter()
-    vec, eig, hf_it = qd.hf_hamiltonian(args.nbody, args.emax, args.hw, mix=args.hf_mix)
+    vec, eig, hf_it = qd.hf_hamiltonian(args.nbody, args.emax, args.hw, mix=args.hf_mix, quad=args.tbme == "quad")
     setup_s = time.perf_counter() - t0
     P = qd.Layout(args.nbody, args.emax, eig=eig, device=local)
     stream = torch.cuda.Stream(device=device)
@@ -372,6 +374,7 @@ def run_flow(args, world, rank, local):
                            "E_HF": float(vec[0]), "E_gs": float(res.E0), "flow_steps": int(res.iterations),
                            "rejected": int(res.rejected), "commutators": comms, "s_final": float(res.s),
                            "hf_setup_s": setup_s, "hf_iterations": hf_it, "hf_mix": args.hf_mix,
+                           "tbme": args.tbme,
                            "bch_terms": [int(x) for x in tr[:, 6]]},
                 "e2e": {"value": e2e_sec, "unit": "s per converged E_gs", "h2d_bytes_per_step": 8 * P.neq,
                         "d2h_bytes_per_step": 8 * P.neq},

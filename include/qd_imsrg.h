@@ -187,21 +187,30 @@ int qd_hf_e2(qd_op* H, double* out);
 /* ---- host-side inputs: Coulomb TBMEs and Hartree-Fock -----------------------
  * The reference computes these on the host (generate_ME.f90, get_TBME.f90,
  * src/HFQDmod.f90:9-254); they are the flow's input, not its hot path.       */
+/* TBME options.  QD_TBME_QUAD: evaluate v_int with every sum and factor in
+ * __float128.  The reference's arithmetic sums terms of up to ~1e21 in
+ * real(8) and loses every digit from radial quantum number n ~ 7 on
+ * (emax >= 15), so emax = 20 inputs need this option; without it v_int is
+ * the reference's, rounding included.                                       */
+#define QD_TBME_QUAD 1u
 /* Write ME.bin (records int32 n1,m1,n2,m2,n3,m3,n4,m4 + float64 Vdir at
  * hbar-omega = 1, the stream read at src/HFQDmod.f90:97-127) for every
  * m-conserving quadruple of spatial orbitals below emax shells, from v_int
- * (src/ME_general.f90:2205-2276, real(16) arithmetic kept).  nthreads <= 0: 1.  */
-int qd_tbme_write(int emax, const char* path, int nthreads);
+ * (src/ME_general.f90:2205-2276).  nthreads <= 0: 1.  options: QD_TBME_QUAD. */
+int qd_tbme_write(int emax, const char* path, int nthreads, unsigned options);
 /* construct_two_particle_HF_BASIS + HF_E2: HF single-particle energies (eig,
  * m = emax*(emax+1), states order) and the normal-ordered HF Hamiltonian in
  * vectorize order (vec, neq entries; E0 = E_HF).  mebin: ME.bin path, or NULL
- * to compute the TBMEs in memory.  mix: fraction of the new density per
- * iteration (1 = the reference's plain iteration, which oscillates for e.g.
- * N=20 at hbar-omega=0.5; 0.5 damps it).  *iterations: HF iterations.      */
-int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double mix, double* eig,
-                      double* vec, int64_t neq, int* iterations);
-/* v_int(qi,qj,qk,ql,hw) with q = (n, ml, ms) (src/ME_general.f90:2205)       */
+ * to compute the TBMEs in memory (options: QD_TBME_QUAD).  mix: fraction of
+ * the new density per iteration (1 = the reference's plain iteration, which
+ * oscillates for e.g. N=20 at hbar-omega=0.5; 0.5 damps it).
+ * *iterations: HF iterations.                                               */
+int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double mix,
+                      unsigned options, double* eig, double* vec, int64_t neq, int* iterations);
+/* v_int(qi,qj,qk,ql,hw) with q = (n, ml, ms) (src/ME_general.f90:2205), in
+ * the reference's arithmetic; qd_v_int_quad in __float128 throughout.       */
 double qd_v_int(const int* qi, const int* qj, const int* qk, const int* ql, double hw);
+double qd_v_int_quad(const int* qi, const int* qj, const int* qk, const int* ql, double hw);
 
 /* ---- BCH / Magnus (src/magnus_IMSRG.f90) ----------------------------------- */
 /* BCH_EXPAND :253-318: HS = sum_k ad_G^k(H) cof(k) with the reference's

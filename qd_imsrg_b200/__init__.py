@@ -24,7 +24,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import QD_FULL_NORM, QD_PANDYA, FlowResult, QDError, check, lib
+from ._native import QD_FULL_NORM, QD_PANDYA, QD_TBME_QUAD, FlowResult, QDError, check, lib
 
 __all__ = [
     "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA", "QD_FULL_NORM",
@@ -313,19 +313,24 @@ def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int =
 
 
 # ---- host-side inputs (the reference's HFQDmod / generate_ME) ----------------
-def tbme_write(emax: int, path: str, nthreads: int = 0) -> None:
-    """Write ME.bin (the reference's Coulomb TBME stream file) for emax shells."""
+def tbme_write(emax: int, path: str, nthreads: int = 0, quad: bool = False) -> None:
+    """Write ME.bin (the reference's Coulomb TBME stream file) for emax shells.
+    quad: v_int in __float128 throughout (needed from emax ~ 15 on; without
+    it the reference's real(8) sums are kept)."""
     import os
 
-    check(lib().qd_tbme_write(int(emax), path.encode(), int(nthreads or (os.cpu_count() or 1))))
+    check(lib().qd_tbme_write(int(emax), path.encode(), int(nthreads or (os.cpu_count() or 1)),
+                              QD_TBME_QUAD if quad else 0))
 
 
-def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, nthreads: int = 0, mix: float = 1.0):
+def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, nthreads: int = 0, mix: float = 1.0,
+                   quad: bool = False):
     """Hartree-Fock for N electrons in emax shells at hbar-omega = hw: returns
     (vec, eig, iterations): the normal-ordered HF Hamiltonian in vectorize
     order (vec[0] = E_HF) and the HF single-particle energies (states order),
     ready for Layout(nbody, emax, eig) and FullHam(..., vec).  mix < 1 damps
-    the density update (1 = the reference's plain iteration)."""
+    the density update (1 = the reference's plain iteration); quad computes
+    the TBMEs with v_int in __float128 (see tbme_write)."""
     import os
 
     L = Layout(nbody, emax, device=HOST_ONLY)
@@ -333,12 +338,14 @@ def hf_hamiltonian(nbody: int, emax: int, hw: float, mebin: str | None = None, n
     vec = np.zeros(L.neq, np.float64)
     it = C.c_int()
     check(lib().qd_hf_hamiltonian(int(nbody), int(emax), float(hw), mebin.encode() if mebin else None,
-                                  int(nthreads or (os.cpu_count() or 1)), float(mix), _d(eig), _d(vec), L.neq,
-                                  C.byref(it)))
+                                  int(nthreads or (os.cpu_count() or 1)), float(mix),
+                                  QD_TBME_QUAD if quad else 0, _d(eig), _d(vec), L.neq, C.byref(it)))
     return vec, eig, it.value
 
 
-def v_int(qi, qj, qk, ql, hw: float = 1.0) -> float:
-    """Coulomb matrix element v_int of the reference, q = (n, ml, ms)."""
+def v_int(qi, qj, qk, ql, hw: float = 1.0, quad: bool = False) -> float:
+    """Coulomb matrix element v_int of the reference, q = (n, ml, ms); quad:
+    every sum in __float128 instead of the reference's real(8)."""
     arrs = [(C.c_int * 3)(*[int(x) for x in q]) for q in (qi, qj, qk, ql)]
-    return float(lib().qd_v_int(*arrs, float(hw)))
+    fn = lib().qd_v_int_quad if quad else lib().qd_v_int
+    return float(fn(*arrs, float(hw)))

@@ -22,6 +22,7 @@ _vpp = C.POINTER(C.c_void_p)
 QD_OK = 0
 QD_PANDYA = 1
 QD_FULL_NORM = 2
+QD_TBME_QUAD = 1
 QD_NSTAGE = 10
 STAGES = ["E0", "c111", "c121", "c221", "c122", "calc_cc", "ladder_gemm", "pandya_gemm", "pandya_gather", "glue"]
 
@@ -92,10 +93,11 @@ SIGNATURES = {
     "qd_magnus_expand": (C.c_int, [_vp, _vp, _vp]),
     "qd_euler_step": (C.c_int, [_vp, _vp, _dp, C.c_double]),
     "qd_magnus_flow": (C.c_int, [_vp, _vp, C.c_uint, C.c_int, _dp, C.POINTER(FlowResult)]),
-    "qd_tbme_write": (C.c_int, [C.c_int, C.c_char_p, C.c_int]),
-    "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, C.c_double, _dp, _dp, _i64,
-                                    _ip]),
+    "qd_tbme_write": (C.c_int, [C.c_int, C.c_char_p, C.c_int, C.c_uint]),
+    "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, C.c_double, C.c_uint,
+                                    _dp, _dp, _i64, _ip]),
     "qd_v_int": (C.c_double, [_ip, _ip, _ip, _ip, C.c_double]),
+    "qd_v_int_quad": (C.c_double, [_ip, _ip, _ip, _ip, C.c_double]),
 }
 
 _lib = None

@@ -8,6 +8,13 @@
 //              (__float128 for the real(16) factorial products; every real(8)
 //              assignment rounds).  The innermost sum depends only on the four
 //              integers gs(1..4) and is memoised per thread (exact).
+//              The two alternating sums accumulate terms of up to ~1e21 in
+//              real(8); from radial quantum numbers n ~ 7 on (emax >= 15) the
+//              cancellation leaves no correct digit (e.g. <(9,1)(9,-1)|V|
+//              (9,-1)(9,1)> = 0.2843 exactly, 1.3e5 in that arithmetic).  The
+//              QD_TBME_QUAD option keeps every sum and factor in __float128
+//              (relative error ~1e-13 up to emax = 20; a test checks it
+//              against exact rational arithmetic).
 //   ME.bin     the stream file read at src/HFQDmod.f90:97-127: records of
 //              int32 n1,m1,n2,m2,n3,m3,n4,m4 and float64 Vdir (hbar-omega = 1).
 //   HF         src/HFQDmod.f90:186-254: density of the lowest N states, mean
@@ -67,6 +74,9 @@ double gamma_hi(double x) {
 
 struct VintCache {
   std::vector<double> memo;  // sm_int by (gs1,gs2,gs3,gs4), NaN = not yet computed
+  std::vector<q128> memoq;   // the same in __float128 (QD_TBME_QUAD), NaN = not yet computed
+  std::vector<q128> gamq;    // gamma(k/2) in __float128
+  std::vector<q128> halfq;   // 0.5**((G+1)/2) in __float128
   int gsd = 0;               // gs values < gsd
   std::vector<q128> binc;    // bin_coef(n,k) at n*(bmax+1)+k
   std::vector<q128> fact;    // fac(n) = ((1*1)*2)*...*n, as fac() computes it
@@ -86,6 +96,22 @@ struct VintCache {
     for (int G = 0; G <= ng; ++G) half[G] = std::pow(0.5, ((double)G + 1.0) * 0.5);
     gsd = nb / 2;
     memo.assign((size_t)gsd * gsd * gsd * gsd, std::nan(""));
+  }
+  void build_quad(int nb, int ng) {
+    build(nb, ng);
+    memo.clear();
+    memoq.assign((size_t)gsd * gsd * gsd * gsd, nanq(""));
+    gamq.assign(ng + 1, 0);
+    for (int k = 1; k <= ng; ++k) {
+      if (k % 2 == 0) {
+        gamq[k] = qfac(k / 2 - 1);  // gamma(j) = (j-1)!
+      } else {
+        const int j = (k - 1) / 2;  // gamma(j + 1/2) = (2j)! / (4^j j!) sqrt(pi)
+        gamq[k] = fac_over_fac(2 * j, j) / powq(4, j) * sqrtq(acosq((q128)-1));
+      }
+    }
+    halfq.assign(ng + 1, 0);
+    for (int G = 0; G <= ng; ++G) halfq[G] = powq((q128)0.5, ((q128)G + 1) / 2);
   }
   q128 bc(int n, int k) const { return binc[(size_t)n * (bmax + 1) + k]; }
   double g2(double x) const { return gam[(int)std::lround(2 * x)]; }  // gamma(x), x half-integer
@@ -151,6 +177,49 @@ double v_int(const int* qi, const int* qj, const int* qk, const int* ql, double 
   return vout;
 }
 
+// v_int with every sum and factor in __float128 (QD_TBME_QUAD); the loop
+// structure is that of v_int above.
+double v_int_quad(const int* qi, const int* qj, const int* qk, const int* ql, double hw, VintCache& C) {
+  if (!(qi[2] == ql[2] && qk[2] == qj[2])) return 0.0;
+  q128 sm = 0;
+  for (int j1 = 0; j1 <= qi[0]; ++j1)
+    for (int j2 = 0; j2 <= qj[0]; ++j2)
+      for (int j3 = 0; j3 <= qk[0]; ++j3)
+        for (int j4 = 0; j4 <= ql[0]; ++j4) {
+          int gs[4];
+          gs[0] = j1 + j4 + (std::abs(qi[1]) + qi[1]) / 2 + (std::abs(ql[1]) - ql[1]) / 2;
+          gs[3] = j1 + j4 + (std::abs(qi[1]) - qi[1]) / 2 + (std::abs(ql[1]) + ql[1]) / 2;
+          gs[1] = j2 + j3 + (std::abs(qj[1]) + qj[1]) / 2 + (std::abs(qk[1]) - qk[1]) / 2;
+          gs[2] = j2 + j3 + (std::abs(qj[1]) - qj[1]) / 2 + (std::abs(qk[1]) + qk[1]) / 2;
+          const int G = gs[0] + gs[1] + gs[2] + gs[3];
+          q128& slot = C.memoq[(((size_t)gs[0] * C.gsd + gs[1]) * C.gsd + gs[2]) * C.gsd + gs[3]];
+          if (isnanq(slot)) {
+            q128 acc = 0;
+            for (int l1 = 0; l1 <= gs[0]; ++l1)
+              for (int l2 = 0; l2 <= gs[1]; ++l2)
+                for (int l3 = 0; l3 <= gs[2]; ++l3) {
+                  const int l4 = l1 + l2 - l3;
+                  if (l4 < 0 || l4 > gs[3]) continue;
+                  const int LAM = l1 + l2 + l3 + l4;
+                  const int sgn = ((gs[1] + gs[2] - l2 - l3) & 1) ? -1 : 1;
+                  q128 t = (q128)sgn * C.bc(gs[0], l1) * C.bc(gs[1], l2) * C.bc(gs[2], l3) * C.bc(gs[3], l4);
+                  acc += t * C.gamq[2 + LAM] * C.gamq[G - LAM + 1];  // gamma(1+LAM/2) gamma((G-LAM+1)/2)
+                }
+            slot = acc;
+          }
+          const int s4 = ((j1 + j2 + j3 + j4) & 1) ? -1 : 1;
+          q128 t = (q128)s4 / (C.fact[j1] * C.fact[j2] * C.fact[j3] * C.fact[j4]);
+          t = t * C.bc(qi[0] + std::abs(qi[1]), qi[0] - j1) * C.bc(qj[0] + std::abs(qj[1]), qj[0] - j2);
+          t = t * C.bc(qk[0] + std::abs(qk[1]), qk[0] - j3) * C.bc(ql[0] + std::abs(ql[1]), ql[0] - j4);
+          sm += t * C.halfq[G] * slot;
+        }
+  q128 f = fac_over_fac(qi[0], qi[0] + std::abs(qi[1]));
+  f = f * fac_over_fac(qj[0], qj[0] + std::abs(qj[1]));
+  f = f * fac_over_fac(qk[0], qk[0] + std::abs(qk[1]));
+  f = f * fac_over_fac(ql[0], ql[0] + std::abs(ql[1]));
+  return (double)(sqrtq((q128)hw) * sm * sqrtq(f));
+}
+
 // spatial orbitals in nm_index order (ME_general.f90:2140-2149)
 struct Spatial {
   int emax, N;
@@ -181,7 +250,8 @@ struct TBME {
   std::vector<std::vector<double>> D;                    // per block, row-major n_M x n_M
 };
 
-static int build_tbme(int emax, TBME& T, int nthreads) {
+static int build_tbme(int emax, TBME& T, int nthreads, unsigned options) {
+  const bool quad = (options & QD_TBME_QUAD) != 0;
   Spatial S(emax);
   const int N = S.N;
   T.emax = emax;
@@ -236,7 +306,10 @@ static int build_tbme(int emax, TBME& T, int nthreads) {
 #pragma omp parallel num_threads(nthreads)
   {
     VintCache C;
-    C.build(nb, ng);
+    if (quad)
+      C.build_quad(nb, ng);
+    else
+      C.build(nb, ng);
 #pragma omp for schedule(dynamic, 64)
     for (long long w = 0; w < (long long)work.size(); ++w) {
       const Q& q = work[w];
@@ -245,7 +318,7 @@ static int build_tbme(int emax, TBME& T, int nthreads) {
       int qa[3] = {S.n[a], S.ml[a], -1}, qb[3] = {S.n[b], S.ml[b], -1};
       int qc[3] = {S.n[c], S.ml[c], -1}, qd_[3] = {S.n[d], S.ml[d], -1};
       // <ab|V|cd>_direct = v_int(a,b,d,c) (get_ints, ME_general.f90:776-779)
-      const double v = v_int(qa, qb, qd_, qc, 1.0, C);
+      const double v = quad ? v_int_quad(qa, qb, qd_, qc, 1.0, C) : v_int(qa, qb, qd_, qc, 1.0, C);
       const int pba = T.pair_idx[(size_t)b * N + a], pdc = T.pair_idx[(size_t)d * N + c];
       const size_t n = P.size();
       double* D = T.D[q.M].data();
@@ -630,26 +703,26 @@ static int build_hamiltonian(int nbody, int emax, double hw, const TBME& T, cons
 // ---- C ABI ----------------------------------------------------------------------
 using namespace qd;
 
-extern "C" int qd_tbme_write(int emax, const char* path, int nthreads) {
-  if (emax < 1 || !path) {
+extern "C" int qd_tbme_write(int emax, const char* path, int nthreads, unsigned options) {
+  if (emax < 1 || !path || (options & ~QD_TBME_QUAD)) {
     set_error("qd_tbme_write: bad arguments");
     return QD_ERR_ARG;
   }
   TBME T;
-  int rc = build_tbme(emax, T, nthreads > 0 ? nthreads : 1);
+  int rc = build_tbme(emax, T, nthreads > 0 ? nthreads : 1, options);
   if (rc) return rc;
   return write_mebin(T, path);
 }
 
 extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double mix,
-                                 double* eig_out, double* vec_out, int64_t neq, int* iterations) {
-  if (nbody < 0 || emax < 1 || !eig_out || !vec_out || !(mix > 0.0 && mix <= 1.0)) {
+                                 unsigned options, double* eig_out, double* vec_out, int64_t neq, int* iterations) {
+  if (nbody < 0 || emax < 1 || !eig_out || !vec_out || !(mix > 0.0 && mix <= 1.0) || (options & ~QD_TBME_QUAD)) {
     set_error("qd_hf_hamiltonian: bad arguments");
     return QD_ERR_ARG;
   }
   const int nt = nthreads > 0 ? nthreads : 1;
   TBME T;
-  int rc = mebin ? read_mebin(mebin, emax, T) : build_tbme(emax, T, nt);
+  int rc = mebin ? read_mebin(mebin, emax, T) : build_tbme(emax, T, nt, options);
   if (rc) return rc;
   HFResult R;
   if ((rc = run_hf(nbody, emax, hw, T, R, nt, mix))) return rc;
@@ -673,4 +746,12 @@ extern "C" double qd_v_int(const int* qi, const int* qj, const int* qk, const in
   for (const int* q : {qi, qj, qk, ql}) big = std::max(big, q[0] + std::abs(q[1]));
   C.build(4 * big + 16, 8 * big + 32);
   return v_int(qi, qj, qk, ql, hw, C);
+}
+
+extern "C" double qd_v_int_quad(const int* qi, const int* qj, const int* qk, const int* ql, double hw) {
+  VintCache C;
+  int big = 0;
+  for (const int* q : {qi, qj, qk, ql}) big = std::max(big, q[0] + std::abs(q[1]));
+  C.build_quad(4 * big + 16, 8 * big + 32);
+  return v_int_quad(qi, qj, qk, ql, hw, C);
 }

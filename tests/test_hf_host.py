@@ -1,6 +1,7 @@
 """CPU checks of the host-side flow inputs: Coulomb TBMEs (v_int of the
-reference, real(16) arithmetic kept) and Hartree-Fock, against closed-form
-and published values for the 2-D quantum dot and against invariants."""
+reference, real(16) arithmetic kept, and its __float128 variant against an
+exact rational evaluation) and Hartree-Fock, against closed-form and
+published values for the 2-D quantum dot and against invariants."""
 import math
 import os
 
@@ -27,6 +28,39 @@ def test_v_int_symmetries():
     v3 = qd.v_int(c, d, b, a)   # <cd|ab>
     assert v1 == pytest.approx(v2, rel=1e-13) and v1 == pytest.approx(v3, rel=1e-13)
     assert abs(v1) > 1e-3
+
+
+# (n, ml, ms) quadruples: low radial quantum numbers, where the reference's
+# real(8) sums still hold ~12 digits, and high ones, where they hold none
+LOW_N = [((0, 1, 1), (0, -1, -1), (0, -1, -1), (0, 1, 1)), ((2, -4, 1), (1, 5, 1), (1, 5, 1), (2, -4, 1)),
+         ((5, 5, 1), (0, 1, 1), (0, 1, 1), (5, 5, 1))]
+MID_N = [((4, 9, 1), (2, -12, 1), (6, -4, 1), (0, 1, 1))]  # reference arithmetic: ~1e-5 relative
+HIGH_N = [((7, 3, 1), (6, -4, 1), (6, -4, 1), (7, 3, 1)), ((9, 1, 1), (9, -1, 1), (9, -1, 1), (9, 1, 1))]
+
+
+@pytest.mark.parametrize("q", LOW_N + MID_N + HIGH_N)
+def test_v_int_quad_matches_exact_rational(q):
+    from oracle.vint_exact import v_int_exact
+
+    ex = v_int_exact(*q)
+    assert qd.v_int(*q, quad=True) == pytest.approx(ex, rel=2e-12, abs=1e-15)
+
+
+@pytest.mark.parametrize("q", LOW_N)
+def test_v_int_reference_arithmetic_low_n(q):
+    from oracle.vint_exact import v_int_exact
+
+    assert qd.v_int(*q) == pytest.approx(v_int_exact(*q), rel=1e-9, abs=1e-14)
+
+
+@pytest.mark.parametrize("q", HIGH_N)
+def test_v_int_reference_arithmetic_fails_at_high_n(q):
+    # the reference's real(8) accumulation cancels away every digit here;
+    # QD_TBME_QUAD exists for this
+    from oracle.vint_exact import v_int_exact
+
+    ex = v_int_exact(*q)
+    assert abs(qd.v_int(*q) - ex) > 10 * abs(ex)
 
 
 @pytest.mark.parametrize("nbody,hw,ref", [(2, 1.0, 3.1619), (6, 1.0, 20.7192), (6, 0.28, 8.0196)])
