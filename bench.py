@@ -1,25 +1,34 @@
 #!/usr/bin/env python
-"""Benchmark of the IM-SRG(2) commutator engine on B200.
+"""Benchmark of the IM-SRG(2) engine on B200.
 
-Workload (one step): the FP64 commutator C = [Omega, H] of two seeded random
-operators in the (M_L,M_S)-blocked layout of an N=20 electron, R=20 shell
-quantum dot (420 spin-orbitals, 61,947,679 stored entries = 495.6 MB per
-operator), with the particle-hole (Pandya) channel on: E0, one- and two-body
-parts through 110/220/111/121/221/122/222.  H is Hermitian, Omega
-anti-Hermitian, entries iid N(0, 0.1^2), then (anti)symmetrised.
+Default workload (--workload flow), the metric's own configuration: seconds
+to a converged ground-state energy of the 2-D quantum dot with N=20
+electrons in R=20 shells at hbar-omega=0.5 (420 spin-orbitals, 61,947,679
+entries = 495.6 MB per operator).  Input: Coulomb TBMEs (v_int in
+__float128, because the reference's real(8) sums lose every digit at R=20)
+and Hartree-Fock on the host (not timed).  One step = one whole Magnus
+IM-SRG(2) flow (first-order Magnus, Euler steps of 0.7, nested BCH series,
+White generator) from the HF Hamiltonian resident in HBM to |MBPT2| <= 1e-9,
+FP64 throughout, ladders only as the reference's run_magnus (--pandya adds
+the particle-hole channel).  value: seconds per converged E_gs (lower is
+better); e2e: the same through the C ABI with the Hamiltonian uploaded from
+pinned host memory and the evolved one downloaded every step.
 
-value: whole-job throughput in TFLOP/s, counting the FP64 work of the
-reference algorithm per commutator (qd_imsrg_b200.flops), inputs resident
-in HBM.  e2e: the same metric through the public API with host buffers
-(upload of both operators, commutator, download of the result) every step.
+--workload commutator: one FP64 commutator [Omega, H] of seeded random
+operators at N=20, R=20 with the Pandya channel, in TFLOP/s of the reference
+algorithm's FP64 work.
+
+--workload batch: the N x hbar-omega grid of 16 flows, concurrently
+(qd_magnus_flow_batch) and one after another.
 
 --gpus N (under torchrun): N independent replicas, one per GPU, no data-path
 collective (weak scaling); the timed region is bracketed by barriers and the
 max over ranks is reported.
 
---impl reference: the CPU restatement of the reference (oracle/, with
-OpenBLAS dgemm) on the host cores; each step is a bounded block sample of
-the same commutator (a stride-S block subset, rotating over steps).
+--impl reference: the CPU restatement of the reference (oracle/, OpenMP,
+OpenBLAS dgemm) on the host cores, on a bounded sample of the same workload
+(block-sampled phases of the flow's commutator, scaled to one flow by the
+flow's commutator count; or of the random commutator).
 """
 from __future__ import annotations
 
@@ -44,7 +53,7 @@ SEED_H, SEED_OMEGA = 1, 2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--nbody", type=int, default=NBODY)
@@ -52,7 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-stride", type=int, default=8)
-    ap.add_argument("--workload", choices=["commutator", "flow"], default="commutator")
+    ap.add_argument("--cpu-phases", type=int, default=2, help="block-sampled phases timed for the CPU baseline")
+    ap.add_argument("--batch-max-iter", type=int, default=300, help="batch: flow step limit per instance")
+    ap.add_argument("--workload", choices=["flow", "commutator", "batch"], default="flow")
     ap.add_argument("--hw", type=float, default=0.5)
     ap.add_argument("--pandya", action="store_true", help="flow: add the particle-hole channel")
     ap.add_argument("--hf-mix", type=float, default=0.5, help="flow: HF density mixing (1 = plain iteration)")
@@ -303,11 +314,63 @@ def sample_flops(P, stride):
 
 
 # --------------------------------------------------------------------------
+# Commutators of the converged FP64 flow at the benchmarked configurations
+# (the flow is deterministic: every run takes the same steps).  They scale
+# the CPU restatement's time per commutator to seconds per E_gs where the
+# whole CPU flow would take hours.
+FLOW_COMMUTATORS = {(20, 20, 0.5, False): 181, (20, 20, 0.5, True): 115}
+
+
+def flow_input(args, nbody=None, emax=None, hw=None):
+    """HF Hamiltonian of a flow workload (host, not timed)."""
+    import qd_imsrg_b200 as qd
+
+    t0 = time.perf_counter()
+    vec, eig, hf_it = qd.hf_hamiltonian(nbody or args.nbody, emax or args.emax, hw or args.hw, mix=args.hf_mix,
+                                        quad=args.tbme == "quad")
+    return vec, eig, hf_it, time.perf_counter() - t0
+
+
+def cpu_flow_estimate(vec, eig, args, commutators: int) -> dict:
+    """The oracle on the host cores on a bounded sample of the flow: phases
+    0..p-1 (of `ref_stride`) of the flow's first BCH commutator [Omega, H],
+    Omega = 0.7 eta(H).  Phase 0 carries E0 and the one-body parts plus its
+    blocks; seconds per commutator = t0 + (stride - 1) * mean(t1..),
+    seconds per E_gs = that times the flow's commutator count."""
+    import oracle
+
+    O = oracle.Layout(args.nbody, args.emax, eig=eig)
+    H = oracle.Op(O, 1, vec)
+    eta = oracle.Op(O, -1)
+    oracle.build_white(eta, H)
+    G = oracle.Op(O, -1)
+    oracle.add_arrays(G, 1.0, eta, float(np.float32(0.7)), G)
+    C = oracle.Op(O, 1)
+    S = oracle.Sampler(G)
+    stride, phases = args.ref_stride, max(2, min(args.cpu_phases, args.ref_stride))
+    ts = []
+    for ph in range(phases):
+        t0 = time.perf_counter()
+        S.run(G, H, C, stride, ph, pandya=args.pandya)
+        ts.append(time.perf_counter() - t0)
+    per_comm = ts[0] + (stride - 1) * (sum(ts[1:]) / (len(ts) - 1))
+    return {"value": per_comm * commutators, "unit": "s per converged E_gs", "cores": oracle.get_threads(),
+            "kind": "port", "seconds_per_commutator": per_comm, "commutators": commutators,
+            "sample": "phases 0..%d of %d block-sampled phases of the flow's first commutator [Omega, H] "
+                      "(Omega = 0.7 eta(H_HF)) timed on the oracle (OpenMP, OpenBLAS); seconds per "
+                      "commutator extrapolated from them, times the flow's %d commutators" %
+                      (phases - 1, stride, commutators)}
+
+
+def flow_desc(args):
+    return "Magnus IM-SRG(2) flow to |MBPT2| <= 1e-9, N=%d R=%d hbar-omega=%g, %s" % (
+        args.nbody, args.emax, args.hw, "particle-hole channel on" if args.pandya else "ladders only (run_magnus)")
+
+
 def run_flow(args, world, rank, local):
-    """Time to a converged ground-state energy: Hartree-Fock on the host, then
-    the Magnus flow (first-order Magnus, Euler steps, BCH series, White
-    generator) on the device to |MBPT2(H(s))| <= 1e-9, one flow per step.
-    The one- plus two-body norm drives the BCH truncation and the step
+    """Seconds to a converged ground-state energy: Hartree-Fock on the host,
+    then the Magnus flow on the device to |MBPT2(H(s))| <= 1e-9, one flow per
+    step.  The one- plus two-body norm drives the BCH truncation and the step
     rejection (the reference's one-body norm never accepts a step on a
     Hartree-Fock Hamiltonian)."""
     import torch
@@ -316,70 +379,80 @@ def run_flow(args, world, rank, local):
 
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    t0 = time.perf_counter()
-    vec, eig, hf_it = qd.hf_hamiltonian(args.nbody, args.emax, args.hw, mix=args.hf_mix, quad=args.tbme == "quad")
-    setup_s = time.perf_counter() - t0
+    vec, eig, hf_it, setup_s = flow_input(args)
     P = qd.Layout(args.nbody, args.emax, eig=eig, device=local)
     stream = torch.cuda.Stream(device=device)
     P.set_stream(stream.cuda_stream)
     H, HS = qd.FullHam(P, 1, vec), qd.FullHam(P, 1)
-    hv = torch.from_numpy(vec).pin_memory().numpy()
-    for _ in range(args.warmup):
-        tr, res = qd.magnus_flow(H, HS, pandya=args.pandya, full_norm=True, max_iter=1000)
+
+    def flow():
+        return qd.magnus_flow(H, HS, pandya=args.pandya, full_norm=True, max_iter=1000)
+
+    for _ in range(max(1, args.warmup)):
+        tr, res = flow()
     clocks = ClockSampler(local)
     launches0 = P.launches()
-    P.profile(True)
     barrier(world)
     torch.cuda.synchronize(device)
     clocks.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        tr, res = qd.magnus_flow(H, HS, pandya=args.pandya, full_norm=True, max_iter=1000)
+        tr, res = flow()
     torch.cuda.synchronize(device)
     sec = (time.perf_counter() - t0) / args.steps
     clk = clocks.stop()
     barrier(world)
+    launches = (P.launches() - launches0) // max(1, args.steps)
+    sec = max_over_ranks(sec, world, device)
+    # one more flow with the per-stage event profiler (outside the timed region)
+    P.profile(True)
+    flow()
+    torch.cuda.synchronize(device)
     prof = P.profile_read()
     P.profile(False)
-    launches = P.launches() - launches0
-    sec = max_over_ranks(sec, world, device)
-    # end to end: Hamiltonian uploaded from pinned host memory, evolved one
-    # downloaded, every step
+    # end to end: Hamiltonian uploaded from pinned host memory, evolved one downloaded, every step
+    hv = torch.from_numpy(vec).pin_memory().numpy()
     hout = torch.empty(P.neq, dtype=torch.float64).pin_memory().numpy()
+    ne2e = max(1, min(args.steps, args.e2e_steps))
+    barrier(world)
+    torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    for _ in range(max(1, min(args.steps, args.e2e_steps))):
+    for _ in range(ne2e):
         H.upload(hv)
-        qd.magnus_flow(H, HS, pandya=args.pandya, full_norm=True, max_iter=1000)
+        flow()
         hout[:] = HS.download()
-    e2e_sec = (time.perf_counter() - t0) / max(1, min(args.steps, args.e2e_steps))
-    e2e_sec = max_over_ranks(e2e_sec, world, device)
+    e2e_sec = max_over_ranks((time.perf_counter() - t0) / ne2e, world, device)
     comms = int(res.commutators)
-    name, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
     n, mp = P.nbody, P.msp - P.nbody
     neq2b = P.neq - (1 + n * n + mp * mp + mp * n)
+    name, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
     per = (ms / max(cnt, 1)) / 1e3
     byts = 3.0 * 8 * neq2b
     roof = {"kernel": name, "bound": "hbm", "achieved": byts / per / 1e9, "peak": hbm_peak_gbs(), "unit": "GB/s",
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs", "algorithmic_per_launch": byts,
-            "note": "bytes = read A, B and write C two-body parts once per launch", "traffic": None}
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)", "algorithmic_per_launch": byts,
+            "note": "stage with the most device time, per launch = per commutator; bytes = read A, B and "
+                    "write C two-body parts once",
+            "traffic": NCU_TRAFFIC[name] * P.neq / NCU_NEQ if name in NCU_TRAFFIC else None}
     roof["frac"] = roof["achieved"] / roof["peak"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_flow_estimate(vec, eig, args, comms)
     if rank == 0:
         line = {"metric": METRIC, "value": sec, "unit": "s per converged E_gs", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "Coulomb TBMEs from v_int (host), Hartree-Fock (host)",
-                "config": {"workload": "Magnus IM-SRG(2) flow to |MBPT2| <= 1e-9, N=%d R=%d hbar-omega=%g, %s"
-                                       % (args.nbody, args.emax, args.hw,
-                                          "particle-hole channel on" if args.pandya else "ladders only (run_magnus)"),
-                           "E_HF": float(vec[0]), "E_gs": float(res.E0), "flow_steps": int(res.iterations),
-                           "rejected": int(res.rejected), "commutators": comms, "s_final": float(res.s),
-                           "hf_setup_s": setup_s, "hf_iterations": hf_it, "hf_mix": args.hf_mix,
-                           "tbme": args.tbme,
-                           "bch_terms": [int(x) for x in tr[:, 6]]},
+                "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
+                "config": {"workload": flow_desc(args), "form": "plain FP64", "E_HF": float(vec[0]),
+                           "E_gs": float(res.E0), "flow_steps": int(res.iterations), "rejected": int(res.rejected),
+                           "commutators": comms, "s_final": float(res.s), "hf_setup_s": setup_s,
+                           "hf_iterations": hf_it, "hf_mix": args.hf_mix, "tbme": args.tbme,
+                           "bch_terms": [int(x) for x in tr[:, 6]],
+                           "l2": "every step streams 495.6 MB operators, far above the 126 MB L2",
+                           "parallelism": "replicas x%d" % world},
                 "e2e": {"value": e2e_sec, "unit": "s per converged E_gs", "h2d_bytes_per_step": 8 * P.neq,
                         "d2h_bytes_per_step": 8 * P.neq},
-                "roofline": roof, "cpu_baseline": None, "gpu_launches": launches, "clocks": clk,
-                "stages_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
+                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+                "stages_ms_per_flow": {k: v[0] for k, v in prof.items()}}
         print(json.dumps(line), flush=True)
     for o in (H, HS):
         o.close()
@@ -387,18 +460,134 @@ def run_flow(args, world, rank, local):
     return 0
 
 
+# Batched instances: N x hbar-omega, R=16 for N <= 12 and R=20 otherwise
+BATCH_GRID = [(nb, hw) for nb in (6, 12, 20, 30) for hw in (0.1, 0.28, 0.5, 1.0)]
+
+
+def run_batch(args, world, rank, local):
+    """16 independent flows (the N x hbar-omega grid) run concurrently by
+    qd_magnus_flow_batch (one host thread and stream per instance) against
+    the same flows one after another; per-instance E_gs must agree."""
+    import torch
+
+    import qd_imsrg_b200 as qd
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    inst, skipped = [], []
+    for nb, hw in BATCH_GRID:
+        R = 16 if nb <= 12 else 20
+        try:
+            vec, eig, _, _ = flow_input(args, nb, R, hw)
+        except qd.QDError as e:
+            skipped.append({"N": nb, "hw": hw, "R": R, "why": str(e)})
+            continue
+        P = qd.Layout(nb, R, eig=eig, device=local)
+        inst.append({"N": nb, "hw": hw, "R": R, "P": P, "H": qd.FullHam(P, 1, vec), "HS": qd.FullHam(P, 1),
+                     "E_HF": float(vec[0])})
+    setup_s = time.perf_counter() - t0
+    kw = dict(pandya=args.pandya, full_norm=True, max_iter=args.batch_max_iter)
+    # one after another (also allocates every layout's flow workspaces)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for d in inst:
+        try:
+            _, r = qd.magnus_flow(d["H"], d["HS"], **kw)
+            d["E_sep"], d["steps"], d["ok"] = float(r.E0), int(r.iterations), True
+        except qd.QDError as e:
+            d["ok"], d["why"] = False, str(e)
+    torch.cuda.synchronize(device)
+    t_sep = time.perf_counter() - t0
+    good = [d for d in inst if d["ok"]]
+    pairs = [(d["H"], d["HS"]) for d in good]
+    for _ in range(max(0, args.warmup - 1)):
+        qd.magnus_flow_batch(pairs, raise_on_error=False, **kw)
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res, st = qd.magnus_flow_batch(pairs, raise_on_error=False, **kw)
+    torch.cuda.synchronize(device)
+    t_batch = (time.perf_counter() - t0) / args.steps
+    clk = clocks.stop()
+    t_batch = max_over_ranks(t_batch, world, device)
+    worst = 0.0
+    for d, r, s_ in zip(good, res, st):
+        d["E_batch"], d["status"] = float(r.E0), s_
+        worst = max(worst, abs(d["E_batch"] - d["E_sep"]))
+    if rank == 0:
+        per = [{k: d[k] for k in ("N", "hw", "R", "E_HF", "E_sep", "E_batch", "steps") if k in d} for d in good]
+        fails = [{"N": d["N"], "hw": d["hw"], "R": d["R"], "why": d["why"]} for d in inst if not d["ok"]]
+        line = {"metric": "s for the %d converged E_gs of the N x hbar-omega grid (batched flows)" % len(good),
+                "value": t_batch, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * t_batch, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
+                "config": {"workload": "batched Magnus IM-SRG(2) flows, N in {6,12,20,30} x hbar-omega in "
+                                       "{0.1,0.28,0.5,1.0}, R=16 for N<=12 else 20, %s" %
+                                       ("particle-hole channel on" if args.pandya else "ladders only"),
+                           "separate_s": t_sep, "speedup_vs_separate": t_sep / t_batch,
+                           "max_abs_dE_batch_vs_separate": worst, "instances": per, "flow_failed": fails,
+                           "hf_failed": skipped, "setup_s": setup_s},
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    for d in inst:
+        d["H"].close()
+        d["HS"].close()
+        d["P"].close()
+    return 0
+
+
+def run_reference_flow(args, world, rank):
+    """Reference arm of the flow workload: the oracle on the host cores, per
+    step a bounded sample (block-sampled phases of the flow's commutator),
+    reported as seconds per converged E_gs."""
+    if rank != 0:
+        return 0
+    key = (args.nbody, args.emax, args.hw, bool(args.pandya))
+    vec, eig, hf_it, setup_s = flow_input(args)
+    if key in FLOW_COMMUTATORS:
+        comms, how = FLOW_COMMUTATORS[key], "the FP64 flow's commutator count at this configuration"
+    else:  # small bases: the whole CPU flow runs; count its commutators
+        import oracle
+
+        O = oracle.Layout(args.nbody, args.emax, eig=eig)
+        tr, _ = oracle.magnus_flow(oracle.Op(O, 1, vec), oracle.Op(O, 1), pandya=args.pandya, max_iter=1000,
+                                   full_norm=True)
+        comms, how = int(np.abs(tr[:, 6]).sum()), "counted by running the CPU flow"
+    vals = []
+    for k in range(args.warmup + args.steps):
+        est = cpu_flow_estimate(vec, eig, args, comms)
+        if k >= args.warmup:
+            vals.append(est)
+    val = statistics.median([e["value"] for e in vals])
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "s per converged E_gs", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * val, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
+            "config": {"workload": flow_desc(args) + "; reference arm: CPU restatement", "commutators": comms,
+                       "commutator_count": how, "hf_setup_s": setup_s},
+            "cpu_baseline": {"value": val, "unit": "s per converged E_gs", "cores": vals[-1]["cores"],
+                             "kind": "port", "sample": vals[-1]["sample"]},
+            "e2e": {"value": val, "unit": "s per converged E_gs", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
-    if args.workload == "flow" and args.impl == "ours":
-        rc = run_flow(args, world, rank, local)
+    if args.workload in ("flow", "batch") and args.impl == "ours":
+        rc = (run_flow if args.workload == "flow" else run_batch)(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
 
             dist.destroy_process_group()
         return rc
     if args.impl == "reference":
-        rc = run_reference(args, world, rank)
+        rc = run_reference_flow(args, world, rank) if args.workload == "flow" else run_reference(args, world, rank)
         if world > 1:
             import torch.distributed as dist
 

@@ -241,6 +241,34 @@ typedef struct qd_flow_result {
 } qd_flow_result;
 int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, double* trace,
                    qd_flow_result* result);
+/* The same flow as a stepping object, for callers that inspect or seed
+ * Omega (no reference counterpart: run_magnus owns its loop).  One flow per
+ * layout at a time (its workspaces are the layout's).
+ *   qd_flow_create      s = 0: HS = HAM, ETA = build_white(HS), nrm1 = |ETA|
+ *   qd_flow_warm_start  Omega = G at flow parameter s: HS = BCH(G, HAM),
+ *                       ETA = build_white(HS); nrm1 keeps its s = 0 value
+ *   qd_flow_step        one pass of s_evolve's loop (accepted or rejected)
+ *   qd_flow_omega       the flow's current Omega (owned by the flow)       */
+typedef struct qd_flow qd_flow;
+typedef struct qd_flow_step_info {
+  double s, E0, nrm1, nrm2, crit;  /* crit: |MBPT2| before the step        */
+  int terms;                       /* BCH commutators of the step           */
+  int accepted;                    /* 0: rejected on eta-norm growth        */
+  int converged;                   /* |MBPT2(HS)| <= 1e-9 after the step    */
+} qd_flow_step_info;
+int qd_flow_create(const qd_op* HAM, qd_op* HS, unsigned flags, qd_flow** flow);
+int qd_flow_warm_start(qd_flow* flow, const qd_op* G, double s);
+int qd_flow_step(qd_flow* flow, qd_flow_step_info* info);
+int qd_flow_omega(const qd_flow* flow, qd_op** G);
+int qd_flow_state(const qd_flow* flow, qd_flow_result* result);
+int qd_flow_destroy(qd_flow* flow);
+/* Several independent flows (e.g. a grid of (N, hbar-omega, emax)), one per
+ * layout, run concurrently: one host thread per instance, each on its own
+ * layout's stream.  No reference counterpart (the reference runs one flow per
+ * process).  status[i] is instance i's qd_magnus_flow code; the call returns
+ * the first failing one (and names the instance in qd_last_error).          */
+int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, unsigned flags, int max_iter,
+                         qd_flow_result* results, int* status);
 
 #ifdef __cplusplus
 }

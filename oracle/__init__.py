@@ -91,7 +91,7 @@ def lib():
             "orc_use_blas": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p]),
             "orc_sampler_new": (_vp, [_vp]),
             "orc_sampler_free": (None, [_vp]),
-            "orc_commutator_sample": (None, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
+            "orc_commutator_sample": (None, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -332,14 +332,18 @@ def bch_expand(HS: Op, G: Op, H: Op, pandya: bool = False, full_norm: bool = Fal
 
 class Sampler:
     """Bounded samples of one commutator [A,B] for CPU timing: phase p of
-    `stride` does the two-body work of every stride-th block (and E0 plus the
-    one-body parts on phase 0); the phases together do one whole commutator."""
+    `stride` does the two-body work of every stride-th block and the
+    cross-coupled products of every stride-th cc block (and E0 plus the
+    one-body parts, and with pandya calc_cc, on phase 0).  The phases
+    together do the work of one whole commutator; without the Pandya channel
+    they also give its result (with it, a phase's ph terms see only the
+    products formed in that phase)."""
 
     def __init__(self, A: Op):
         self.h = lib().orc_sampler_new(A.h)
 
-    def run(self, A: Op, B: Op, Cop: Op, stride: int, phase: int) -> None:
-        lib().orc_commutator_sample(self.h, A.h, B.h, Cop.h, int(stride), int(phase))
+    def run(self, A: Op, B: Op, Cop: Op, stride: int, phase: int, pandya: bool = True) -> None:
+        lib().orc_commutator_sample(self.h, A.h, B.h, Cop.h, int(stride), int(phase), int(pandya))
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

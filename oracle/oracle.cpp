@@ -993,9 +993,11 @@ void sampled_commutator(Op& A, Op& B, Op& C, Op& w1, Op& w2, CC& ACC, CC& BCC, i
     for (int JJ = 1; JJ <= nb; ++JJ)
       for (int II = 1; II <= nb; ++II) run(P(b.qnph, II, 1), P(b.qnph, II, 0), P(b.qnph, JJ, 1), P(b.qnph, JJ, 0), 1, elr(C.Vphph(q), nb, II, JJ));
   }
-  // cross-coupled products of the selected cc blocks
-  std::vector<double> XCC(L.x2size, 0.0), YCC(L.x2size, 0.0);
-  for (int q = 1 + phase; q <= L.ccn; q += stride) {
+  // cross-coupled products of the selected cc blocks (none when the X are
+  // known to be zero, as commutator_222 skips them: the ph terms add zeros)
+  const bool have_cc = !(ACC.zero && BCC.zero);
+  std::vector<double> XCC(have_cc ? L.x2size : 0, 0.0), YCC(have_cc ? L.x2size : 0, 0.0);
+  for (int q = 1 + phase; have_cc && q <= L.ccn; q += stride) {
     const CCBlk& c = L.cc[q - 1];
     if (c.r == 0 || c.nb == 0) continue;
     dgemm('N', 'T', c.r, c.r, c.nb, BCC.herm, &ACC.X[c.off], c.r, &BCC.X[c.off], c.r, 0.0, &XCC[c.off2], c.r);
@@ -1016,6 +1018,7 @@ void sampled_commutator(Op& A, Op& B, Op& C, Op& w1, Op& w2, CC& ACC, CC& BCC, i
   for (int q = 1 + phase; q <= L.nblock; q += stride) {
     const Blk& b = L.blk[q - 1];
     matrix_mult222(A, B, C, w1, q, b.nhh, b.npp, b.nph);
+    if (!have_cc) continue;
     auto ph = [&](int b1, int b2, int k1, int k2) {
       int q31, r31, q24, r24, q32, r32, q14, r14, q41, r41, q23, r23, q42, r42, q13, r13;
       mp(k1, b1, q31, r31); mp(b2, k2, q24, r24);
@@ -1250,11 +1253,11 @@ int orc_use_blas(const char* path, const char* dgemm_sym, const char* threads_sy
 // Bounded sample of [A,B] (see sampled_commutator); cross-coupled matrices of
 // both operators are filled on phase 0 and reused by later phases.
 void* orc_sampler_new(void* A) { return new Sampler(((Op*)A)->L); }
-void orc_commutator_sample(void* sampler, void* A, void* B, void* C, int stride, int phase) {
+void orc_commutator_sample(void* sampler, void* A, void* B, void* C, int stride, int phase, int pandya) {
   Sampler* s = (Sampler*)sampler;
   Op& a = *(Op*)A;
   Op& b = *(Op*)B;
-  if (phase == 0) {
+  if (phase == 0 && pandya) {
     calc_cc(a, s->a);
     s->a.herm = a.herm;
     calc_cc(b, s->b);

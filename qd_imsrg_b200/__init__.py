@@ -24,7 +24,7 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import QD_FULL_NORM, QD_PANDYA, QD_TBME_QUAD, FlowResult, QDError, check, lib
+from ._native import QD_FULL_NORM, QD_PANDYA, QD_TBME_QUAD, FlowResult, FlowStepInfo, QDError, check, lib
 
 __all__ = [
     "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA", "QD_FULL_NORM",
@@ -167,7 +167,8 @@ class FullHam:
 
     def close(self) -> None:
         if getattr(self, "h", None) and self.h.value:
-            lib().qd_op_destroy(self.h)
+            if getattr(self, "_owned", True):
+                lib().qd_op_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
@@ -310,6 +311,94 @@ def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int =
     res = FlowResult()
     check(lib().qd_magnus_flow(HAM.h, HS.h, _flags(pandya, full_norm), int(max_iter), _d(trace), C.byref(res)))
     return trace[: res.rows], res
+
+
+class Flow:
+    """s_evolve as a stepping object: Flow(HAM, HS) starts at s = 0;
+    warm_start(G, s) seeds Omega = G at flow parameter s; step() runs one
+    pass of the loop; omega() is the flow's Omega (owned by the flow)."""
+
+    def __init__(self, HAM: FullHam, HS: FullHam, pandya: bool = False, full_norm: bool = False):
+        self.layout = HAM.layout
+        self.h = C.c_void_p()
+        check(lib().qd_flow_create(HAM.h, HS.h, _flags(pandya, full_norm), C.byref(self.h)))
+
+    def warm_start(self, G: FullHam, s: float) -> None:
+        check(lib().qd_flow_warm_start(self.h, G.h, float(s)))
+
+    def step(self) -> FlowStepInfo:
+        info = FlowStepInfo()
+        check(lib().qd_flow_step(self.h, C.byref(info)))
+        return info
+
+    def omega(self) -> FullHam:
+        g = C.c_void_p()
+        check(lib().qd_flow_omega(self.h, C.byref(g)))
+        return _borrowed(self.layout, g)
+
+    def state(self) -> FlowResult:
+        r = FlowResult()
+        check(lib().qd_flow_state(self.h, C.byref(r)))
+        return r
+
+    def run(self, max_iter: int = 500) -> FlowResult:
+        """Step until converged; raises QDError after max_iter steps."""
+        for _ in range(max_iter + 1):
+            if self.step().converged:
+                return self.state()
+        raise QDError(6, "Flow.run: not converged after %d steps" % max_iter)
+
+    def close(self) -> None:
+        if getattr(self, "h", None) and self.h.value:
+            lib().qd_flow_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _borrowed(layout: Layout, handle) -> FullHam:
+    """A FullHam view of an operator owned by the library (never destroyed
+    from Python)."""
+    op = FullHam.__new__(FullHam)
+    op.layout = layout
+    op.h = C.c_void_p(handle.value)
+    op._owned = False
+    return op
+
+
+class DeviceView:
+    """__cuda_array_interface__ of an operator's device array (float64, neq
+    entries, vectorize order): zero-copy access from torch and the like.
+    Taking it clears the operator's known-zero parts (writes may follow)."""
+
+    def __init__(self, op: FullHam):
+        self.ptr = op.device_ptr()
+        self.n = op.layout.neq
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.n,), "typestr": "<f8", "data": (self.ptr, False), "version": 3, "strides": None}
+
+
+def magnus_flow_batch(pairs, pandya: bool = False, max_iter: int = 500, full_norm: bool = False,
+                      raise_on_error: bool = True):
+    """Run several independent flows concurrently: pairs = [(HAM, HS), ...],
+    each pair on its own layout.  Returns ([FlowResult], [status]); with
+    raise_on_error, raises QDError for the first failing instance."""
+    n = len(pairs)
+    hams = (C.c_void_p * n)(*[h.h.value for h, _ in pairs])
+    hss = (C.c_void_p * n)(*[s.h.value for _, s in pairs])
+    res = (FlowResult * n)()
+    st = (C.c_int * n)()
+    rc = lib().qd_magnus_flow_batch(n, hams, hss, _flags(pandya, full_norm), int(max_iter), res, st)
+    out = [res[i] for i in range(n)], [int(st[i]) for i in range(n)]
+    if raise_on_error:
+        check(rc)
+    return out
 
 
 # ---- host-side inputs (the reference's HFQDmod / generate_ME) ----------------

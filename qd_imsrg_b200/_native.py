@@ -38,6 +38,11 @@ class QDError(RuntimeError):
         self.code = code
 
 
+class FlowStepInfo(C.Structure):
+    _fields_ = [("s", C.c_double), ("E0", C.c_double), ("nrm1", C.c_double), ("nrm2", C.c_double),
+                ("crit", C.c_double), ("terms", C.c_int), ("accepted", C.c_int), ("converged", C.c_int)]
+
+
 class FlowResult(C.Structure):
     _fields_ = [("E0", C.c_double), ("s", C.c_double), ("iterations", C.c_int), ("rejected", C.c_int),
                 ("commutators", C.c_int), ("rows", C.c_int)]
@@ -93,6 +98,14 @@ SIGNATURES = {
     "qd_magnus_expand": (C.c_int, [_vp, _vp, _vp]),
     "qd_euler_step": (C.c_int, [_vp, _vp, _dp, C.c_double]),
     "qd_magnus_flow": (C.c_int, [_vp, _vp, C.c_uint, C.c_int, _dp, C.POINTER(FlowResult)]),
+    "qd_magnus_flow_batch": (C.c_int, [C.c_int, C.POINTER(_vp), C.POINTER(_vp), C.c_uint, C.c_int,
+                                       C.POINTER(FlowResult), C.POINTER(C.c_int)]),
+    "qd_flow_create": (C.c_int, [_vp, _vp, C.c_uint, C.POINTER(_vp)]),
+    "qd_flow_warm_start": (C.c_int, [_vp, _vp, C.c_double]),
+    "qd_flow_step": (C.c_int, [_vp, C.POINTER(FlowStepInfo)]),
+    "qd_flow_omega": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "qd_flow_state": (C.c_int, [_vp, C.POINTER(FlowResult)]),
+    "qd_flow_destroy": (C.c_int, [_vp]),
     "qd_tbme_write": (C.c_int, [C.c_int, C.c_char_p, C.c_int, C.c_uint]),
     "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, C.c_double, C.c_uint,
                                     _dp, _dp, _i64, _ip]),

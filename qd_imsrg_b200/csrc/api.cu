@@ -5,7 +5,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
 #include <utility>
+#include <vector>
 
 #include "dev_common.cuh"
 
@@ -23,11 +28,16 @@ struct Workspace {
   qd_op* w2 = nullptr;
   qd_cc* ca = nullptr;
   qd_cc* cb = nullptr;
+  // Magnus flow: ETA, G, DG, ETA0, G0, HS0, INT1, INT2, AD, w1, w2 and HCC,
+  // OCC, allocated by the first flow on the layout and kept
+  qd_op* flow[11] = {nullptr};
+  qd_cc* flow_cc[2] = {nullptr};
 };
 std::map<const qd_layout*, Workspace>& workspaces() {
   static std::map<const qd_layout*, Workspace> m;
   return m;
 }
+std::mutex g_ws_mutex;  // workspaces of different layouts from concurrent host threads
 
 #define CHECK(cond, code, ...)    \
   do {                            \
@@ -60,16 +70,41 @@ int op_new(qd_layout* L, int herm, qd_op** out) {
     delete op;
     return cuda_fail(e, "cudaMalloc(operator)");
   }
+  ++L->children;
   QD_CUDA(cudaMemsetAsync(op->d, 0, sizeof(double) * L->neq, L->stream));
   op->zero_mask = ALL_PARTS;
   *out = op;
   return QD_OK;
 }
 
+// Tear down a layout's device state and the layout itself.
+void layout_finish(qd_layout* L) {
+  drop_122_plan(L);
+  layout_free_device(L);
+  delete L;
+}
+
+// A layout destroyed while operators or cross-coupled matrices still refer
+// to it (e.g. a garbage collector finalising the layout first) stays alive
+// until the last of them is freed.
+void release_child(qd_layout* L) {
+  if (--L->children == 0 && L->closing) layout_finish(L);
+}
+
 void op_free(qd_op* op) {
   if (!op) return;
+  qd_layout* L = op->L;
   if (op->d) cudaFree(op->d);
   delete op;
+  release_child(L);
+}
+
+void cc_free(qd_cc* c) {
+  if (!c) return;
+  qd_layout* L = c->L;
+  if (c->d) cudaFree(c->d);
+  delete c;
+  release_child(L);
 }
 
 int cc_new(qd_layout* L, double herm, qd_cc** out) {
@@ -82,8 +117,9 @@ int cc_new(qd_layout* L, double herm, qd_cc** out) {
       delete c;
       return cuda_fail(e, "cudaMalloc(cc)");
     }
-    QD_CUDA(cudaMemsetAsync(c->d, 0, sizeof(double) * L->xsize, L->stream));
   }
+  ++L->children;
+  if (c->d) QD_CUDA(cudaMemsetAsync(c->d, 0, sizeof(double) * L->xsize, L->stream));
   *out = c;
   return QD_OK;
 }
@@ -173,6 +209,7 @@ int stage_111(qd_layout* L, const qd_op* A, const qd_op* B, qd_op* C) {
   return QD_OK;
 }
 
+// commutator_221 with the reference's visible intermediates w1, w2
 int stage_221(qd_layout* L, const qd_op* A, const qd_op* B, qd_op* C, qd_op* w1, qd_op* w2) {
   StageTimer tm(L, S_221);
   QD_CUDA(cudaMemsetAsync(w1->d, 0, sizeof(double) * L->neq, L->stream));
@@ -216,7 +253,12 @@ int commutator_seq(qd_layout* L, const qd_op* A, const qd_op* B, qd_op* C, qd_op
     StageTimer tm(L, S_121);
     TRY(launch_121(L, A, B, C->d));
   }
-  TRY(stage_221(L, A, B, C, w1, w2));
+  {  // w1, w2 are workspaces of the whole commutator: the fused 221 leaves them untouched
+    (void)w1;
+    (void)w2;
+    StageTimer tm(L, S_221);
+    TRY(launch_221_fused(L, A, B, C->d));
+  }
   {
     StageTimer tm(L, S_122);
     TRY(launch_122(L, A, B, C->d));
@@ -236,6 +278,7 @@ int commutator_seq(qd_layout* L, const qd_op* A, const qd_op* B, qd_op* C, qd_op
 }
 
 int get_ws(qd_layout* L, Workspace** out) {
+  std::lock_guard<std::mutex> lock(g_ws_mutex);
   Workspace& w = workspaces()[L];
   if (!w.w1) TRY(op_new(L, 1, &w.w1));
   if (!w.w2) TRY(op_new(L, 1, &w.w2));
@@ -246,17 +289,21 @@ int get_ws(qd_layout* L, Workspace** out) {
 }
 
 void drop_ws(const qd_layout* L) {
-  auto& m = workspaces();
-  auto it = m.find(L);
-  if (it == m.end()) return;
-  op_free(it->second.w1);
-  op_free(it->second.w2);
-  for (qd_cc* c : {it->second.ca, it->second.cb})
-    if (c) {
-      if (c->d) cudaFree(c->d);
-      delete c;
-    }
-  m.erase(it);
+  Workspace w;
+  {
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    auto& m = workspaces();
+    auto it = m.find(L);
+    if (it == m.end()) return;
+    w = it->second;
+    m.erase(it);
+  }
+  op_free(w.w1);
+  op_free(w.w2);
+  cc_free(w.ca);
+  cc_free(w.cb);
+  for (qd_op* o : w.flow) op_free(o);
+  for (qd_cc* c : w.flow_cc) cc_free(c);
 }
 
 const double kCof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666, 0.0083333333333333333,
@@ -330,9 +377,11 @@ int qd_layout_destroy(qd_layout* L) {
   cudaSetDevice(L->device);
   cudaStreamSynchronize(L->stream);
   drop_ws(L);
-  drop_122_plan(L);
-  layout_free_device(L);
-  delete L;
+  if (L->children > 0)
+    L->closing = true;  // the last operator or cc freed finishes the teardown
+  else
+    layout_finish(L);
+  (void)cudaGetLastError();
   return QD_OK;
 }
 
@@ -450,6 +499,7 @@ int qd_op_destroy(qd_op* op) {
   cudaSetDevice(op->L->device);
   cudaStreamSynchronize(op->L->stream);
   op_free(op);
+  (void)cudaGetLastError();  // teardown errors are not reported; do not leave them pending
   return QD_OK;
 }
 
@@ -632,8 +682,8 @@ int qd_cc_destroy(qd_cc* cc) {
   if (!cc) return QD_OK;
   cudaSetDevice(cc->L->device);
   cudaStreamSynchronize(cc->L->stream);
-  if (cc->d) cudaFree(cc->d);
-  delete cc;
+  cc_free(cc);
+  (void)cudaGetLastError();
   return QD_OK;
 }
 int qd_cc_set_herm(qd_cc* cc, double herm) {
@@ -704,7 +754,6 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   TRY(use_device(L));
   TRY(build_programs(L));
   const bool pandya = (flags & QD_PANDYA) != 0;
-  auto norm = (flags & QD_FULL_NORM) ? reduce_norm_full : reduce_norm1b;
   CHECK(!pandya || (HCC && OCC), QD_ERR_ARG, "qd_bch_expand: QD_PANDYA needs HCC and OCC");
   const double conv = (double)1e-5f;  // "conv = 1e-5" is a real(4) literal in the reference
   INT2->herm = 1;
@@ -715,16 +764,17 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   for (int i = 2; i <= 12; ++i) {
     std::swap(INT2->d, AD->d);  // AD = previous term; INT2 becomes the output buffer
     std::swap(INT2->zero_mask, AD->zero_mask);
-    TRY(norm(L, HS->d, red_slot(L, 1)));  // |INT1| = |HS| before the update
     if (pandya) {
       TRY(commutator_seq(L, G, AD, INT2, w1, w2, OCC, HCC, true));
     } else {
       TRY(commutator_seq(L, G, AD, INT2, w1, w2, nullptr, nullptr, false));
     }
     ++count;
-    TRY(norm(L, INT2->d, red_slot(L, 2)));
     const double cof = kCof[i - 2];
-    TRY(launch_axpy(L, HS->d, 1.0, INT2->d, cof, HS->d, L->neq));
+    {  // HS += cof * INT2 with |INT1| = |HS| before the update and |INT2| in the same pass
+      StageTimer tm(L, S_GLUE);
+      TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, (flags & QD_FULL_NORM) ? 1 : 0, red_slot(L, 1)));
+    }
     HS->zero_mask &= INT2->zero_mask;
     QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     QD_CUDA(cudaStreamSynchronize(L->stream));
@@ -746,127 +796,254 @@ int qd_euler_step(qd_op* G, const qd_op* DG, double* s, double stp) {
   return QD_OK;
 }
 
-int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, double* trace,
-                   qd_flow_result* result) {
-  TRY(same_layout(HAM, HS));
-  qd_layout* L = HAM->L;
-  TRY(use_device(L));
-  const double conv_criteria = (double)1e-9f;  // real(4) literal in the reference
+}  // extern "C"
+
+// ---- the Magnus flow as a stepping object (s_evolve, magnus_IMSRG.f90:194-248)
+struct qd_flow {
+  qd_layout* L = nullptr;
+  const qd_op* HAM = nullptr;
+  qd_op* HS = nullptr;
+  unsigned flags = 0;
   qd_op *ETA = nullptr, *G = nullptr, *DG = nullptr, *ETA0 = nullptr, *G0 = nullptr, *HS0 = nullptr;
   qd_op *INT1 = nullptr, *INT2 = nullptr, *AD = nullptr, *w1 = nullptr, *w2 = nullptr;
   qd_cc *HCC = nullptr, *OCC = nullptr;
-  int rc = QD_OK;
-  auto cleanup = [&]() {
-    cudaStreamSynchronize(L->stream);
-    for (qd_op* o : {ETA, G, DG, ETA0, G0, HS0, INT1, INT2, AD, w1, w2}) op_free(o);
-    for (qd_cc* c : {HCC, OCC})
-      if (c) {
-        if (c->d) cudaFree(c->d);
-        delete c;
-      }
-  };
-#define FLOW(x)          \
-  do {                   \
-    rc = (x);            \
-    if (rc) {            \
-      cleanup();         \
-      return rc;         \
-    }                    \
-  } while (0)
-  FLOW(op_new(L, -1, &ETA));
-  FLOW(op_new(L, -1, &G));
-  FLOW(op_new(L, -1, &DG));
-  FLOW(op_new(L, -1, &ETA0));
-  FLOW(op_new(L, -1, &G0));
-  FLOW(op_new(L, 1, &HS0));
-  FLOW(op_new(L, 1, &INT1));
-  FLOW(op_new(L, 1, &INT2));
-  FLOW(op_new(L, 1, &AD));
-  FLOW(op_new(L, 1, &w1));
-  FLOW(op_new(L, 1, &w2));
-  FLOW(cc_new(L, 1.0, &HCC));
-  FLOW(cc_new(L, -1.0, &OCC));
   double s = 0.0, stp = (double)0.7f;  // "stp=.7" is a real(4) literal
-  FLOW(qd_copy_arrays(HAM, HS));
-  HS->herm = 1;
-  auto eta_norm = [&](const qd_op* op, double* out) -> int {
-    if (!(flags & QD_FULL_NORM)) return qd_mat_2_norm(op, out);
-    TRY(reduce_norm_full(L, op->d, red_slot(L, 0)));
-    return scalar_out(L, red_slot(L, 0), out);
-  };
-  FLOW(qd_build_white(ETA, HS));
-  double nrm1, crit;
-  FLOW(eta_norm(ETA, &nrm1));
-  FLOW(qd_mbpt2(HAM, &crit));
-  crit = std::fabs(crit);
-  int iteration = 0, rows = 0, loops = 0, rejected = 0, comms = 0;
-  while (crit > conv_criteria) {
-    if (loops++ >= max_iter) {
-      cleanup();
-      if (result) {
-        result->rows = rows;
-        result->iterations = iteration;
-        result->rejected = rejected;
-        result->commutators = comms;
-        result->s = s;
-      }
-      qd::set_error("qd_magnus_flow: not converged after %d steps (crit %.3e)", max_iter, crit);
-      return QD_ERR_NOCONV;
-    }
-    FLOW(qd_copy_arrays(G, G0));
-    FLOW(qd_magnus_expand(DG, G, ETA));
-    FLOW(qd_euler_step(G, DG, &s, stp));
-    FLOW(qd_copy_arrays(HS, HS0));
-    int terms = 0;
-    FLOW(qd_bch_expand(HS, G, HAM, INT1, INT2, AD, w1, w2, HCC, OCC, flags, &terms));
-    comms += terms;
-    FLOW(qd_copy_arrays(ETA, ETA0));
-    FLOW(qd_build_white(ETA, HS));
-    double nrm2;
-    FLOW(eta_norm(ETA, &nrm2));
-    double E0;
-    QD_CUDA(cudaMemcpyAsync(L->h_red + 8, HS->d, sizeof(double), cudaMemcpyDeviceToHost, L->stream));
-    QD_CUDA(cudaStreamSynchronize(L->stream));
-    E0 = L->h_red[8];
-    if (!std::isfinite(E0) || !std::isfinite(nrm2)) {
-      cleanup();
-      qd::set_error("qd_magnus_flow: non-finite energy or generator norm at step %d", loops);
-      return QD_ERR_NAN;
-    }
-    if (trace && rows < max_iter) {
-      double* t = trace + 7 * rows;
-      t[0] = iteration; t[1] = s; t[2] = E0; t[3] = nrm1; t[4] = nrm2; t[5] = crit; t[6] = terms;
-    }
-    ++rows;
-    if (nrm1 * 1.5 < nrm2) {
-      if (trace && rows - 1 < max_iter) trace[7 * (rows - 1) + 6] = -terms;
-      ++rejected;
-      s = s - stp;
-      FLOW(qd_copy_arrays(G0, G));
-      FLOW(qd_copy_arrays(HS0, HS));
-      FLOW(qd_copy_arrays(ETA0, ETA));
-      stp = stp / 2.0 + (double)1e-3f;
-      continue;
-    }
-    double mb;
-    FLOW(qd_mbpt2(HS, &mb));
-    crit = std::fabs(mb);
-    iteration = iteration + 1;
-  }
-  double E0;
-  QD_CUDA(cudaMemcpyAsync(L->h_red + 8, HS->d, sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+  double nrm1 = 0.0, crit = 0.0, E0 = 0.0;
+  int iteration = 0, rejected = 0, comms = 0, rows = 0;
+};
+
+namespace {
+const double kConvCriteria = (double)1e-9f;  // real(4) literal in the reference
+
+int flow_eta_norm(qd_flow* f, const qd_op* op, double* out) {
+  if (!(f->flags & QD_FULL_NORM)) return qd_mat_2_norm(op, out);
+  TRY(reduce_norm_full(f->L, op->d, red_slot(f->L, 0)));
+  return scalar_out(f->L, red_slot(f->L, 0), out);
+}
+
+int flow_e0(qd_flow* f, double* e0) {
+  qd_layout* L = f->L;
+  QD_CUDA(cudaMemcpyAsync(L->h_red + 8, f->HS->d, sizeof(double), cudaMemcpyDeviceToHost, L->stream));
   QD_CUDA(cudaStreamSynchronize(L->stream));
-  E0 = L->h_red[8];
-  cleanup();
-#undef FLOW
-  if (result) {
-    result->E0 = E0;
-    result->s = s;
-    result->iterations = iteration;
-    result->rejected = rejected;
-    result->commutators = comms;
-    result->rows = rows;
+  *e0 = L->h_red[8];
+  return QD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int qd_flow_create(const qd_op* HAM, qd_op* HS, unsigned flags, qd_flow** out) {
+  CHECK(out, QD_ERR_ARG, "qd_flow_create: null output");
+  *out = nullptr;
+  TRY(same_layout(HAM, HS));
+  CHECK(HAM != HS, QD_ERR_ARG, "qd_flow_create: HS must not alias HAM");
+  qd_layout* L = HAM->L;
+  TRY(use_device(L));
+  // workspaces: allocated by the first flow on this layout and kept (they
+  // hold 11 operators; freeing them per flow would cost a device sync each)
+  Workspace* ws;
+  {
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    ws = &workspaces()[L];
   }
+  const int fherm[11] = {-1, -1, -1, -1, -1, 1, 1, 1, 1, 1, 1};
+  for (int k = 0; k < 11; ++k)
+    if (!ws->flow[k]) TRY(op_new(L, fherm[k], &ws->flow[k]));
+  if (!ws->flow_cc[0]) TRY(cc_new(L, 1.0, &ws->flow_cc[0]));
+  if (!ws->flow_cc[1]) TRY(cc_new(L, -1.0, &ws->flow_cc[1]));
+  qd_flow* f = new qd_flow();
+  f->L = L;
+  f->HAM = HAM;
+  f->HS = HS;
+  f->flags = flags;
+  qd_op** o = ws->flow;
+  f->ETA = o[0]; f->G = o[1]; f->DG = o[2]; f->ETA0 = o[3]; f->G0 = o[4]; f->HS0 = o[5];
+  f->INT1 = o[6]; f->INT2 = o[7]; f->AD = o[8]; f->w1 = o[9]; f->w2 = o[10];
+  f->HCC = ws->flow_cc[0];
+  f->OCC = ws->flow_cc[1];
+  for (int k = 0; k < 11; ++k) o[k]->herm = fherm[k];
+  f->HCC->herm = 1.0;
+  f->OCC->herm = -1.0;
+  f->HCC->filled = f->OCC->filled = false;  // run_magnus never fills them (the Pandya option does, per commutator)
+  int rc = QD_OK;
+  // the generator and the Magnus operator start from zero (allocate_everything)
+  for (qd_op* z : {f->ETA, f->G}) {
+    if (cudaMemsetAsync(z->d, 0, sizeof(double) * L->neq, L->stream) != cudaSuccess) rc = QD_ERR_CUDA;
+    z->zero_mask = ALL_PARTS;
+  }
+  if (!rc) rc = qd_copy_arrays(HAM, HS);
+  HS->herm = 1;
+  if (!rc) rc = qd_build_white(f->ETA, HS);
+  if (!rc) rc = flow_eta_norm(f, f->ETA, &f->nrm1);
+  if (!rc) rc = qd_mbpt2(HAM, &f->crit);
+  if (!rc) rc = flow_e0(f, &f->E0);
+  if (rc) {
+    delete f;
+    return rc;
+  }
+  f->crit = std::fabs(f->crit);
+  *out = f;
+  return QD_OK;
+}
+
+int qd_flow_warm_start(qd_flow* f, const qd_op* G, double s) {
+  CHECK(f && G, QD_ERR_ARG, "qd_flow_warm_start: null argument");
+  CHECK(G->L == f->L, QD_ERR_ARG, "qd_flow_warm_start: Omega on another layout");
+  CHECK(G != f->G, QD_ERR_ARG, "qd_flow_warm_start: pass a copy of the flow's own Omega");
+  TRY(use_device(f->L));
+  TRY(qd_copy_arrays(G, f->G));
+  f->G->herm = -1;
+  f->s = s;
+  int terms = 0;
+  TRY(qd_bch_expand(f->HS, f->G, f->HAM, f->INT1, f->INT2, f->AD, f->w1, f->w2, f->HCC, f->OCC, f->flags, &terms));
+  f->comms += terms;
+  TRY(qd_build_white(f->ETA, f->HS));
+  double mb;
+  TRY(qd_mbpt2(f->HS, &mb));
+  f->crit = std::fabs(mb);
+  TRY(flow_e0(f, &f->E0));
+  CHECK(std::isfinite(f->E0) && std::isfinite(f->crit), QD_ERR_NAN, "qd_flow_warm_start: non-finite state");
+  return QD_OK;
+}
+
+int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
+  CHECK(f, QD_ERR_ARG, "qd_flow_step: null flow");
+  qd_layout* L = f->L;
+  TRY(use_device(L));
+  qd_flow_step_info inf;
+  std::memset(&inf, 0, sizeof(inf));
+  if (f->crit <= kConvCriteria) {  // converged: nothing to do
+    inf.s = f->s;
+    inf.E0 = f->E0;
+    inf.nrm1 = f->nrm1;
+    inf.crit = f->crit;
+    inf.converged = 1;
+    if (info) *info = inf;
+    return QD_OK;
+  }
+  TRY(qd_copy_arrays(f->G, f->G0));
+  TRY(qd_magnus_expand(f->DG, f->G, f->ETA));
+  TRY(qd_euler_step(f->G, f->DG, &f->s, f->stp));
+  TRY(qd_copy_arrays(f->HS, f->HS0));
+  int terms = 0;
+  TRY(qd_bch_expand(f->HS, f->G, f->HAM, f->INT1, f->INT2, f->AD, f->w1, f->w2, f->HCC, f->OCC, f->flags, &terms));
+  f->comms += terms;
+  TRY(qd_copy_arrays(f->ETA, f->ETA0));
+  TRY(qd_build_white(f->ETA, f->HS));
+  double nrm2, E0;
+  TRY(flow_eta_norm(f, f->ETA, &nrm2));
+  TRY(flow_e0(f, &E0));
+  CHECK(std::isfinite(E0) && std::isfinite(nrm2), QD_ERR_NAN,
+        "qd_flow_step: non-finite energy or generator norm at s = %g", f->s);
+  inf.s = f->s;
+  inf.E0 = E0;
+  inf.nrm1 = f->nrm1;
+  inf.nrm2 = nrm2;
+  inf.crit = f->crit;  // the criterion before this step, as the reference's trace
+  inf.terms = terms;
+  ++f->rows;
+  if (f->nrm1 * 1.5 < nrm2) {  // reject: back to the previous state, smaller step
+    ++f->rejected;
+    f->s = f->s - f->stp;
+    TRY(qd_copy_arrays(f->G0, f->G));
+    TRY(qd_copy_arrays(f->HS0, f->HS));
+    TRY(qd_copy_arrays(f->ETA0, f->ETA));
+    f->stp = f->stp / 2.0 + (double)1e-3f;
+    inf.accepted = 0;
+  } else {
+    double mb;
+    TRY(qd_mbpt2(f->HS, &mb));
+    f->crit = std::fabs(mb);
+    f->E0 = E0;
+    f->iteration += 1;
+    inf.accepted = 1;
+  }
+  inf.converged = f->crit <= kConvCriteria ? 1 : 0;
+  if (info) *info = inf;
+  return QD_OK;
+}
+
+int qd_flow_omega(const qd_flow* f, qd_op** G) {
+  CHECK(f && G, QD_ERR_ARG, "qd_flow_omega: null argument");
+  *G = f->G;
+  return QD_OK;
+}
+
+int qd_flow_state(const qd_flow* f, qd_flow_result* r) {
+  CHECK(f && r, QD_ERR_ARG, "qd_flow_state: null argument");
+  r->E0 = f->E0;
+  r->s = f->s;
+  r->iterations = f->iteration;
+  r->rejected = f->rejected;
+  r->commutators = f->comms;
+  r->rows = f->rows;
+  return QD_OK;
+}
+
+int qd_flow_destroy(qd_flow* f) {
+  if (!f) return QD_OK;
+  cudaSetDevice(f->L->device);
+  cudaStreamSynchronize(f->L->stream);
+  (void)cudaGetLastError();
+  delete f;  // the workspaces stay with the layout
+  return QD_OK;
+}
+
+int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, double* trace,
+                   qd_flow_result* result) {
+  qd_flow* f = nullptr;
+  TRY(qd_flow_create(HAM, HS, flags, &f));
+  int rc = QD_OK, loops = 0;
+  while (f->crit > kConvCriteria) {
+    if (loops++ >= max_iter) {
+      qd::set_error("qd_magnus_flow: not converged after %d steps (crit %.3e)", max_iter, f->crit);
+      rc = QD_ERR_NOCONV;
+      break;
+    }
+    qd_flow_step_info inf;
+    if ((rc = qd_flow_step(f, &inf))) break;
+    const int row = f->rows - 1;
+    if (trace && row < max_iter) {
+      double* t = trace + 7 * row;
+      t[0] = f->iteration - inf.accepted; t[1] = inf.s; t[2] = inf.E0; t[3] = inf.nrm1; t[4] = inf.nrm2;
+      t[5] = inf.crit; t[6] = inf.accepted ? inf.terms : -inf.terms;
+    }
+  }
+  if (result) qd_flow_state(f, result);
+  std::string msg = rc ? qd::last_error() : std::string();
+  qd_flow_destroy(f);
+  if (rc) qd::set_error("%s", msg.c_str());
+  return rc;
+}
+
+int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, unsigned flags, int max_iter,
+                         qd_flow_result* results, int* status) {
+  CHECK(count >= 0, QD_ERR_ARG, "qd_magnus_flow_batch: negative count");
+  if (count == 0) return QD_OK;
+  CHECK(HAM && HS && results && status, QD_ERR_ARG, "qd_magnus_flow_batch: null argument");
+  for (int i = 0; i < count; ++i) {
+    CHECK(HAM[i] && HS[i], QD_ERR_ARG, "qd_magnus_flow_batch: null operator %d", i);
+    for (int j = 0; j < i; ++j)
+      CHECK(HAM[i]->L != HAM[j]->L, QD_ERR_ARG,
+            "qd_magnus_flow_batch: instances %d and %d share a layout (one stream per instance)", j, i);
+  }
+  // one host thread per instance; each flow runs on its own layout's stream,
+  // so the instances' kernels run concurrently on the device
+  std::vector<std::string> msg(count);
+  std::vector<std::thread> th;
+  th.reserve(count);
+  for (int i = 0; i < count; ++i)
+    th.emplace_back([&, i]() {
+      std::memset(&results[i], 0, sizeof(qd_flow_result));
+      status[i] = qd_magnus_flow(HAM[i], HS[i], flags, max_iter, nullptr, &results[i]);
+      if (status[i] != QD_OK) msg[i] = qd::last_error();
+    });
+  for (auto& t : th) t.join();
+  for (int i = 0; i < count; ++i)
+    if (status[i] != QD_OK) {
+      qd::set_error("qd_magnus_flow_batch: instance %d: %s", i, msg[i].c_str());
+      return status[i];
+    }
   return QD_OK;
 }
 

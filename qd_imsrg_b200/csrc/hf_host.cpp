@@ -32,6 +32,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <tuple>
 #include <vector>
 #ifdef _OPENMP
@@ -714,6 +716,41 @@ extern "C" int qd_tbme_write(int emax, const char* path, int nthreads, unsigned 
   return write_mebin(T, path);
 }
 
+namespace qd {
+namespace {
+// The TBMEs depend only on (emax, options) and are computed at hbar-omega = 1
+// (HF scales them by sqrt(hw)): keep the last two sets, so that a grid of
+// (N, hbar-omega) instances computes each set once.
+struct TbmeCache {
+  std::mutex mu;
+  std::vector<std::pair<std::pair<int, unsigned>, std::shared_ptr<const TBME>>> sets;
+};
+TbmeCache& tbme_cache() {
+  static TbmeCache c;
+  return c;
+}
+int cached_tbme(int emax, unsigned options, int nthreads, std::shared_ptr<const TBME>* out) {
+  TbmeCache& c = tbme_cache();
+  {
+    std::lock_guard<std::mutex> lock(c.mu);
+    for (auto& e : c.sets)
+      if (e.first == std::make_pair(emax, options)) {
+        *out = e.second;
+        return QD_OK;
+      }
+  }
+  auto T = std::make_shared<TBME>();
+  int rc = build_tbme(emax, *T, nthreads, options);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(c.mu);
+  c.sets.push_back({{emax, options}, T});
+  if (c.sets.size() > 2) c.sets.erase(c.sets.begin());
+  *out = T;
+  return QD_OK;
+}
+}  // namespace
+}  // namespace qd
+
 extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* mebin, int nthreads, double mix,
                                  unsigned options, double* eig_out, double* vec_out, int64_t neq, int* iterations) {
   if (nbody < 0 || emax < 1 || !eig_out || !vec_out || !(mix > 0.0 && mix <= 1.0) || (options & ~QD_TBME_QUAD)) {
@@ -721,9 +758,16 @@ extern "C" int qd_hf_hamiltonian(int nbody, int emax, double hw, const char* meb
     return QD_ERR_ARG;
   }
   const int nt = nthreads > 0 ? nthreads : 1;
-  TBME T;
-  int rc = mebin ? read_mebin(mebin, emax, T) : build_tbme(emax, T, nt, options);
-  if (rc) return rc;
+  std::shared_ptr<const TBME> Tp;
+  int rc;
+  if (mebin) {
+    auto t = std::make_shared<TBME>();
+    if ((rc = read_mebin(mebin, emax, *t))) return rc;
+    Tp = t;
+  } else if ((rc = cached_tbme(emax, options, nt, &Tp))) {
+    return rc;
+  }
+  const TBME& T = *Tp;
   HFResult R;
   if ((rc = run_hf(nbody, emax, hw, T, R, nt, mix))) return rc;
   qd_layout L;

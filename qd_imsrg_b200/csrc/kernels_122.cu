@@ -21,12 +21,14 @@
 // F table: group-diagonal one-body reads) are shared by TJ lanes and the
 // shared-memory reads of one row group are contiguous.
 #include <algorithm>
+#include <mutex>
 
 #include "dev_common.cuh"
 
 namespace qd {
 
 constexpr int T122 = 512;  // threads per CTA
+constexpr size_t SMEM_MAX_ATTR_122 = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 // TJ: columns (bra pass) / rows (ket pass) staged per CTA; a warp handles
 // 32/TJ rows (bra) or columns (ket) at a time, TJ lanes each.
 
@@ -48,13 +50,20 @@ __device__ __forceinline__ int off_of(int c, int4 bd) { return c == 0 ? 0 : (c =
 __device__ __forceinline__ int cnt_of(int c, int4 bd) { return c == 0 ? bd.x : (c == 1 ? bd.y : bd.z); }
 __device__ __forceinline__ int cls_of(int P, int nh, int nb) { return P < nh ? 0 : (P < nh + nb ? 1 : 2); }
 
-// V(P1, P2) of one operator for block q, any classes (upper via herm)
-__device__ __forceinline__ double vfull(const double* __restrict__ op, const i64* o, int4 bd, double herm, int P1,
-                                        int P2) {
+// V(P1, P2) of one operator for block q, any classes (upper via herm); parts
+// set in zmask are known to be zero and not read
+__device__ __forceinline__ double vfull(const double* __restrict__ op, const i64* o, int4 bd, double herm,
+                                        unsigned zmask, int P1, int P2) {
   int c1 = cls_of(P1, bd.x, bd.y), c2 = cls_of(P2, bd.x, bd.y);
   int r1 = P1 - off_of(c1, bd), r2 = P2 - off_of(c2, bd);
-  if (c1 >= c2) return op[__ldg(o + slot_of(c1, c2)) + r1 + (i64)r2 * cnt_of(c1, bd)];
-  return herm * op[__ldg(o + slot_of(c2, c1)) + r2 + (i64)r1 * cnt_of(c2, bd)];
+  if (c1 >= c2) {
+    const int sl = slot_of(c1, c2);
+    if ((zmask >> (P_HHHH + sl)) & 1u) return 0.0;
+    return op[__ldg(o + sl) + r1 + (i64)r2 * cnt_of(c1, bd)];
+  }
+  const int sl = slot_of(c2, c1);
+  if ((zmask >> (P_HHHH + sl)) & 1u) return 0.0;
+  return herm * op[__ldg(o + sl) + r2 + (i64)r1 * cnt_of(c2, bd)];
 }
 
 // Leg-table entry (static per layout), for pair P = (x1<x2) of a block:
@@ -123,8 +132,9 @@ template <int TJ>
 __global__ void __launch_bounds__(T122) k_122_bra(DevLayout L, const Task122* __restrict__ tasks,
                                                   const int* __restrict__ legstart, const int* __restrict__ legs,
                                                   const double2* __restrict__ Ftab, int gmax,
-                                                  const double* __restrict__ A, double hA,
-                                                  const double* __restrict__ B, double hB, double* __restrict__ C) {
+                                                  const double* __restrict__ A, double hA, unsigned zA,
+                                                  const double* __restrict__ B, double hB, unsigned zB,
+                                                  double* __restrict__ C) {
   extern __shared__ double2 smv[];  // (VA, VB) of each (row, column)
   const Task122 tk = tasks[blockIdx.x];
   const int q = tk.q, c2 = tk.cls;
@@ -138,8 +148,8 @@ __global__ void __launch_bounds__(T122) k_122_bra(DevLayout L, const Task122* __
     double va = 0.0, vb = 0.0;
     if (j < ncol) {
       int P2 = offc2 + tk.first + j;
-      va = vfull(A, o, bd, hA, P1, P2);
-      vb = vfull(B, o, bd, hB, P1, P2);
+      va = vfull(A, o, bd, hA, zA, P1, P2);
+      vb = vfull(B, o, bd, hB, zB, P1, P2);
     }
     smv[P1 * TJ + j] = make_double2(va, vb);
   }
@@ -166,8 +176,9 @@ template <int TJ>
 __global__ void __launch_bounds__(T122) k_122_ket(DevLayout L, const Task122* __restrict__ tasks,
                                                   const int* __restrict__ legstart, const int* __restrict__ legs,
                                                   const double2* __restrict__ Ftab, int gmax,
-                                                  const double* __restrict__ A, double hA,
-                                                  const double* __restrict__ B, double hB, double* __restrict__ C) {
+                                                  const double* __restrict__ A, double hA, unsigned zA,
+                                                  const double* __restrict__ B, double hB, unsigned zB,
+                                                  double* __restrict__ C) {
   extern __shared__ double2 smv[];
   const Task122 tk = tasks[blockIdx.x];
   const int q = tk.q, c1 = tk.cls;
@@ -182,8 +193,8 @@ __global__ void __launch_bounds__(T122) k_122_ket(DevLayout L, const Task122* __
     double va = 0.0, vb = 0.0;
     if (i < nrow) {
       int P1 = offc1 + tk.first + i;
-      va = vfull(A, o, bd, hA, P1, P2);
-      vb = vfull(B, o, bd, hB, P1, P2);
+      va = vfull(A, o, bd, hA, zA, P1, P2);
+      vb = vfull(B, o, bd, hB, zB, P1, P2);
     }
     smv[P2 * TJ + i] = make_double2(va, vb);
   }
@@ -230,9 +241,13 @@ std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
   return m;
 }
+// plans of different layouts are built and dropped from concurrent host
+// threads (batched flows); map nodes stay put, so a found plan needs no lock
+std::mutex g_plan_mutex;
 }  // namespace
 
 static int plan_122(qd_layout* L, Plan122** out) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
   auto it = plans().find(L);
   if (it != plans().end()) {
     *out = &it->second;
@@ -303,7 +318,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
     bk.first = (int)hb.size();
     bk.count = (int)v.size();
     bk.smem = sizeof(double2) * (size_t)bmax * bk.tj;
-    if (bk.smem > 227 * 1024) {
+    if (bk.smem > SMEM_MAX_ATTR_122) {
       set_error("commutator_122: block of %d pairs exceeds shared memory", bmax);
       return QD_ERR_ARG;
     }
@@ -326,15 +341,14 @@ static int plan_122(qd_layout* L, Plan122** out) {
   if (!legs.empty()) QD_CUDA(cudaMemcpy(p.d_legs, legs.data(), legs.size() * sizeof(int), cudaMemcpyHostToDevice));
   QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)L->m * p.gmax));
   L->ws_bytes += (i64)(legstart.size() + legs.size()) * 4 + (i64)sizeof(double) * 4 * L->m * p.gmax;
-  size_t s8 = 0, s4 = 0;
-  for (auto& b : p.buckets) (b.tj == 8 ? s8 : s4) = std::max(b.tj == 8 ? s8 : s4, b.smem);
-  if (s8) {
-    QD_CUDA(cudaFuncSetAttribute(k_122_bra<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8));
-    QD_CUDA(cudaFuncSetAttribute(k_122_ket<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8));
-  }
-  if (s4) {
-    QD_CUDA(cudaFuncSetAttribute(k_122_bra<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4));
-    QD_CUDA(cudaFuncSetAttribute(k_122_ket<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4));
+  // the attribute is process-wide: set it to the device limit, so that plans
+  // built concurrently for other layouts can never lower it below a need
+  if (!p.buckets.empty()) {
+    const int lim = (int)SMEM_MAX_ATTR_122;
+    QD_CUDA(cudaFuncSetAttribute(k_122_bra<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    QD_CUDA(cudaFuncSetAttribute(k_122_ket<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    QD_CUDA(cudaFuncSetAttribute(k_122_bra<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    QD_CUDA(cudaFuncSetAttribute(k_122_ket<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
   }
   plans()[L] = p;
   *out = &plans()[L];
@@ -342,6 +356,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
 }
 
 void drop_122_plan(const qd_layout* L) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
   auto it = plans().find(L);
   if (it == plans().end()) return;
   for (void* ptr : {(void*)it->second.d_bra, (void*)it->second.d_ket, (void*)it->second.d_legstart,
@@ -362,20 +377,24 @@ int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
     const Task122* tb = p->d_bra + b.first;
     if (b.tj == 8)
       k_122_bra<8><<<b.count, T122, b.smem, L->stream>>>(L->dev, tb, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, B->d, (double)B->herm, C);
+                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
+                                                          B->zero_mask, C);
     else
       k_122_bra<4><<<b.count, T122, b.smem, L->stream>>>(L->dev, tb, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, B->d, (double)B->herm, C);
+                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
+                                                          B->zero_mask, C);
     ++L->nlaunch;
   }
   for (const Bucket122& b : p->buckets) {
     const Task122* tk = p->d_ket + b.first;
     if (b.tj == 8)
       k_122_ket<8><<<b.count, T122, b.smem, L->stream>>>(L->dev, tk, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, B->d, (double)B->herm, C);
+                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
+                                                          B->zero_mask, C);
     else
       k_122_ket<4><<<b.count, T122, b.smem, L->stream>>>(L->dev, tk, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, B->d, (double)B->herm, C);
+                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
+                                                          B->zero_mask, C);
     ++L->nlaunch;
   }
   L->nlaunch += 1;

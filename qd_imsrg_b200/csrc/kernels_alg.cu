@@ -191,6 +191,78 @@ int reduce_norm_full(qd_layout* L, const double* a, double* dout) {
   return QD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// One BCH_EXPAND term update in one pass (magnus_IMSRG.f90:298-316):
+//   c = sa*a + sb*b  (add_arrays, bit-identical: no FMA contraction)
+// together with the norms of both inputs, |a| = |INT1| (HS before the update)
+// and |b| = |INT2|, over the one-body parts (mat_2_norm) or over every stored
+// entry but E0 (full).  Fixed grid and fixed element -> thread assignment:
+// deterministic.  Partial sums: 4 per CTA (a 1-body, a rest, b 1-body, b rest).
+// ---------------------------------------------------------------------------
+constexpr int AXN_BLOCKS = 4 * 148, AXN_THREADS = 256;
+
+__global__ void __launch_bounds__(AXN_THREADS) k_axpy_norms(const double* __restrict__ a, double sa,
+                                                            const double* __restrict__ b, double sb,
+                                                            double* __restrict__ c, i64 n, i64 o1, i64 e1,
+                                                            double* __restrict__ partial) {
+  __shared__ double sh[AXN_THREADS / 32];
+  double a1 = 0.0, a2 = 0.0, b1 = 0.0, b2 = 0.0;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double x = a[i], y = b[i];
+    c[i] = __dadd_rn(__dmul_rn(sa, x), __dmul_rn(sb, y));
+    if (i >= o1) {
+      if (i < e1) {
+        a1 += x * x;
+        b1 += y * y;
+      } else {
+        a2 += x * x;
+        b2 += y * y;
+      }
+    }
+  }
+  a1 = block_sum<AXN_THREADS>(a1, sh);
+  a2 = block_sum<AXN_THREADS>(a2, sh);
+  b1 = block_sum<AXN_THREADS>(b1, sh);
+  b2 = block_sum<AXN_THREADS>(b2, sh);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = a1;
+    partial[gridDim.x + blockIdx.x] = a2;
+    partial[2 * gridDim.x + blockIdx.x] = b1;
+    partial[3 * gridDim.x + blockIdx.x] = b2;
+  }
+}
+
+// out[0] = |a|, out[1] = |b| (one-body only, or one- plus two-body)
+__global__ void k_axpy_norms_final(const double* __restrict__ partial, int np, int full, double* __restrict__ out) {
+  __shared__ double sh[RED_THREADS / 32];
+  double v[4];
+  for (int k = 0; k < 4; ++k) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[k * np + i];
+    v[k] = block_sum<RED_THREADS>(s, sh);
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sqrt(full ? v[0] + v[1] : v[0]);
+    out[1] = sqrt(full ? v[2] + v[3] : v[2]);
+  }
+}
+
+int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, int full,
+                      double* dout2) {
+  if (!L->d_axn) {
+    QD_CUDA(cudaMalloc(&L->d_axn, sizeof(double) * 4 * AXN_BLOCKS));
+    L->ws_bytes += sizeof(double) * 4 * AXN_BLOCKS;
+  }
+  const i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
+  k_axpy_norms<<<AXN_BLOCKS, AXN_THREADS, 0, L->stream>>>(a, sa, b, sb, c, L->neq, L->o_fhh, L->o_fhh + n1,
+                                                          L->d_axn);
+  k_axpy_norms_final<<<1, RED_THREADS, 0, L->stream>>>(L->d_axn, AXN_BLOCKS, full, dout2);
+  L->nlaunch += 2;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
 // mat_2_norm: one-body parts only, sqrt taken on the device
 int reduce_norm1b(qd_layout* L, const double* a, double* dout) {
   i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;

@@ -1,13 +1,14 @@
-// kernels_body.cu -- the v_elem-driven contractions of the commutator:
-// commutator_121, the trace part of commutator_221 and commutator_122.
+// kernels_body.cu -- the v_elem-driven one-body contractions of the
+// commutator: commutator_121 and the trace part of commutator_221.
+#include <vector>
+
 #include "dev_common.cuh"
 
 namespace qd {
 
 // one-body target t in vectorize order of the one-body part:
 //   fhh(x,y) n*n, then fpp n_p*n_p, then fph n_p*n  -> (x,y) as 0-based states
-__device__ __forceinline__ void decode1b(const DevLayout& L, i64 t, int& x, int& y) {
-  const int n = L.n, mp = L.mp;
+__host__ __device__ inline void decode1b(int n, int mp, i64 t, int& x, int& y) {
   i64 nhh = (i64)n * n, npp = (i64)mp * mp;
   if (t < nhh) {
     x = (int)(t % n);
@@ -31,19 +32,33 @@ __device__ __forceinline__ void decode1b(const DevLayout& L, i64 t, int& x, int&
 // VB(a,x,i,y) is non-zero only for (i hole, a particle) with
 // ml_i - ml_a = ml_x - ml_y (and ms alike): the (hole, particle) column list
 // of cross-coupled block ccmap(x,y); VB(i,x,a,y) needs the block ccmap(y,x).
+// Every term carries a factor fph(a,i) of A or B; a cross-coupled block in
+// which both are zero (for operators that conserve (m_l, m_s): every block
+// but Delta m_l = Delta m_s = 0) adds exact zeros and is skipped (ccflag).
 // ---------------------------------------------------------------------------
+__global__ void k_ccflag(DevLayout L, const double* __restrict__ A, const double* __restrict__ B,
+                         int* __restrict__ flag) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;  // (hole i, particle a) = (e % n, n + e / n)
+  if (e >= L.n * L.mp) return;
+  const int i = e % L.n, a = L.n + e / L.n;
+  const i64 f = L.o_fph + (a - L.n) + (i64)i * L.mp;
+  if (A[f] != 0.0 || B[f] != 0.0) flag[__ldg(&L.ccmap[i * L.m + a]).x] = 1;
+}
+
 __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, const double* __restrict__ B, double hB,
-                      double* __restrict__ C) {
+                      const int* __restrict__ flag, double* __restrict__ C) {
   const i64 n1 = (i64)L.n * L.n + (i64)L.mp * L.mp + (i64)L.mp * L.n;
   i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n1) return;
   int x, y;
-  decode1b(L, t, x, y);
+  decode1b(L.n, L.mp, t, x, y);
   const int n = L.n, mp = L.mp;
+  const int q1 = __ldg(&L.ccmap[x * L.m + y]).x, q2 = __ldg(&L.ccmap[y * L.m + x]).x;
+  const bool on1 = __ldg(flag + q1) != 0, on2 = __ldg(flag + q2) != 0;
+  if (!on1 && !on2) return;
   double s = 0.0;
-  {
-    int q = __ldg(&L.ccmap[x * L.m + y]).x;
-    int base = __ldg(&L.cchp_base[q]), nb = __ldg(&L.ccdim[q]).y;
+  if (on1) {
+    int base = __ldg(&L.cchp_base[q1]), nb = __ldg(&L.ccdim[q1]).y;
     for (int k = 0; k < nb; ++k) {
       int2 ia = __ldg(&L.cchp[base + k]);
       const int i = ia.x, a = ia.y;
@@ -51,9 +66,8 @@ __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, cons
       s += fa * hA * dv_elem(L, B, hB, a, x, i, y) - fb * hB * dv_elem(L, A, hA, a, x, i, y);
     }
   }
-  {
-    int q = __ldg(&L.ccmap[y * L.m + x]).x;
-    int base = __ldg(&L.cchp_base[q]), nb = __ldg(&L.ccdim[q]).y;
+  if (on2) {
+    int base = __ldg(&L.cchp_base[q2]), nb = __ldg(&L.ccdim[q2]).y;
     for (int k = 0; k < nb; ++k) {
       int2 ia = __ldg(&L.cchp[base + k]);
       const int i = ia.x, a = ia.y;
@@ -65,12 +79,23 @@ __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, cons
 }
 
 int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
-  i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
-  if (n1 > 0) {
-    k_121<<<(unsigned)((n1 + 127) / 128), 128, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d, (double)B->herm,
-                                                               C);
+  const i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
+  if (n1 == 0 || L->ncc == 0) return QD_OK;
+  if (!L->d_ccflag) {
+    void* p = nullptr;
+    QD_CUDA(cudaMalloc(&p, sizeof(int) * L->ncc));
+    L->dev_allocs.push_back(p);
+    L->d_ccflag = (int*)p;
+  }
+  QD_CUDA(cudaMemsetAsync(L->d_ccflag, 0, sizeof(int) * L->ncc, L->stream));
+  const int nhp = L->n * L->mp;
+  if (nhp > 0) {
+    k_ccflag<<<(nhp + 255) / 256, 256, 0, L->stream>>>(L->dev, A->d, B->d, L->d_ccflag);
     ++L->nlaunch;
   }
+  k_121<<<(unsigned)((n1 + 127) / 128), 128, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d, (double)B->herm,
+                                                             L->d_ccflag, C);
+  ++L->nlaunch;
   QD_CUDA(cudaGetLastError());
   return QD_OK;
 }
@@ -88,7 +113,7 @@ __global__ void k_221_trace(DevLayout L, double hA, double hB, const double* __r
   i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n1) return;
   int x, y;
-  decode1b(L, t, x, y);
+  decode1b(n, mp, t, x, y);
   if (__ldg(&L.gid[x]) != __ldg(&L.gid[y])) return;
   double s = 0.0;
   if (t < nhh) {  // fhh(h,h2): x = h, y = h2
@@ -109,6 +134,163 @@ int launch_221_trace(qd_layout* L, const qd_op* A, const qd_op* B, const qd_op* 
   if (n1 > 0) {
     k_221_trace<<<(unsigned)((n1 + 127) / 128), 128, 0, L->stream>>>(L->dev, (double)A->herm, (double)B->herm, w1->d,
                                                                      (double)w1->herm, w2->d, (double)w2->herm, C);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// commutator_221 without its intermediates.  The trace above reads w1 and
+// w2 (herm +1, as allocate_everything leaves them) only at
+//   fhh: w1 hhhh (i legs), w2 phph (a legs);  fpp: w1 phph, w1 pppp;
+//   fph: w2/w1 phhh (i legs), w2/w1 ppph (a legs),
+// and each stored element of those parts is one column dot product of the
+// products commutator_221 forms (src/commutators.f90:211-278):
+//   w1 hhhh = Bpphh^T Apphh   w1 pppp = Apphh Bpphh^T   w1 phph = Bppph^T Appph
+//   w2 phph = Aphhh Bphhh^T   w1 phhh = Bppph^T Apphh   w2 phhh = Appph^T Bpphh
+//   w1 ppph = Apphh Bphhh^T   w2 ppph = Bpphh Aphhh^T
+// k_221_fused evaluates exactly those elements on the fly (one CTA per
+// target whose states share (m_l, m_s); threads over the hole/particle leg,
+// fixed-order block sum), so the w1/w2 products and their memsets (2 x 8 neq
+// bytes written per commutator) disappear.  Used by the full commutator;
+// qd_commutator_221 keeps the reference's visible w1/w2.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double w221_stored(const DevLayout& L, int which, int q, int sl, int r, int c,
+                                              const double* __restrict__ A, const double* __restrict__ B) {
+  const int4 bd = __ldg(&L.blk[q]);
+  const int nh = bd.x, nb = bd.y, np = bd.z;
+  const i64* o = L.boff + 6 * q;
+  double s = 0.0;
+  // slots: 0 hhhh, 1 pppp, 2 pphh, 3 phph, 4 ppph, 5 phhh
+  if (which == 1) {
+    switch (sl) {
+      case 0: {  // Bpphh^T Apphh
+        const double* u = B + __ldg(o + 2) + (i64)r * np;
+        const double* v = A + __ldg(o + 2) + (i64)c * np;
+        for (int k = 0; k < np; ++k) s += u[k] * v[k];
+        break;
+      }
+      case 1: {  // Apphh Bpphh^T
+        const double* u = A + __ldg(o + 2) + r;
+        const double* v = B + __ldg(o + 2) + c;
+        for (int k = 0; k < nh; ++k) s += u[(i64)k * np] * v[(i64)k * np];
+        break;
+      }
+      case 3: {  // Bppph^T Appph
+        const double* u = B + __ldg(o + 4) + (i64)r * np;
+        const double* v = A + __ldg(o + 4) + (i64)c * np;
+        for (int k = 0; k < np; ++k) s += u[k] * v[k];
+        break;
+      }
+      case 5: {  // Bppph^T Apphh
+        const double* u = B + __ldg(o + 4) + (i64)r * np;
+        const double* v = A + __ldg(o + 2) + (i64)c * np;
+        for (int k = 0; k < np; ++k) s += u[k] * v[k];
+        break;
+      }
+      case 4: {  // Apphh Bphhh^T
+        const double* u = A + __ldg(o + 2) + r;
+        const double* v = B + __ldg(o + 5) + c;
+        for (int k = 0; k < nh; ++k) s += u[(i64)k * np] * v[(i64)k * nb];
+        break;
+      }
+      default: break;
+    }
+  } else {
+    switch (sl) {
+      case 3: {  // Aphhh Bphhh^T
+        const double* u = A + __ldg(o + 5) + r;
+        const double* v = B + __ldg(o + 5) + c;
+        for (int k = 0; k < nh; ++k) s += u[(i64)k * nb] * v[(i64)k * nb];
+        break;
+      }
+      case 5: {  // Appph^T Bpphh
+        const double* u = A + __ldg(o + 4) + (i64)r * np;
+        const double* v = B + __ldg(o + 2) + (i64)c * np;
+        for (int k = 0; k < np; ++k) s += u[k] * v[k];
+        break;
+      }
+      case 4: {  // Bpphh Aphhh^T
+        const double* u = B + __ldg(o + 2) + r;
+        const double* v = A + __ldg(o + 5) + c;
+        for (int k = 0; k < nh; ++k) s += u[(i64)k * np] * v[(i64)k * nb];
+        break;
+      }
+      default: break;
+    }
+  }
+  return s;
+}
+
+// v_elem(w, a, b, c, d) of intermediate w (herm +1) through w221_stored
+__device__ __forceinline__ double w221(const DevLayout& L, int which, const double* __restrict__ A,
+                                       const double* __restrict__ B, int a, int b, int c, int d) {
+  if (a == b || c == d) return 0.0;
+  const int e1 = __ldg(&L.ptab[a * L.m + b]);
+  const int e2 = __ldg(&L.ptab[c * L.m + d]);
+  const int q = pt_blk(e1);
+  if (q != pt_blk(e2)) return 0.0;
+  const double sgn = (pt_swap(e1) ^ pt_swap(e2)) ? -1.0 : 1.0;
+  int c1 = pt_cls(e1), c2 = pt_cls(e2), i1 = pt_idx(e1), i2 = pt_idx(e2);
+  if (c1 < c2) {  // upper class: herm (+1) times the transposed stored element
+    int t = c1; c1 = c2; c2 = t;
+    t = i1; i1 = i2; i2 = t;
+  }
+  int sl;
+  if (c1 == 0) sl = 0;
+  else if (c1 == 1) sl = c2 == 0 ? 5 : 3;
+  else sl = c2 == 0 ? 2 : (c2 == 1 ? 4 : 1);
+  return sgn * w221_stored(L, which, q, sl, i1, i2, A, B);
+}
+
+constexpr int T221 = 128;
+
+__global__ void __launch_bounds__(T221) k_221_fused(DevLayout L, const int* __restrict__ targets, double hA,
+                                                    double hB, const double* __restrict__ A,
+                                                    const double* __restrict__ B, double* __restrict__ C) {
+  __shared__ double sh[T221 / 32];
+  const int n = L.n, mp = L.mp, m = L.m;
+  const i64 nhh = (i64)n * n, npp = (i64)mp * mp;
+  const i64 t = __ldg(targets + blockIdx.x);
+  int x, y;
+  decode1b(n, mp, t, x, y);
+  double s = 0.0;
+  for (int u = threadIdx.x; u < m; u += T221) {
+    if (t < nhh) {  // fhh(h,h2): x = h, y = h2
+      if (u < n) s += hA * w221(L, 1, A, B, u, y, u, x) - hB * w221(L, 1, A, B, u, x, u, y);
+      else s += -hA * w221(L, 2, A, B, u, y, u, x) + hB * w221(L, 2, A, B, u, x, u, y);
+    } else if (t < nhh + npp) {  // fpp(p,p2)
+      if (u < n) s += hA * w221(L, 1, A, B, u, y, u, x) - hB * w221(L, 1, A, B, u, x, u, y);
+      else s += -hA * w221(L, 1, A, B, u, y, u, x) + hB * w221(L, 1, A, B, u, x, u, y);
+    } else {  // fph(p,h)
+      if (u < n) s += hA * w221(L, 2, A, B, u, x, u, y) - hB * w221(L, 1, A, B, u, x, u, y);
+      else s += -hA * w221(L, 2, A, B, u, x, u, y) + hB * w221(L, 1, A, B, u, x, u, y);
+    }
+  }
+  s = block_sum<T221>(s, sh);
+  if (threadIdx.x == 0) C[L.o_fhh + t] += s;
+}
+
+int launch_221_fused(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
+  if (L->ntgt221 < 0) {  // targets whose two states share (m_l, m_s)
+    std::vector<int> tg;
+    const i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
+    for (i64 t = 0; t < n1; ++t) {
+      int x, y;
+      decode1b(L->n, L->mp, t, x, y);
+      if (L->gid[x] == L->gid[y]) tg.push_back((int)t);
+    }
+    void* p = nullptr;
+    QD_CUDA(cudaMalloc(&p, sizeof(int) * std::max<size_t>(1, tg.size())));
+    L->dev_allocs.push_back(p);
+    if (!tg.empty()) QD_CUDA(cudaMemcpy(p, tg.data(), sizeof(int) * tg.size(), cudaMemcpyHostToDevice));
+    L->d_tgt221 = (const int*)p;
+    L->ntgt221 = (int)tg.size();
+  }
+  if (L->ntgt221 > 0) {
+    k_221_fused<<<L->ntgt221, T221, 0, L->stream>>>(L->dev, L->d_tgt221, (double)A->herm, (double)B->herm, A->d,
+                                                   B->d, C);
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());

@@ -300,10 +300,15 @@ void layout_free_device(qd_layout* L) {
   L->prog_pandya.clear_device();
   if (L->d_z) cudaFree(L->d_z);
   if (L->d_red) cudaFree(L->d_red);
+  if (L->d_axn) cudaFree(L->d_axn);
+  L->d_axn = nullptr;
   if (L->h_red) cudaFreeHost(L->h_red);
   L->d_z = nullptr;
   L->d_red = nullptr;
   L->h_red = nullptr;
+  L->d_ccflag = nullptr;  // in dev_allocs
+  L->d_tgt221 = nullptr;
+  L->ntgt221 = -1;
   if (L->own_stream && L->stream) cudaStreamDestroy(L->stream);
   L->stream = nullptr;
 }

@@ -120,6 +120,8 @@ struct StageProf {
 
 struct qd_layout {
   int device = 0;
+  int children = 0;      // live operators and cross-coupled matrices on this layout
+  bool closing = false;  // qd_layout_destroy was called while children were alive
   qd::StageProf prof;
   long long nlaunch = 0;  // kernels this library launched for the layout
   int n = 0, m = 0, mp = 0, emax = 0, nblock = 0, ncc = 0, mlmax = 0;
@@ -146,6 +148,10 @@ struct qd_layout {
   double* d_z = nullptr;          // Pandya products, zsize doubles
   double* d_red = nullptr;        // reduction partials
   double* h_red = nullptr;        // pinned scalar results
+  double* d_axn = nullptr;        // partial sums of the fused BCH update (axpy + norms)
+  int* d_ccflag = nullptr;        // per cross-coupled block: fph of A or B non-zero (121)
+  const int* d_tgt221 = nullptr;  // one-body targets whose states share (m_l, m_s) (fused 221)
+  int ntgt221 = -1;
   qd::i64 ws_bytes = 0;
   // GEMM programs
   qd::GemmProgram prog_ladder, prog_221, prog_111, prog_pandya;
@@ -189,6 +195,8 @@ i64 part_count(const qd_layout* L, int part);  // total elements of a part over 
 
 // kernels (kernels_*.cu)
 int launch_axpy(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, i64 n);
+int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, int full,
+                      double* dout2);
 int reduce_dot_range(qd_layout* L, const double* a, const double* b, i64 o, i64 n, double scale, double add,
                      double* dout);
 int reduce_dot_part(qd_layout* L, const double* a, const double* b, int part, double scale, double add, double* dout);
@@ -200,6 +208,7 @@ double* red_slot(qd_layout* L, int k);
 int launch_white(qd_layout* L, double* gen, const double* h, int herm);
 int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
 int launch_221_trace(qd_layout* L, const qd_op* A, const qd_op* B, const qd_op* w1, const qd_op* w2, double* C);
+int launch_221_fused(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
 int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
 int launch_calc_cc(qd_layout* L, const qd_op* H, double* X);
 int launch_pandya_gather(qd_layout* L, const double* Z, double* C);

@@ -122,3 +122,20 @@ def test_magnus_without_cc_drops_particle_hole_channel():
     nb1 = 1 + n * n + mp * mp + mp * n
     assert np.abs(d[:nb1]).max() == 0.0
     assert np.abs(d[nb1:]).max() > 1e-3
+
+
+def test_block_sampler_phases_make_the_whole_commutator():
+    # the CPU baseline times phases of oracle.Sampler; without the Pandya
+    # channel the phases together are exactly one commutator (with it, each
+    # phase forms only its own cross-coupled products: the same work, split)
+    L = oracle.Layout(6, 5)
+    rng = np.random.default_rng(17)
+    a, b = numpy_random_op(L, -1, rng), numpy_random_op(L, 1, rng)
+    A, B = oracle.Op(L, -1, a), oracle.Op(L, 1, b)
+    full = oracle.Op(L, 1)
+    oracle.commutator(A, B, full, pandya=False)
+    samp = oracle.Op(L, 1)
+    S = oracle.Sampler(A)
+    for ph in range(3):
+        S.run(A, B, samp, 3, ph, pandya=False)
+    compare_parts(L, samp.get(), full.get(), rtol=1e-13, atol=1e-15)
