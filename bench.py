@@ -63,7 +63,12 @@ def parse():
     ap.add_argument("--ref-stride", type=int, default=8)
     ap.add_argument("--cpu-phases", type=int, default=2, help="block-sampled phases timed for the CPU baseline")
     ap.add_argument("--batch-max-iter", type=int, default=300, help="batch: flow step limit per instance")
-    ap.add_argument("--workload", choices=["flow", "commutator", "batch"], default="flow")
+    ap.add_argument("--ws-train", type=int, default=64, help="warmstart: training draws")
+    ap.add_argument("--ws-eval", type=int, default=16, help="warmstart: held-out draws at N=20, R=20")
+    ap.add_argument("--ws-steps", type=int, default=3000, help="warmstart: Adam steps")
+    ap.add_argument("--ws-sample", type=int, default=4096, help="warmstart: recorded entries per flow")
+    ap.add_argument("--ws-s", type=float, default=0.0, help="warmstart: target s (0: half the median final s)")
+    ap.add_argument("--workload", choices=["flow", "commutator", "batch", "warmstart"], default="flow")
     ap.add_argument("--hw", type=float, default=0.5)
     ap.add_argument("--pandya", action="store_true", help="flow: add the particle-hole channel")
     ap.add_argument("--hf-mix", type=float, default=0.5, help="flow: HF density mixing (1 = plain iteration)")
@@ -547,6 +552,89 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+def run_warmstart(args, world, rank, local):
+    """Learned warm start: train the per-entry network on plain-flow Omega(s)
+    trajectories (hbar-omega ~ U[0.1, 1], N in {12, 20}, R in {16, 20}), then
+    on held-out hbar-omega at N=20, R=20 run the plain flow from Omega = 0
+    (cold) and from the predicted Omega(s_target) (warm)."""
+    import torch
+
+    from qd_imsrg_b200 import warmstart as ws
+
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(2024)
+    t0 = time.perf_counter()
+    Xs, Ts, sfin, trfail = [], [], {}, []
+    for k in range(args.ws_train):
+        nb, R = (12, 20)[k % 2], (16, 20)[(k // 2) % 2]
+        hw = float(rng.uniform(0.1, 1.0))
+        try:
+            inst = ws.Instance(nb, R, hw, device=local, mix=args.hf_mix, quad=args.tbme == "quad")
+        except Exception as e:  # HF failure: the draw is dropped
+            trfail.append({"N": nb, "R": R, "hw": hw, "why": str(e)})
+            continue
+        try:
+            idx, svals, om, res = ws.trajectory(inst, args.ws_sample, rng)
+            X, T = ws.samples(inst, idx, svals, om)
+            Xs.append(X)
+            Ts.append(T)
+            sfin.setdefault((nb, R), []).append(float(res.s))
+        except Exception as e:
+            trfail.append({"N": nb, "R": R, "hw": hw, "why": str(e)})
+        inst.close()
+        torch.cuda.empty_cache()
+    X, T = torch.cat(Xs), torch.cat(Ts)
+    t_data = time.perf_counter() - t0
+    mlp = ws.MLP(local, seed=7)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = ws.train(mlp, X, T, steps=args.ws_steps, batch=8192, lr=1e-3, seed=1, log_every=max(1, args.ws_steps // 10))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    ref_s = sfin.get((20, 20)) or [v for vals in sfin.values() for v in vals] or [20.0]
+    s_target = args.ws_s or 0.5 * float(np.median(ref_s))
+    evals = []
+    for k in range(args.ws_eval):
+        hw = float(rng.uniform(0.1, 1.0))
+        try:
+            inst = ws.Instance(20, 20, hw, device=local, mix=args.hf_mix, quad=args.tbme == "quad")
+        except Exception as e:
+            evals.append({"hw": hw, "why": str(e)})
+            continue
+        try:
+            cold = ws.cold_flow(inst)
+            warm = ws.warm_flow(mlp, inst, s_target)
+            evals.append({"hw": hw, "E_HF": inst.E_HF, "cold": cold, "warm": warm,
+                          "dE": abs(warm["E"] - cold["E"])})
+        except Exception as e:
+            evals.append({"hw": hw, "why": str(e)})
+        inst.close()
+        torch.cuda.empty_cache()
+    ok = [e for e in evals if "cold" in e]
+    if rank == 0:
+        tot = lambda key, side: sum(e[side][key] for e in ok)
+        line = {"metric": "learned warm start: flow seconds, N=20 R=20, held-out hbar-omega (warm vs cold)",
+                "value": tot("seconds", "warm") / max(1, len(ok)), "unit": "s per converged E_gs (warm start)",
+                "n_gpus": world, "steps": len(ok), "warmup": 0, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 flow, bf16/f32 network",
+                "data": "synthetic: Coulomb TBMEs and HF computed on the host; network trained on the plain "
+                        "flow's own Omega(s) trajectories",
+                "config": {"workload": "Magnus flows N=20 R=20 from Omega = 0 and from the network's "
+                                       "Omega(s_target)", "s_target": s_target,
+                           "cold_s_per_flow": tot("seconds", "cold") / max(1, len(ok)),
+                           "speedup": tot("seconds", "cold") / max(1e-30, tot("seconds", "warm")),
+                           "steps_cold": tot("steps", "cold"), "steps_warm": tot("steps", "warm"),
+                           "commutators_cold": tot("commutators", "cold"),
+                           "commutators_warm": tot("commutators", "warm"),
+                           "accepted": sum(1 for e in ok if e["warm"]["accepted"]), "evaluated": len(ok),
+                           "max_abs_dE": max([e["dE"] for e in ok] or [None]),
+                           "train_rows": int(X.shape[0]), "train_draws": len(Xs), "train_failed": trfail,
+                           "data_s": t_data, "train_s": t_train, "loss_history": hist, "per_instance": evals}}
+        print(json.dumps(line, default=float), flush=True)
+    mlp.close()
+    return 0
+
+
 def run_reference_flow(args, world, rank):
     """Reference arm of the flow workload: the oracle on the host cores, per
     step a bounded sample (block-sampled phases of the flow's commutator),
@@ -586,8 +674,8 @@ def run_reference_flow(args, world, rank):
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
-    if args.workload in ("flow", "batch") and args.impl == "ours":
-        rc = (run_flow if args.workload == "flow" else run_batch)(args, world, rank, local)
+    if args.workload in ("flow", "batch", "warmstart") and args.impl == "ours":
+        rc = {"flow": run_flow, "batch": run_batch, "warmstart": run_warmstart}[args.workload](args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
 

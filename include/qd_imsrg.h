@@ -270,6 +270,34 @@ int qd_flow_destroy(qd_flow* flow);
 int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, unsigned flags, int max_iter,
                          qd_flow_result* results, int* status);
 
+/* ---- learned warm start (no reference counterpart) -------------------------
+ * Omega of the White-generator flow is non-zero only in fph and Vpphh; its
+ * "entries" are fph ((m-n) x n) followed by every block's Vpphh, in vectorize
+ * order.  Device pointers (d_*) are the caller's.                           */
+int qd_omega_count(const qd_layout* L, int64_t* n);
+int qd_omega_gather(const qd_op* G, double* d_out, int64_t n);              /* d_out[e] = entry e of G */
+int qd_omega_scatter(qd_op* G, const float* d_in, float scale, int64_t n);  /* G = 0 but entries scale*d_in */
+/* 16 float features per entry (16-byte aligned rows): energies of the four
+ * legs and their occupations, the H element, hbar-omega, N, the channel
+ * (M_L, M_S), the target flow parameter s, the shells and the entry kind.    */
+int qd_omega_features(const qd_op* H, double hw, double s, float* d_X, int64_t n);
+
+/* The per-entry network 16 -> 256 -> 256 -> 1 (GELU), FP32 master weights,
+ * BF16 operands of the 256-wide layer on the tensor cores, FP32 accumulation.
+ * Parameters: W1[256][16], b1[256], W2[256][256], b2[256], w3[256], b3.
+ * qd_mlp_grad / qd_mlp_train_step: mean squared error over a batch whose size
+ * is a multiple of 32; train_step = grad + one Adam step (lr).              */
+#define QD_MLP_NPARAM 70401
+typedef struct qd_mlp qd_mlp;
+int qd_mlp_create(int device, uint64_t seed, qd_mlp** mlp);
+int qd_mlp_destroy(qd_mlp* mlp);
+int qd_mlp_get_params(const qd_mlp* mlp, float* host, int64_t n);
+int qd_mlp_set_params(qd_mlp* mlp, const float* host, int64_t n);
+int qd_mlp_forward(qd_mlp* mlp, const float* d_X, float* d_y, int64_t n, void* stream);
+int qd_mlp_grad(qd_mlp* mlp, const float* d_X, const float* d_T, int64_t n, float* d_grad, float* loss, void* stream);
+int qd_mlp_train_step(qd_mlp* mlp, const float* d_X, const float* d_T, int64_t n, float lr, float* loss,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libqdimsrg.so")
 _i64 = C.c_int64
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
+_ip64 = C.POINTER(C.c_int64)
 _lp = C.POINTER(_i64)
 _vp = C.c_void_p
 _vpp = C.POINTER(C.c_void_p)
@@ -106,6 +107,17 @@ SIGNATURES = {
     "qd_flow_omega": (C.c_int, [_vp, C.POINTER(_vp)]),
     "qd_flow_state": (C.c_int, [_vp, C.POINTER(FlowResult)]),
     "qd_flow_destroy": (C.c_int, [_vp]),
+    "qd_omega_count": (C.c_int, [_vp, _ip64]),
+    "qd_omega_gather": (C.c_int, [_vp, _vp, _i64]),
+    "qd_omega_scatter": (C.c_int, [_vp, _vp, C.c_float, _i64]),
+    "qd_omega_features": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _i64]),
+    "qd_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    "qd_mlp_destroy": (C.c_int, [_vp]),
+    "qd_mlp_get_params": (C.c_int, [_vp, C.POINTER(C.c_float), _i64]),
+    "qd_mlp_set_params": (C.c_int, [_vp, C.POINTER(C.c_float), _i64]),
+    "qd_mlp_forward": (C.c_int, [_vp, _vp, _vp, _i64, _vp]),
+    "qd_mlp_grad": (C.c_int, [_vp, _vp, _vp, _i64, _vp, C.POINTER(C.c_float), _vp]),
+    "qd_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i64, C.c_float, C.POINTER(C.c_float), _vp]),
     "qd_tbme_write": (C.c_int, [C.c_int, C.c_char_p, C.c_int, C.c_uint]),
     "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, C.c_double, C.c_uint,
                                     _dp, _dp, _i64, _ip]),

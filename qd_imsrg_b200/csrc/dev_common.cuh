@@ -96,6 +96,20 @@ __host__ __device__ inline int part_rows(int part, int4 bd) {
   }
 }
 
+// element e of two-body part p -> (block, offset of the element in vectorize order)
+__device__ __forceinline__ void part_elem(const DevLayout& L, int p, i64 e, int& q, i64& pos, int& row, int& col) {
+  const i64* cum = L.pcum + (i64)p * L.nblock;
+  q = find_seg(cum, L.nblock, e);
+  i64 loc = e - __ldg(cum + q);
+  const int4 bd = __ldg(&L.blk[q]);
+  int part = P_HHHH + p;
+  int rows = part_rows(part, bd);
+  row = (int)(loc % rows);
+  col = (int)(loc / rows);
+  // the six block offsets are stored in part order (hhhh, pppp, pphh, phph, ppph, phhh)
+  pos = __ldg(L.boff + 6 * q + p) + loc;
+}
+
 // block-level sum of a double across a CTA (fixed order => deterministic)
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* sh) {

@@ -60,20 +60,6 @@ struct RedDotRange {  // sum a[i]*b[i] (or a[i]^2) over [o, o+n)
   }
 };
 
-// element e of two-body part p -> (block, offset of the element in vectorize order)
-__device__ __forceinline__ void part_elem(const DevLayout& L, int p, i64 e, int& q, i64& pos, int& row, int& col) {
-  const i64* cum = L.pcum + (i64)p * L.nblock;
-  q = find_seg(cum, L.nblock, e);
-  i64 loc = e - __ldg(cum + q);
-  const int4 bd = __ldg(&L.blk[q]);
-  int part = P_HHHH + p;
-  int rows = part_rows(part, bd);
-  row = (int)(loc % rows);
-  col = (int)(loc / rows);
-  // the six block offsets are stored in part order (hhhh, pppp, pphh, phph, ppph, phhh)
-  pos = __ldg(L.boff + 6 * q + p) + loc;
-}
-
 struct RedDotPart {  // sum over all entries of one two-body part: a*b (or a^2)
   DevLayout L;
   const double* a;
