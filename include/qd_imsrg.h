@@ -276,7 +276,8 @@ int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, u
  * order.  Device pointers (d_*) are the caller's.                           */
 int qd_omega_count(const qd_layout* L, int64_t* n);
 int qd_omega_gather(const qd_op* G, double* d_out, int64_t n);              /* d_out[e] = entry e of G */
-int qd_omega_scatter(qd_op* G, const float* d_in, float scale, int64_t n);  /* G = 0 but entries scale*d_in */
+/* G = 0 except entries e = scale * d_in[e] * (d_escale ? d_escale[e] : 1)    */
+int qd_omega_scatter(qd_op* G, const float* d_in, float scale, const double* d_escale, int64_t n);
 /* 16 float features per entry (16-byte aligned rows): energies of the four
  * legs and their occupations, the H element, hbar-omega, N, the channel
  * (M_L, M_S), the target flow parameter s, the shells and the entry kind.    */

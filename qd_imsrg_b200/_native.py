@@ -109,7 +109,7 @@ SIGNATURES = {
     "qd_flow_destroy": (C.c_int, [_vp]),
     "qd_omega_count": (C.c_int, [_vp, _ip64]),
     "qd_omega_gather": (C.c_int, [_vp, _vp, _i64]),
-    "qd_omega_scatter": (C.c_int, [_vp, _vp, C.c_float, _i64]),
+    "qd_omega_scatter": (C.c_int, [_vp, _vp, C.c_float, _vp, _i64]),
     "qd_omega_features": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _i64]),
     "qd_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
     "qd_mlp_destroy": (C.c_int, [_vp]),

@@ -7,6 +7,7 @@
 //   qd_omega_count     number of entries
 //   qd_omega_gather    the entries of an operator (double, device)
 //   qd_omega_scatter   an operator that is zero except its Omega entries
+//                      (value * scale, times a per-entry factor if given)
 //   qd_omega_features  16 float features per entry (the network's input)
 #include "dev_common.cuh"
 
@@ -32,12 +33,12 @@ __global__ void k_omega_gather(DevLayout L, const double* __restrict__ G, double
   out[e] = G[omega_pos(L, e, q, r, c)];
 }
 
-__global__ void k_omega_scatter(DevLayout L, const float* __restrict__ in, float scale, double* __restrict__ G,
-                                i64 n) {
+__global__ void k_omega_scatter(DevLayout L, const float* __restrict__ in, float scale,
+                                const double* __restrict__ escale, double* __restrict__ G, i64 n) {
   const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   int q, r, c;
-  G[omega_pos(L, e, q, r, c)] = (double)scale * (double)in[e];
+  G[omega_pos(L, e, q, r, c)] = (double)scale * (double)in[e] * (escale ? escale[e] : 1.0);
 }
 
 // Features of entry e (all scaled to O(1)):
@@ -128,7 +129,7 @@ int qd_omega_gather(const qd_op* G, double* d_out, int64_t n) {
   return QD_OK;
 }
 
-int qd_omega_scatter(qd_op* G, const float* d_in, float scale, int64_t n) {
+int qd_omega_scatter(qd_op* G, const float* d_in, float scale, const double* d_escale, int64_t n) {
   if (!G || !d_in) {
     set_error("qd_omega_scatter: null argument");
     return QD_ERR_ARG;
@@ -140,7 +141,8 @@ int qd_omega_scatter(qd_op* G, const float* d_in, float scale, int64_t n) {
   }
   QD_CUDA(cudaSetDevice(L->device));
   QD_CUDA(cudaMemsetAsync(G->d, 0, sizeof(double) * L->neq, L->stream));
-  if (n > 0) k_omega_scatter<<<(unsigned)((n + 255) / 256), 256, 0, L->stream>>>(L->dev, d_in, scale, G->d, n);
+  if (n > 0)
+    k_omega_scatter<<<(unsigned)((n + 255) / 256), 256, 0, L->stream>>>(L->dev, d_in, scale, d_escale, G->d, n);
   ++L->nlaunch;
   G->herm = -1;
   G->zero_mask = ALL_PARTS & ~((1u << P_FPH) | (1u << P_PPHH));

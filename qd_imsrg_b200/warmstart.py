@@ -2,7 +2,11 @@
 
 A small per-entry network predicts the Magnus operator Omega at a flow
 parameter s from features of each of Omega's entries (fph and Vpphh: the
-only parts the White-generator flow fills).  The plain flow then continues
+only parts the White-generator flow fills).  It predicts each entry as a
+multiple of the first-order generator, Omega_e(s) = eta0_e * r_e(s) with
+eta0 = build_white(H_HF) (the flow's own first step direction), so that its
+error on an entry scales with that entry; an absolute error on each of the
+~10^6 entries would add up to a large change of Omega.  The plain flow then continues
 from the prediction (qd_flow_warm_start) to the reference's convergence
 criterion; if the predicted state is worse than the Hartree-Fock start
 (|MBPT2| not below its s = 0 value), the prediction is rejected and the flow
@@ -19,12 +23,13 @@ import time
 
 import numpy as np
 
-from . import FullHam, Flow, Layout, _native, hf_hamiltonian, mbpt2
+from . import FullHam, Flow, Layout, build_white, hf_hamiltonian, mbpt2
 from ._native import check, lib
 
 NFEAT = 16
 NPARAM = 70401
-TARGET_SCALE = 10.0  # the network's output is 10 * Omega
+RATIO_CLAMP = 4.0  # training targets r = Omega / eta0 are clipped to [-4, 4]
+ETA_FLOOR = 1e-10  # entries with |eta0| below this are not trained on (Omega ~ 0 there)
 
 
 def _torch():
@@ -48,9 +53,11 @@ def omega_gather(G: FullHam, out) -> None:
     check(lib().qd_omega_gather(G.h, _ptr(out), out.numel()))
 
 
-def omega_scatter(G: FullHam, vals, scale: float) -> None:
-    """G = 0 except its Omega entries = scale * vals (float32 device tensor)."""
-    check(lib().qd_omega_scatter(G.h, _ptr(vals), float(scale), vals.numel()))
+def omega_scatter(G: FullHam, vals, scale: float, escale=None) -> None:
+    """G = 0 except its Omega entries = scale * vals (float32 device tensor),
+    times escale (float64 device tensor) entry by entry if given."""
+    check(lib().qd_omega_scatter(G.h, _ptr(vals), float(scale), _ptr(escale) if escale is not None else None,
+                                 vals.numel()))
 
 
 def omega_features(H: FullHam, hw: float, s: float, out) -> None:
@@ -115,6 +122,12 @@ class Instance:
         self.E_HF = float(vec[0])
         self.n = omega_count(self.P)
         self.crit0 = abs(mbpt2(self.H))
+        torch = _torch()
+        eta = FullHam(self.P, -1)
+        build_white(eta, self.H)
+        self.eta0 = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        omega_gather(eta, self.eta0)
+        eta.close()
 
     def close(self):
         self.H.close()
@@ -152,17 +165,19 @@ def trajectory(inst: Instance, nsample: int, rng, max_iter: int = 300):
 
 def samples(inst: Instance, idx, svals, omegas):
     """Training rows: features of the recorded entries at each recorded s,
-    target 10 * Omega."""
+    target r = Omega / eta0 (entries with |eta0| >= ETA_FLOOR, clipped)."""
     torch = _torch()
     X0 = torch.empty((inst.n, NFEAT), dtype=torch.float32, device="cuda")
     omega_features(inst.H, inst.hw, 0.0, X0)
-    base = X0[idx]
+    eta = inst.eta0[idx]
+    keep = eta.abs() >= ETA_FLOOR
+    base, eta = X0[idx][keep], eta[keep]
     xs, ts = [], []
     for s, om in zip(svals, omegas):
         x = base.clone()
         x[:, 13] = float(s) / 10.0
         xs.append(x)
-        ts.append(om * TARGET_SCALE)
+        ts.append((om[keep].double() / eta).clamp(-RATIO_CLAMP, RATIO_CLAMP).float())
     return torch.cat(xs), torch.cat(ts)
 
 
@@ -193,7 +208,7 @@ def predict_omega(mlp: MLP, inst: Instance, s: float) -> FullHam:
     y = torch.empty(inst.n, dtype=torch.float32, device="cuda")
     mlp.forward(X, y)
     G = FullHam(inst.P, -1)
-    omega_scatter(G, y, 1.0 / TARGET_SCALE)
+    omega_scatter(G, y, 1.0, inst.eta0)
     torch.cuda.synchronize()
     return G
 
@@ -225,7 +240,8 @@ def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300):
     f = Flow(inst.H, HS, full_norm=True)
     f.warm_start(G, s_target)
     first = f.step()
-    accepted = first.crit < inst.crit0
+    crit_warm = float(first.crit)
+    accepted = crit_warm < inst.crit0
     wasted = 0
     if not accepted:
         wasted = f.state().commutators
@@ -236,7 +252,7 @@ def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     out = {"E": r.E0, "steps": r.iterations, "commutators": r.commutators + wasted, "seconds": dt,
-           "accepted": bool(accepted), "crit_warm": float(first.crit) if first is not None else None}
+           "accepted": bool(accepted), "crit_warm": crit_warm, "crit0": inst.crit0}
     f.close()
     HS.close()
     G.close()

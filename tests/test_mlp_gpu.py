@@ -88,6 +88,13 @@ def test_omega_kernels_match_host_statements(gpu):
     ref = np.zeros_like(v)
     ref[idx] = v[idx].astype(np.float32)
     assert np.array_equal(w, ref)
+    # with a per-entry factor (the warm start's eta0 scaling)
+    fac = torch.linspace(-2.0, 2.0, N, dtype=torch.float64, device="cuda")
+    ws.omega_scatter(G2, buf.float(), 0.5, fac)
+    w = G2.download()
+    ref = np.zeros_like(v)
+    ref[idx] = 0.5 * v[idx].astype(np.float32).astype(np.float64) * fac.cpu().numpy()
+    assert np.allclose(w, ref, rtol=1e-15, atol=0)
     # features of a Hamiltonian-like operator at s = 3.5
     from helpers import synth_hamiltonian
 
