@@ -67,7 +67,9 @@ def parse():
     ap.add_argument("--ws-eval", type=int, default=16, help="warmstart: held-out draws at N=20, R=20")
     ap.add_argument("--ws-steps", type=int, default=3000, help="warmstart: Adam steps")
     ap.add_argument("--ws-sample", type=int, default=4096, help="warmstart: recorded entries per flow")
-    ap.add_argument("--ws-s", type=float, default=0.0, help="warmstart: target s (0: half the median final s)")
+    ap.add_argument("--ws-frac", default="0.5,0.7,0.85",
+                    help="warmstart: target s as fractions of the training flows' median final s; the first "
+                         "is the headline, the others are reported beside it")
     ap.add_argument("--workload", choices=["flow", "commutator", "batch", "warmstart"], default="flow")
     ap.add_argument("--hw", type=float, default=0.5)
     ap.add_argument("--pandya", action="store_true", help="flow: add the particle-hole channel")
@@ -592,7 +594,9 @@ def run_warmstart(args, world, rank, local):
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     ref_s = sfin.get((20, 20)) or [v for vals in sfin.values() for v in vals] or [20.0]
-    s_target = args.ws_s or 0.5 * float(np.median(ref_s))
+    fracs = [float(x) for x in args.ws_frac.split(",")]
+    s_targets = [f * float(np.median(ref_s)) for f in fracs]
+    s_target = s_targets[0]
     evals = []
     for k in range(args.ws_eval):
         hw = float(rng.uniform(0.1, 1.0))
@@ -603,9 +607,9 @@ def run_warmstart(args, world, rank, local):
             continue
         try:
             cold = ws.cold_flow(inst)
-            warm = ws.warm_flow(mlp, inst, s_target)
-            evals.append({"hw": hw, "E_HF": inst.E_HF, "cold": cold, "warm": warm,
-                          "dE": abs(warm["E"] - cold["E"])})
+            warms = [ws.warm_flow(mlp, inst, st) for st in s_targets]
+            evals.append({"hw": hw, "E_HF": inst.E_HF, "cold": cold, "warm": warms[0], "sweep": warms[1:],
+                          "dE": abs(warms[0]["E"] - cold["E"])})
         except Exception as e:
             evals.append({"hw": hw, "why": str(e)})
         inst.close()
@@ -628,6 +632,15 @@ def run_warmstart(args, world, rank, local):
                            "commutators_warm": tot("commutators", "warm"),
                            "accepted": sum(1 for e in ok if e["warm"]["accepted"]), "evaluated": len(ok),
                            "max_abs_dE": max([e["dE"] for e in ok] or [None]),
+                           "s_fraction": fracs[0],
+                           "sweep": [{"s_fraction": f, "s_target": st,
+                                      "seconds_warm": sum(e["sweep"][k]["seconds"] for e in ok),
+                                      "steps_warm": sum(e["sweep"][k]["steps"] for e in ok),
+                                      "commutators_warm": sum(e["sweep"][k]["commutators"] for e in ok),
+                                      "accepted": sum(1 for e in ok if e["sweep"][k]["accepted"]),
+                                      "max_abs_dE": max(abs(e["sweep"][k]["E"] - e["cold"]["E"]) for e in ok)
+                                      if ok else None}
+                                     for k, (f, st) in enumerate(zip(fracs[1:], s_targets[1:]))],
                            "train_rows": int(X.shape[0]), "train_draws": len(Xs), "train_failed": trfail,
                            "data_s": t_data, "train_s": t_train, "loss_history": hist, "per_instance": evals}}
         print(json.dumps(line, default=float), flush=True)
