@@ -229,9 +229,13 @@ def cold_flow(inst: Instance, max_iter: int = 300):
 
 
 def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300):
-    """The plain flow from the predicted Omega(s_target); a prediction whose
-    state is not better than the HF start (|MBPT2| >= its s = 0 value) is
-    rejected and the flow restarts from Omega = 0."""
+    """The plain flow from the predicted Omega(s_target).  The prediction is
+    judged by the flow itself and abandoned (the flow restarts from
+    Omega = 0, its work counted) if the predicted state is not better than
+    the HF start (|MBPT2| not below its s = 0 value) or if the continued flow
+    rejects a step: a rejection shrinks the Euler step for the rest of the
+    flow (stp -> stp/2 + 1e-3, as s_evolve does), and such a flow can take
+    several times the steps of the plain one."""
     torch = _torch()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -239,20 +243,25 @@ def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300):
     HS = FullHam(inst.P, 1)
     f = Flow(inst.H, HS, full_norm=True)
     f.warm_start(G, s_target)
-    first = f.step()
-    crit_warm = float(first.crit)
-    accepted = crit_warm < inst.crit0
+    info = f.step()
+    crit_warm = float(info.crit)
+    accepted = crit_warm < inst.crit0 and bool(info.accepted or info.converged)
+    while accepted and not info.converged:
+        info = f.step()
+        if not info.accepted and not info.converged:
+            accepted = False
     wasted = 0
-    if not accepted:
+    if accepted:
+        r = f.state()
+    else:
         wasted = f.state().commutators
         f.close()
         f = Flow(inst.H, HS, full_norm=True)
-        first = None
-    r = f.state() if first is not None and first.converged else f.run(max_iter)
+        r = f.run(max_iter)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     out = {"E": r.E0, "steps": r.iterations, "commutators": r.commutators + wasted, "seconds": dt,
-           "accepted": bool(accepted), "crit_warm": crit_warm, "crit0": inst.crit0}
+           "accepted": bool(accepted), "crit_warm": crit_warm, "crit0": inst.crit0, "wasted_commutators": wasted}
     f.close()
     HS.close()
     G.close()
