@@ -566,7 +566,7 @@ def run_warmstart(args, world, rank, local):
     torch.cuda.set_device(local)
     rng = np.random.default_rng(2024)
     t0 = time.perf_counter()
-    Xs, Ts, sfin, trfail = [], [], {}, []
+    Xs, Ts, sfin, nsteps, trfail = [], [], {}, {}, []
     for k in range(args.ws_train):
         nb, R = (12, 20)[k % 2], (16, 20)[(k // 2) % 2]
         hw = float(rng.uniform(0.1, 1.0))
@@ -581,6 +581,7 @@ def run_warmstart(args, world, rank, local):
             Xs.append(X)
             Ts.append(T)
             sfin.setdefault((nb, R), []).append(float(res.s))
+            nsteps.setdefault((nb, R), []).append(int(res.iterations))
         except Exception as e:
             trfail.append({"N": nb, "R": R, "hw": hw, "why": str(e)})
         inst.close()
@@ -597,6 +598,8 @@ def run_warmstart(args, world, rank, local):
     fracs = [float(x) for x in args.ws_frac.split(",")]
     s_targets = [f * float(np.median(ref_s)) for f in fracs]
     s_target = s_targets[0]
+    ref_n = nsteps.get((20, 20)) or [v for vals in nsteps.values() for v in vals] or [40]
+    budget = int(np.median(ref_n))
     evals = []
     for k in range(args.ws_eval):
         hw = float(rng.uniform(0.1, 1.0))
@@ -607,7 +610,7 @@ def run_warmstart(args, world, rank, local):
             continue
         try:
             cold = ws.cold_flow(inst)
-            warms = [ws.warm_flow(mlp, inst, st) for st in s_targets]
+            warms = [ws.warm_flow(mlp, inst, st, step_budget=budget) for st in s_targets]
             evals.append({"hw": hw, "E_HF": inst.E_HF, "cold": cold, "warm": warms[0], "sweep": warms[1:],
                           "dE": abs(warms[0]["E"] - cold["E"])})
         except Exception as e:
@@ -632,7 +635,7 @@ def run_warmstart(args, world, rank, local):
                            "commutators_warm": tot("commutators", "warm"),
                            "accepted": sum(1 for e in ok if e["warm"]["accepted"]), "evaluated": len(ok),
                            "max_abs_dE": max([e["dE"] for e in ok] or [None]),
-                           "s_fraction": fracs[0],
+                           "s_fraction": fracs[0], "step_budget": budget,
                            "sweep": [{"s_fraction": f, "s_target": st,
                                       "seconds_warm": sum(e["sweep"][k]["seconds"] for e in ok),
                                       "steps_warm": sum(e["sweep"][k]["steps"] for e in ok),
