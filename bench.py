@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--ws-eval", type=int, default=16, help="warmstart: held-out draws at N=20, R=20")
     ap.add_argument("--ws-steps", type=int, default=3000, help="warmstart: Adam steps")
     ap.add_argument("--ws-sample", type=int, default=4096, help="warmstart: recorded entries per flow")
+    ap.add_argument("--ws-eval-seed", type=int, default=77, help="warmstart: seed of the held-out draws")
     ap.add_argument("--ws-frac", default="0.5,0.7,0.85",
                     help="warmstart: target s as fractions of the training flows' median final s; the first "
                          "is the headline, the others are reported beside it")
@@ -598,11 +599,11 @@ def run_warmstart(args, world, rank, local):
     fracs = [float(x) for x in args.ws_frac.split(",")]
     s_targets = [f * float(np.median(ref_s)) for f in fracs]
     s_target = s_targets[0]
-    ref_n = nsteps.get((20, 20)) or [v for vals in nsteps.values() for v in vals] or [40]
-    budget = int(np.median(ref_n))
+
     evals = []
+    erng = np.random.default_rng(args.ws_eval_seed)  # held-out draws: their own generator
     for k in range(args.ws_eval):
-        hw = float(rng.uniform(0.1, 1.0))
+        hw = float(erng.uniform(0.1, 1.0))
         try:
             inst = ws.Instance(20, 20, hw, device=local, mix=args.hf_mix, quad=args.tbme == "quad")
         except Exception as e:
@@ -610,7 +611,7 @@ def run_warmstart(args, world, rank, local):
             continue
         try:
             cold = ws.cold_flow(inst)
-            warms = [ws.warm_flow(mlp, inst, st, step_budget=budget) for st in s_targets]
+            warms = [ws.warm_flow(mlp, inst, st) for st in s_targets]
             evals.append({"hw": hw, "E_HF": inst.E_HF, "cold": cold, "warm": warms[0], "sweep": warms[1:],
                           "dE": abs(warms[0]["E"] - cold["E"])})
         except Exception as e:
@@ -635,7 +636,7 @@ def run_warmstart(args, world, rank, local):
                            "commutators_warm": tot("commutators", "warm"),
                            "accepted": sum(1 for e in ok if e["warm"]["accepted"]), "evaluated": len(ok),
                            "max_abs_dE": max([e["dE"] for e in ok] or [None]),
-                           "s_fraction": fracs[0], "step_budget": budget,
+                           "s_fraction": fracs[0], "eval_seed": args.ws_eval_seed,
                            "sweep": [{"s_fraction": f, "s_target": st,
                                       "seconds_warm": sum(e["sweep"][k]["seconds"] for e in ok),
                                       "steps_warm": sum(e["sweep"][k]["steps"] for e in ok),

@@ -228,16 +228,17 @@ def cold_flow(inst: Instance, max_iter: int = 300):
     return out
 
 
-def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300, step_budget: int = 0):
+def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300, window: int = 4,
+              drop: float = 0.5):
     """The plain flow from the predicted Omega(s_target).  The prediction is
     judged by the flow itself and abandoned (the flow restarts from
     Omega = 0, its work counted) if the predicted state is not better than
     the HF start (|MBPT2| not below its s = 0 value), if the continued flow
     rejects a step (a rejection shrinks the Euler step for the rest of the
-    flow, stp -> stp/2 + 1e-3, as s_evolve does) or if it needs more than
-    step_budget steps (0: no budget).  Either of the last two means that the
+    flow, stp -> stp/2 + 1e-3, as s_evolve does) or if |MBPT2| falls by less
+    than `drop` over `window` accepted steps.  The last two mean that the
     prediction seeded a slow mode: such flows can take several times the
-    steps of the plain one."""
+    steps of the plain one (whose |MBPT2| falls about 10x over four steps)."""
     torch = _torch()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -248,12 +249,15 @@ def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300, st
     info = f.step()
     crit_warm = float(info.crit)
     accepted = crit_warm < inst.crit0 and bool(info.accepted or info.converged)
-    nstep = 1
+    hist = [crit_warm]
     while accepted and not info.converged:
         info = f.step()
-        nstep += 1
-        if (not info.accepted and not info.converged) or (step_budget and nstep > step_budget):
+        if not info.accepted and not info.converged:
             accepted = False
+        elif info.accepted:
+            hist.append(float(info.crit))
+            if len(hist) > window and hist[-1] > drop * hist[-1 - window]:
+                accepted = False
     wasted = 0
     if accepted:
         r = f.state()
