@@ -1,5 +1,6 @@
 // kernels_122.cu -- commutator_122 (src/commutators.f90:355-676) as two
-// shared-memory-staged sparse passes per (M_L,M_S) block.
+// shared-memory-staged passes per (M_L,M_S) block, evaluated group pair by
+// group pair as small dense products.
 //
 // In block q the pairs are ordered [hh | ph | pp] (block-local index P); the
 // full block matrix V(P1,P2) holds the stored classes (class(P1) >=
@@ -12,25 +13,39 @@
 // G(x) = states with the (m_l, m_s) of x: the only t whose pair (t,b2) lies in
 // block q.  F/F' are the reference's one-body reads (see dev_common.cuh).
 //
+// Group pairs.  The pairs of block q split into the sets S(g,h) of pairs with
+// one state in (m_l,m_s) group g and one in group h (g <= h).  Indexing S(g,h)
+// as cells (k1,k2) <-> (t1,t2) = (G_g[k1], G_h[k2]) and writing the block's
+// antisymmetric matrix in that orientation, M(k1,k2) = V(t1 t2|.) (= -V of the
+// stored pair when t1 > t2; 0 on the diagonal when g = h), the bra legs of
+// every pair of S(g,h) are
+//   Y = F_g M + M F_h^T,   F_g(k1',k1) = F(G_g[k1'], k1-th member of G_g),
+// and C(pair) = (orientation sign) * Y(cell).  The ket legs are the same with
+// F' and V transposed.  Each product runs along "fibers": a fixed k2 (F_g,
+// length |G_g|) or a fixed k1 (F_h, length |G_h|).  A warp takes one group
+// pair and direction at a time; each lane keeps one row of F in registers
+// and the lanes of a fiber read its cells as shared-memory broadcasts.
+//
 // Pass 1 (bra, SET): a CTA stages TJ columns of V_A and V_B (all ntot rows,
-// upper classes through herm) in shared memory and writes those columns of
-// every stored class.  Pass 2 (ket, ACC): a CTA stages TJ rows and adds the
-// ket legs of those rows.  Each pass reads both operators about once; the
-// gathers over t hit shared memory.  A warp covers 32/TJ rows x TJ columns, so
-// the per-term lookups (static leg table: partner pair and sign; per-call
-// F table: group-diagonal one-body reads) are shared by TJ lanes and the
-// shared-memory reads of one row group are contiguous.
+// upper classes through herm) in shared memory in cell order, runs the k1
+// fibers, then the k2 fibers, and writes those columns of every stored class.
+// Pass 2 (ket, ACC): a CTA stages TJ rows and subtracts the ket legs of those
+// rows.  Each pass reads both operators about once; the products read shared
+// memory and registers only.
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <type_traits>
 
 #include "dev_common.cuh"
 
 namespace qd {
 
-constexpr int T122 = 512;  // threads per CTA
-constexpr size_t SMEM_MAX_ATTR_122 = 227 * 1024;  // opt-in shared memory per CTA on sm_100
-// TJ: columns (bra pass) / rows (ket pass) staged per CTA; a warp handles
-// 32/TJ rows (bra) or columns (ket) at a time, TJ lanes each.
+constexpr int T122 = 256;                          // threads per CTA
+constexpr int GMAX122 = 16;                        // largest (m_l,m_s) group (fiber length)
+constexpr size_t SMEM_MAX_ATTR_122 = 227 * 1024;   // opt-in shared memory per CTA on sm_100
+constexpr size_t SMEM_TARGET_122 = 74 * 1024;      // per-CTA staging goal: three CTAs per SM
+constexpr size_t SMEM_STATIC_122 = 1024;           // bound on the pass kernels' static shared memory
 
 struct Task122 {
   int q;
@@ -50,191 +65,242 @@ __device__ __forceinline__ int off_of(int c, int4 bd) { return c == 0 ? 0 : (c =
 __device__ __forceinline__ int cnt_of(int c, int4 bd) { return c == 0 ? bd.x : (c == 1 ? bd.y : bd.z); }
 __device__ __forceinline__ int cls_of(int P, int nh, int nb) { return P < nh ? 0 : (P < nh + nb ? 1 : 2); }
 
-// V(P1, P2) of one operator for block q, any classes (upper via herm); parts
-// set in zmask are known to be zero and not read
-__device__ __forceinline__ double vfull(const double* __restrict__ op, const i64* o, int4 bd, double herm,
-                                        unsigned zmask, int P1, int P2) {
-  int c1 = cls_of(P1, bd.x, bd.y), c2 = cls_of(P2, bd.x, bd.y);
-  int r1 = P1 - off_of(c1, bd), r2 = P2 - off_of(c2, bd);
-  if (c1 >= c2) {
-    const int sl = slot_of(c1, c2);
-    if ((zmask >> (P_HHHH + sl)) & 1u) return 0.0;
-    return op[__ldg(o + sl) + r1 + (i64)r2 * cnt_of(c1, bd)];
-  }
-  const int sl = slot_of(c2, c1);
-  if ((zmask >> (P_HHHH + sl)) & 1u) return 0.0;
-  return herm * op[__ldg(o + sl) + r2 + (i64)r1 * cnt_of(c2, bd)];
-}
-
-// Leg-table entry (static per layout), for pair P = (x1<x2) of a block:
-//   leg 0: t = G(x1)[k], t != x2, partner pair (t,x2); leg 1: t = G(x2)[k],
-//   t != x1, partner pair (x1,t).  Packed: block-local index of the partner
-//   (13 bits) | k (5 bits) << 13 | leg << 18 | (ordering sign < 0) << 19.
-__device__ __forceinline__ int leg_idx(int e) { return e & 0x1FFF; }
-__device__ __forceinline__ int leg_k(int e) { return (e >> 13) & 31; }
-__device__ __forceinline__ int leg_leg(int e) { return (e >> 18) & 1; }
-__device__ __forceinline__ double leg_sign(int e) { return ((e >> 19) & 1) ? -1.0 : 1.0; }
-
-// F tables (per call): [2][m][gmax] double2: (FA, FB) for the bra legs, then
-// (FA', FB') for the ket legs, of (state s, k-th member t of G(s)).
-__global__ void k_ftab(DevLayout L, const double* __restrict__ A, double hA, const double* __restrict__ B, double hB,
-                       double2* __restrict__ F, int gmax) {
+// Static tables of a layout (built once, see plan_122):
+//   meta[q]   = {cells of block q, first group pair, end of its group pairs, 0}
+//   sub[u]    = {first cell, |G_g| | |G_h| << 8 | (g = h) << 16, offset of F_g,
+//               offset of F_h} (group pairs of a block in decreasing size)
+//   cell[gp]  = for the pair gp = pbase[q] + P: {primary cell << 1 | (orientation sign < 0),
+//               mirror cell (the same pair seen as (t2,t1) when g = h) or -1}
+//   sbase[s]  = offset of state s's row in the group-major F table
+// Per call: F table [2][nfent] double2 (FA, FB) bra, then (FA', FB') ket,
+// group-major: F[goff_g + k1' * |G_g| + k].
+__global__ void k_ftab(DevLayout L, const int* __restrict__ sbase, const double* __restrict__ A, double hA,
+                       const double* __restrict__ B, double hB, double2* __restrict__ F, int gmax, int nfent) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= L.m * gmax) return;
   int s = e / gmax, k = e % gmax;
   int g = __ldg(&L.gid[s]);
   int b = __ldg(&L.gstart[g]), sz = __ldg(&L.gstart[g + 1]) - b;
-  double fab = 0.0, fbb = 0.0, fak = 0.0, fbk = 0.0;
-  if (k < sz) {
-    int t = __ldg(&L.gmem[b + k]);
-    if (t < L.n) {
-      double xa = f_hole(L, A, s, t), xb = f_hole(L, B, s, t);
-      fab = xa; fbb = xb; fak = hA * xa; fbk = hB * xb;
-    } else {
-      double xa = f_part(L, A, t, s), xb = f_part(L, B, t, s);
-      fab = hA * xa; fbb = hB * xb; fak = xa; fbk = xb;
-    }
+  if (k >= sz) return;
+  const int t = __ldg(&L.gmem[b + k]);
+  double fab, fbb, fak, fbk;
+  if (t < L.n) {
+    const double xa = f_hole(L, A, s, t), xb = f_hole(L, B, s, t);
+    fab = xa; fbb = xb; fak = hA * xa; fbk = hB * xb;
+  } else {
+    const double xa = f_part(L, A, t, s), xb = f_part(L, B, t, s);
+    fab = hA * xa; fbb = hB * xb; fak = xa; fbk = xb;
   }
-  F[e] = make_double2(fab, fbb);
-  F[L.m * gmax + e] = make_double2(fak, fbk);
+  const int pos = __ldg(&sbase[s]) + k;
+  F[pos] = make_double2(fab, fbb);
+  F[nfent + pos] = make_double2(fak, fbk);
 }
 
-// sum over the leg entries [l0, l1) of sg * (FA * VB - FB * VA), unrolled by 4
-// so that the four entries' loads are independent
-template <int TJ>
-__device__ __forceinline__ double leg_sum(const int* __restrict__ legs, int l0, int l1, int s0, int s1,
-                                          const double2* __restrict__ Ft, int gmax, const double2* sV, int lane_off) {
-  double acc = 0.0;
-  int u = l0;
-  for (; u + 4 <= l1; u += 4) {
-    int e[4];
+// One direction of one group pair, by one warp.  DIR 0: fibers are the
+// columns k2 of the cell grid (length N = |G_g|, F_g); DIR 1: the rows k1
+// (length N = |G_h|, F_h).  Lane (slot, r) keeps row r of F in registers and,
+// for the fibers (and staged columns j) of its slot, forms
+// sum_k F(r,k) (FA * VB - FB * VA)(cell k) into the fiber's cell r: DIR 0
+// assigns (it reaches every cell once), DIR 1 adds.  The lanes of a slot read
+// the same cells (shared-memory broadcast).
+template <int N, int TJ, int DIR>
+__device__ __forceinline__ void pair_dir(int base, int n1, int n2, int fofs, int lane, const double2* __restrict__ Vc,
+                                         double* __restrict__ Yc, const double2* __restrict__ F) {
+  constexpr int NSLOT = 32 / N;
+  const int slot = lane / N, r = lane - slot * N;
+  if (slot >= NSLOT) return;
+  double2 f[N];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) e[r] = __ldg(&legs[u + r]);
-    double2 f[4], v[4];
+  for (int k = 0; k < N; ++k) f[k] = __ldg(&F[fofs + r * N + k]);
+  const int nfib = (DIR ? n1 : n2) * TJ;
+  const int step = (DIR ? 1 : n2) * TJ;  // between the fiber's cells, in staged elements
+  for (int it = slot; it < nfib; it += NSLOT) {
+    const int fi = it / TJ, j = it % TJ;
+    const int e0 = (DIR ? base + fi * n2 : base + fi) * TJ + j;
+    const double2* v = Vc + e0;
+    double y0 = 0.0, y1 = 0.0;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      f[r] = __ldg(&Ft[(leg_leg(e[r]) ? s1 : s0) * gmax + leg_k(e[r])]);
-      v[r] = sV[leg_idx(e[r]) * TJ + lane_off];
+    for (int k = 0; k < N; ++k) {
+      const double2 x = v[k * step];
+      if (k & 1) {
+        y1 = fma(f[k].x, x.y, y1);
+        y1 = fma(-f[k].y, x.x, y1);
+      } else {
+        y0 = fma(f[k].x, x.y, y0);
+        y0 = fma(-f[k].y, x.x, y0);
+      }
     }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) acc += leg_sign(e[r]) * (f[r].x * v[r].y - f[r].y * v[r].x);
+    double* yo = Yc + e0 + r * step;
+    if (DIR)
+      *yo += y0 + y1;
+    else
+      *yo = y0 + y1;
   }
-  for (; u < l1; ++u) {
-    const int e = __ldg(&legs[u]);
-    const double2 f = __ldg(&Ft[(leg_leg(e) ? s1 : s0) * gmax + leg_k(e)]);
-    const double2 v = sV[leg_idx(e) * TJ + lane_off];
-    acc += leg_sign(e) * (f.x * v.y - f.y * v.x);
-  }
-  return acc;
 }
 
-template <int TJ>
-__global__ void __launch_bounds__(T122) k_122_bra(DevLayout L, const Task122* __restrict__ tasks,
-                                                  const int* __restrict__ legstart, const int* __restrict__ legs,
-                                                  const double2* __restrict__ Ftab, int gmax,
-                                                  const double* __restrict__ A, double hA, unsigned zA,
-                                                  const double* __restrict__ B, double hB, unsigned zB,
-                                                  double* __restrict__ C) {
-  extern __shared__ double2 smv[];  // (VA, VB) of each (row, column)
-  const Task122 tk = tasks[blockIdx.x];
-  const int q = tk.q, c2 = tk.cls;
-  const int4 bd = __ldg(&L.blk[q]);
-  const int nh = bd.x, nb = bd.y, ntot = bd.w;
-  const int ncol = min(TJ, cnt_of(c2, bd) - tk.first);
-  const int offc2 = off_of(c2, bd);
-  const i64* o = L.boff + 6 * q;
-  for (int e = threadIdx.x; e < ntot * TJ; e += blockDim.x) {
-    int P1 = e % ntot, j = e / ntot;
-    double va = 0.0, vb = 0.0;
-    if (j < ncol) {
-      int P2 = offc2 + tk.first + j;
-      va = vfull(A, o, bd, hA, zA, P1, P2);
-      vb = vfull(B, o, bd, hB, zB, P1, P2);
-    }
-    smv[P1 * TJ + j] = make_double2(va, vb);
-  }
-  __syncthreads();
-  const int pb = __ldg(&L.pbase[q]);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  constexpr int RPW = 32 / TJ;
-  const int j = lane % TJ, sub = lane / TJ;
-  for (int base = offc2 + warp * RPW; base < ntot; base += nwarp * RPW) {
-    const int P1 = base + sub;
-    if (P1 >= ntot) continue;
-    const int2 br = __ldg(&L.pairs[pb + P1]);
-    const double acc = leg_sum<TJ>(legs, __ldg(&legstart[pb + P1]), __ldg(&legstart[pb + P1 + 1]), br.x, br.y, Ftab,
-                               gmax, smv, j);
-    if (j < ncol) {
-      const int c1 = cls_of(P1, nh, nb);
-      const int rows = cnt_of(c1, bd);
-      C[__ldg(o + slot_of(c1, c2)) + (P1 - off_of(c1, bd)) + (i64)(tk.first + j) * rows] = acc;
+// all group pairs of the block, one direction; warps take group pairs in turn
+// (no two group pairs share a cell, no two fibers of a direction share a cell)
+template <int TJ, int DIR, int GM>
+__device__ __forceinline__ void run_dir(const int4* __restrict__ sub, int ns, const double2* Vc, double* Yc,
+                                        const double2* __restrict__ F) {
+  const int lane = threadIdx.x & 31;
+  for (int u = threadIdx.x >> 5; u < ns; u += T122 / 32) {
+    const int4 d = __ldg(&sub[u]);
+    const int n1 = d.y & 0xFF, n2 = (d.y >> 8) & 0xFF;
+    const int fofs = DIR ? d.w : d.z;
+    switch (DIR ? n2 : n1) {
+#define QD_DIR_CASE(N)                                                         \
+  case N:                                                                      \
+    if constexpr (N <= GM) pair_dir<N, TJ, DIR>(d.x, n1, n2, fofs, lane, Vc, Yc, F); \
+    break;
+      QD_DIR_CASE(1) QD_DIR_CASE(2) QD_DIR_CASE(3) QD_DIR_CASE(4)
+      QD_DIR_CASE(5) QD_DIR_CASE(6) QD_DIR_CASE(7) QD_DIR_CASE(8)
+      QD_DIR_CASE(9) QD_DIR_CASE(10) QD_DIR_CASE(11) QD_DIR_CASE(12)
+      QD_DIR_CASE(13) QD_DIR_CASE(14) QD_DIR_CASE(15) QD_DIR_CASE(16)
+#undef QD_DIR_CASE
+      default: break;
     }
   }
 }
 
+// stage (VA, VB) of a pair into its cell(s), staged column/row j
 template <int TJ>
-__global__ void __launch_bounds__(T122) k_122_ket(DevLayout L, const Task122* __restrict__ tasks,
-                                                  const int* __restrict__ legstart, const int* __restrict__ legs,
-                                                  const double2* __restrict__ Ftab, int gmax,
-                                                  const double* __restrict__ A, double hA, unsigned zA,
-                                                  const double* __restrict__ B, double hB, unsigned zB,
-                                                  double* __restrict__ C) {
+__device__ __forceinline__ void stage_cell(double2* Vc, int2 cl, int j, double va, double vb) {
+  const double s = (cl.x & 1) ? -1.0 : 1.0;
+  Vc[(cl.x >> 1) * TJ + j] = make_double2(s * va, s * vb);
+  if (cl.y >= 0) Vc[cl.y * TJ + j] = make_double2(-s * va, -s * vb);
+}
+
+constexpr int U122 = 4;  // staging loads in flight per thread
+
+// Pass kernels.  KET = 0: bra pass over TJ columns of class ct = tk.cls
+// (SET); KET = 1: ket pass over TJ rows of class ct (subtract).  The staged
+// operand values V(P1,P2) are read class segment by class segment of the
+// other index: segment c (cnt_c pairs) of stored part (max(c,ct), min(c,ct))
+// is contiguous along the pair index when its rows are the varying index,
+// else strided; the upper segments carry herm.
+template <int TJ, int KET, int GM>
+__global__ void __launch_bounds__(T122, GM <= 10 ? 3 : 2) k_122_pass(DevLayout L, const Task122* __restrict__ tasks,
+                                                   const int4* __restrict__ meta, const int4* __restrict__ sub,
+                                                   const int2* __restrict__ cell, const double2* __restrict__ Ftab,
+                                                   const double* __restrict__ A, double hA, unsigned zA,
+                                                   const double* __restrict__ B, double hB, unsigned zB,
+                                                   double* __restrict__ C) {
   extern __shared__ double2 smv[];
   const Task122 tk = tasks[blockIdx.x];
-  const int q = tk.q, c1 = tk.cls;
+  const int q = tk.q, ct = tk.cls;
   const int4 bd = __ldg(&L.blk[q]);
-  const int nh = bd.x, nb = bd.y, ntot = bd.w;
-  const int rows = cnt_of(c1, bd);
-  const int nrow = min(TJ, rows - tk.first);
-  const int offc1 = off_of(c1, bd);
+  const int4 mt = __ldg(&meta[q]);
+  double2* Vc = smv;                                        // [cells][TJ] (VA, VB)
+  double* Yc = reinterpret_cast<double*>(smv + mt.x * TJ);  // [cells][TJ]
+  int* pc = reinterpret_cast<int*>(Yc + mt.x * TJ);          // [ntot] primary cell << 1 | sign
+  const int nct = cnt_of(ct, bd);
+  const int nj = min(TJ, nct - tk.first);  // staged columns (bra) / rows (ket)
+  const int pb = __ldg(&L.pbase[q]);
   const i64* o = L.boff + 6 * q;
-  for (int e = threadIdx.x; e < ntot * TJ; e += blockDim.x) {
-    int i = e % TJ, P2 = e / TJ;
-    double va = 0.0, vb = 0.0;
-    if (i < nrow) {
-      int P1 = offc1 + tk.first + i;
-      va = vfull(A, o, bd, hA, zA, P1, P2);
-      vb = vfull(B, o, bd, hB, zB, P1, P2);
+  const int ns = mt.z - mt.y;
+  sub += mt.y;
+  // cells of no pair: the diagonal (t,t) of same-group pairs
+  for (int u = threadIdx.x; u < ns; u += T122) {
+    const int4 d = __ldg(&sub[u]);
+    if (d.y >> 16) {
+      const int n = d.y & 0xFF;
+      for (int k = 0; k < n; ++k)
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) Vc[(d.x + k * (n + 1)) * TJ + j] = make_double2(0.0, 0.0);
     }
-    smv[P2 * TJ + i] = make_double2(va, vb);
+  }
+  for (int c = 0; c < 3; ++c) {
+    const int nc = cnt_of(c, bd);
+    if (nc == 0) continue;
+    // element (r, j): the pair r of segment c against staged index j
+    const bool lower = KET ? (ct >= c) : (c >= ct);  // stored without transposition
+    const int sl = KET ? (lower ? slot_of(ct, c) : slot_of(c, ct)) : (lower ? slot_of(c, ct) : slot_of(ct, c));
+    const bool za = (zA >> (P_HHHH + sl)) & 1u, zb = (zB >> (P_HHHH + sl)) & 1u;
+    const double fa = lower ? 1.0 : hA, fb = lower ? 1.0 : hB;
+    // bra: V(row r of c, column first+j); ket: V(row first+j, column r of c).
+    // The stored part's rows are segment c (bra lower, ket upper): address
+    // r + (first+j) * nc; else its rows are class ct: (first+j) + r * nct.
+    const bool crow = KET ? !lower : lower;
+    const i64 rs = crow ? 1 : nct, js = crow ? nc : 1;
+    const i64 b0 = __ldg(o + sl) + (crow ? (i64)tk.first * nc : (i64)tk.first);
+    const int offc = off_of(c, bd);
+    const int total = nc * TJ;
+    for (int e0 = threadIdx.x; e0 < total; e0 += U122 * T122) {
+      double va[U122], vb[U122];
+      int2 cl[U122];
+#pragma unroll
+      for (int u = 0; u < U122; ++u) {
+        const int e = e0 + u * T122;
+        const int r = e / TJ, j = e % TJ;
+        va[u] = vb[u] = 0.0;
+        cl[u] = make_int2(-1, -1);
+        if (e < total && j < nj) {
+          const i64 a = b0 + r * rs + j * js;
+          cl[u] = __ldg(&cell[pb + offc + r]);
+          if (!za) va[u] = fa * __ldg(A + a);
+          if (!zb) vb[u] = fb * __ldg(B + a);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U122; ++u)
+        if (cl[u].x >= 0) {
+          const int e = e0 + u * T122;
+          stage_cell<TJ>(Vc, cl[u], e % TJ, va[u], vb[u]);
+          if (e % TJ == 0) pc[offc + e / TJ] = cl[u].x;
+        }
+    }
   }
   __syncthreads();
-  const int pb = __ldg(&L.pbase[q]);
-  const double2* Fket = Ftab + (i64)L.m * gmax;
-  const int ncols = offc1 + rows;  // output columns: classes <= c1
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  constexpr int RPW = 32 / TJ;
-  const int i = lane % TJ, sub = lane / TJ;
-  for (int base = warp * RPW; base < ncols; base += nwarp * RPW) {
-    const int P2 = base + sub;
-    if (P2 >= ncols) continue;
-    const int2 kt = __ldg(&L.pairs[pb + P2]);
-    const double acc = leg_sum<TJ>(legs, __ldg(&legstart[pb + P2]), __ldg(&legstart[pb + P2 + 1]), kt.x, kt.y, Fket,
-                               gmax, smv, i);
-    if (i < nrow) {
-      const int c2 = cls_of(P2, nh, nb);
-      C[__ldg(o + slot_of(c1, c2)) + (i64)(P2 - off_of(c2, bd)) * rows + tk.first + i] -= acc;
+  run_dir<TJ, 0, GM>(sub, ns, Vc, Yc, Ftab);
+  __syncthreads();
+  run_dir<TJ, 1, GM>(sub, ns, Vc, Yc, Ftab);
+  __syncthreads();
+  // output: bra -> rows of classes c >= ct of the staged columns (SET);
+  // ket -> columns of classes c <= ct of the staged rows (subtract)
+  for (int c = KET ? 0 : ct; c <= (KET ? ct : 2); ++c) {
+    const int nc = cnt_of(c, bd);
+    if (nc == 0) continue;
+    const int sl = KET ? slot_of(ct, c) : slot_of(c, ct);
+    const i64 rs = KET ? nct : 1, js = KET ? 1 : nc;
+    const i64 b0 = __ldg(o + sl) + (KET ? (i64)tk.first : (i64)tk.first * nc);
+    const int offc = off_of(c, bd);
+    for (int e0 = threadIdx.x; e0 < nc * TJ; e0 += U122 * T122) {
+#pragma unroll
+      for (int u = 0; u < U122; ++u) {
+        const int e = e0 + u * T122;
+        const int r = e / TJ, j = e % TJ;
+        if (e >= nc * TJ || j >= nj) continue;
+        const int cx = pc[offc + r];
+        const double y = Yc[(cx >> 1) * TJ + j];
+        double* out = C + b0 + r * rs + j * js;
+        if (KET)
+          *out -= (cx & 1) ? -y : y;
+        else
+          *out = (cx & 1) ? -y : y;
+      }
     }
   }
 }
 
 // ---- host side --------------------------------------------------------------
 namespace {
-// Tasks are grouped in buckets of similar block size; each bucket is one
-// launch whose dynamic shared memory fits its largest block.
+// Tasks are grouped in buckets by TJ; each bucket is one launch per pass
+// whose dynamic shared memory fits its largest block.
 struct Bucket122 {
-  int tj;       // 8 or 4
-  int first;    // range in the task arrays
+  int tj;       // 2, 4, 8 or 16
+  int first;    // range in the task array
   int count;
   size_t smem;
 };
 struct Plan122 {
-  Task122* d_bra = nullptr;
-  Task122* d_ket = nullptr;
-  int* d_legstart = nullptr;
-  int* d_legs = nullptr;
+  Task122* d_task = nullptr;
+  int4* d_meta = nullptr;
+  int4* d_sub = nullptr;
+  int2* d_cell = nullptr;
+  int* d_sbase = nullptr;
   double2* d_ftab = nullptr;
-  int nbra = 0, nket = 0, gmax = 0;
+  int ntask = 0, gmax = 0, nfent = 0;
   std::vector<Bucket122> buckets;
 };
 std::map<const qd_layout*, Plan122>& plans() {
@@ -244,7 +310,48 @@ std::map<const qd_layout*, Plan122>& plans() {
 // plans of different layouts are built and dropped from concurrent host
 // threads (batched flows); map nodes stay put, so a found plan needs no lock
 std::mutex g_plan_mutex;
+
+size_t smem_122(int cells, int npair, int tj) {
+  return (sizeof(double2) + sizeof(double)) * (size_t)cells * tj + sizeof(int) * (size_t)((npair + 3) & ~3);
+}
 }  // namespace
+
+// the attribute is process-wide: set it to the device limit, so that plans
+// built concurrently for other layouts can never lower it below a need
+template <int GM>
+static int set_attr_122() {
+  const void* fns[8] = {(const void*)k_122_pass<16, 0, GM>, (const void*)k_122_pass<16, 1, GM>,
+                        (const void*)k_122_pass<8, 0, GM>,  (const void*)k_122_pass<8, 1, GM>,
+                        (const void*)k_122_pass<4, 0, GM>,  (const void*)k_122_pass<4, 1, GM>,
+                        (const void*)k_122_pass<2, 0, GM>,  (const void*)k_122_pass<2, 1, GM>};
+  for (const void* fn : fns) {
+    cudaFuncAttributes fa;
+    QD_CUDA(cudaFuncGetAttributes(&fa, fn));  // static + dynamic shared memory <= the limit
+    QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMEM_MAX_ATTR_122 - (int)fa.sharedSizeBytes));
+  }
+  return QD_OK;
+}
+
+template <int GM, int KET>
+static void pass_122(const Plan122* p, qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
+  const double2* ft = p->d_ftab + (KET ? p->nfent : 0);
+  for (const Bucket122& b : p->buckets) {
+#define QD_122_LAUNCH(TJ)                                                                                          \
+  k_122_pass<TJ, KET, GM><<<b.count, T122, b.smem, L->stream>>>(L->dev, p->d_task + b.first, p->d_meta, p->d_sub, \
+                                                                p->d_cell, ft, A->d, (double)A->herm,             \
+                                                                A->zero_mask, B->d, (double)B->herm,              \
+                                                                B->zero_mask, C)
+    switch (b.tj) {
+      case 16: QD_122_LAUNCH(16); break;
+      case 8: QD_122_LAUNCH(8); break;
+      case 4: QD_122_LAUNCH(4); break;
+      default: QD_122_LAUNCH(2); break;
+    }
+#undef QD_122_LAUNCH
+    ++L->nlaunch;
+  }
+}
 
 static int plan_122(qd_layout* L, Plan122** out) {
   std::lock_guard<std::mutex> lock(g_plan_mutex);
@@ -254,101 +361,127 @@ static int plan_122(qd_layout* L, Plan122** out) {
     return QD_OK;
   }
   Plan122 p;
-  // group sizes
-  int ngroup = (int)L->gstart.size() - 1;
-  for (int g = 0; g < ngroup; ++g) p.gmax = std::max(p.gmax, L->gstart[g + 1] - L->gstart[g]);
-  if (p.gmax > 31) {
-    set_error("commutator_122: (ml,ms) group of %d states exceeds the leg-table range", p.gmax);
+  const int m = L->m;
+  const int ngroup = (int)L->gstart.size() - 1;
+  std::vector<int> gsz(ngroup), goff(ngroup + 1, 0), kpos(m, 0), sbase(m, 0);
+  for (int g = 0; g < ngroup; ++g) {
+    gsz[g] = L->gstart[g + 1] - L->gstart[g];
+    p.gmax = std::max(p.gmax, gsz[g]);
+    goff[g + 1] = goff[g] + gsz[g] * gsz[g];
+    for (int k = 0; k < gsz[g]; ++k) kpos[L->gmem[L->gstart[g] + k]] = k;
+  }
+  if (p.gmax > GMAX122) {
+    set_error("commutator_122: (ml,ms) group of %d states exceeds %d", p.gmax, GMAX122);
     return QD_ERR_ARG;
   }
-  // leg table over all pairs of all blocks (global pair index = pbase[q] + P)
-  std::vector<int> legstart(L->pairs.size() + 1, 0), legs;
-  const int m = L->m;
+  p.nfent = goff[ngroup];
+  for (int s = 0; s < m; ++s) sbase[s] = goff[L->gid[s]] + kpos[s] * gsz[L->gid[s]];
+
+  // group pairs and cells of every block
+  std::vector<int4> meta(L->nblock), sub;
+  std::vector<int2> cell(L->pairs.size(), int2{-1, -1});
   for (int q = 0; q < L->nblock; ++q) {
-    const int nh = L->blk[q].x, nb = L->blk[q].y;
-    for (int P = 0; P < L->blk[q].w; ++P) {
-      const int gp = L->pbase[q] + P;
-      legstart[gp] = (int)legs.size();
-      const int x1 = L->pairs[gp].x, x2 = L->pairs[gp].y;
-      for (int leg = 0; leg < 2; ++leg) {
-        const int xs = leg ? x2 : x1, other = leg ? x1 : x2;
-        const int g = L->gid[xs];
-        for (int k = 0; k < L->gstart[g + 1] - L->gstart[g]; ++k) {
-          const int t = L->gmem[L->gstart[g] + k];
-          if (t == other) continue;
-          const int a = leg ? x1 : t, b = leg ? t : x2;
-          const int e = L->ptab[(size_t)a * m + b];
-          if (pt_blk(e) != q) {
-            set_error("commutator_122: leg partner outside its block (layout inconsistency)");
+    const int nh = L->blk[q].x, nb = L->blk[q].y, ntot = L->blk[q].w, pb = L->pbase[q];
+    std::map<std::pair<int, int>, int> subs;  // (g <= h) -> first cell
+    std::vector<std::pair<int, int>> order;
+    int ncell = 0;
+    for (int P = 0; P < ntot; ++P) {
+      const int2 pr = L->pairs[pb + P];
+      const int g = std::min(L->gid[pr.x], L->gid[pr.y]), h = std::max(L->gid[pr.x], L->gid[pr.y]);
+      if (subs.emplace(std::make_pair(g, h), ncell).second) {
+        order.push_back({g, h});
+        ncell += gsz[g] * gsz[h];
+      }
+    }
+    std::vector<int4> sv;
+    for (const auto& gh : order) {
+      const int g = gh.first, h = gh.second, base = subs[gh], n1 = gsz[g], n2 = gsz[h];
+      for (int k1 = 0; k1 < n1; ++k1)
+        for (int k2 = 0; k2 < n2; ++k2) {
+          if (g == h && k1 == k2) continue;  // (t,t): no pair, M = 0
+          const int t1 = L->gmem[L->gstart[g] + k1], t2 = L->gmem[L->gstart[h] + k2];
+          const int e = L->ptab[(size_t)t1 * m + t2];
+          if (e < 0 || pt_blk(e) != q) {
+            set_error("commutator_122: group pair outside its block (layout inconsistency)");
             return QD_ERR_LAYOUT;
           }
           const int c = pt_cls(e);
-          const int idx = pt_idx(e) + (c == 0 ? 0 : (c == 1 ? nh : nh + nb));
-          if (idx > 0x1FFF) {
-            set_error("commutator_122: block too large for the leg table");
-            return QD_ERR_ARG;
-          }
-          legs.push_back(idx | (k << 13) | (leg << 18) | (pt_swap(e) << 19));
+          const int P = pt_idx(e) + (c == 0 ? 0 : (c == 1 ? nh : nh + nb));
+          const int cidx = base + k1 * n2 + k2;
+          if (g != h || k1 < k2)
+            cell[pb + P].x = cidx << 1 | pt_swap(e);
+          else
+            cell[pb + P].y = cidx;
         }
-      }
+      sv.push_back(int4{base, n1 | n2 << 8 | (g == h) << 16, goff[g], goff[h]});
     }
+    for (int P = 0; P < ntot; ++P)
+      if (cell[pb + P].x < 0) {
+        set_error("commutator_122: pair without a group-pair cell (layout inconsistency)");
+        return QD_ERR_LAYOUT;
+      }
+    // largest group pairs first: the warps take them in turn
+    std::stable_sort(sv.begin(), sv.end(), [](const int4& a, const int4& b) {
+      return (a.y & 0xFF) * ((a.y >> 8) & 0xFF) > (b.y & 0xFF) * ((b.y >> 8) & 0xFF);
+    });
+    meta[q] = int4{ncell, (int)sub.size(), (int)(sub.size() + sv.size()), 0};
+    sub.insert(sub.end(), sv.begin(), sv.end());
   }
-  legstart[L->pairs.size()] = (int)legs.size();
-  // buckets: (max block size, TJ)
-  const int lim[4] = {200, 400, 800, 1 << 30};
-  const int tjs[4] = {8, 8, 8, 4};
-  std::vector<Task122> hb;
-  int maxtot = 0;
+
+  // tasks: TJ = the largest power of two (2..16) whose staging fits the
+  // per-CTA goal; larger blocks first within a bucket
+  const int tjs[4] = {16, 8, 4, 2};
+  std::vector<Task122> ht;
   for (int bkt = 0; bkt < 4; ++bkt) {
-    const int lo = bkt ? lim[bkt - 1] : 0;
+    const int tj = tjs[bkt];
     std::vector<std::pair<int, Task122>> v;
-    int bmax = 0;
+    int cmax = 0;
     for (int q = 0; q < L->nblock; ++q) {
-      const int ntot = L->blk[q].w;
-      if (ntot <= lo || ntot > lim[bkt]) continue;
+      const int nc = meta[q].x;
+      if (L->blk[q].w == 0) continue;
+      int want = 2;
+      for (int t : tjs)
+        if (smem_122(nc, L->blk[q].w, t) <= SMEM_TARGET_122) {
+          want = t;
+          break;
+        }
+      if (want != tj) continue;
+      if (smem_122(nc, L->blk[q].w, tj) > SMEM_MAX_ATTR_122 - SMEM_STATIC_122) {
+        set_error("commutator_122: block of %d cells exceeds shared memory", nc);
+        return QD_ERR_ARG;
+      }
+      cmax = std::max(cmax, (int)smem_122(nc, L->blk[q].w, tj));
       const int cnt[3] = {L->blk[q].x, L->blk[q].y, L->blk[q].z};
-      bmax = std::max(bmax, ntot);
       for (int c = 0; c < 3; ++c)
-        for (int f = 0; f < cnt[c]; f += tjs[bkt]) v.push_back({ntot, Task122{q, (short)c, 0, f}});
+        for (int f = 0; f < cnt[c]; f += tj) v.push_back({nc, Task122{q, (short)c, 0, f}});
     }
     if (v.empty()) continue;
     std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     Bucket122 bk;
-    bk.tj = tjs[bkt];
-    bk.first = (int)hb.size();
+    bk.tj = tj;
+    bk.first = (int)ht.size();
     bk.count = (int)v.size();
-    bk.smem = sizeof(double2) * (size_t)bmax * bk.tj;
-    if (bk.smem > SMEM_MAX_ATTR_122) {
-      set_error("commutator_122: block of %d pairs exceeds shared memory", bmax);
-      return QD_ERR_ARG;
-    }
-    for (auto& x : v) hb.push_back(x.second);
+    bk.smem = (size_t)cmax;
+    for (auto& x : v) ht.push_back(x.second);
     p.buckets.push_back(bk);
-    maxtot = std::max(maxtot, bmax);
   }
-  std::vector<Task122>& hk = hb;  // the ket pass uses the same (block, class, first) tasks
-  p.nbra = (int)hb.size();
-  p.nket = (int)hk.size();
-  if (p.nbra) {
-    QD_CUDA(cudaMalloc(&p.d_bra, hb.size() * sizeof(Task122)));
-    QD_CUDA(cudaMemcpy(p.d_bra, hb.data(), hb.size() * sizeof(Task122), cudaMemcpyHostToDevice));
-    QD_CUDA(cudaMalloc(&p.d_ket, hk.size() * sizeof(Task122)));
-    QD_CUDA(cudaMemcpy(p.d_ket, hk.data(), hk.size() * sizeof(Task122), cudaMemcpyHostToDevice));
-  }
-  QD_CUDA(cudaMalloc(&p.d_legstart, legstart.size() * sizeof(int)));
-  QD_CUDA(cudaMemcpy(p.d_legstart, legstart.data(), legstart.size() * sizeof(int), cudaMemcpyHostToDevice));
-  QD_CUDA(cudaMalloc(&p.d_legs, std::max<size_t>(1, legs.size()) * sizeof(int)));
-  if (!legs.empty()) QD_CUDA(cudaMemcpy(p.d_legs, legs.data(), legs.size() * sizeof(int), cudaMemcpyHostToDevice));
-  QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)L->m * p.gmax));
-  L->ws_bytes += (i64)(legstart.size() + legs.size()) * 4 + (i64)sizeof(double) * 4 * L->m * p.gmax;
-  // the attribute is process-wide: set it to the device limit, so that plans
-  // built concurrently for other layouts can never lower it below a need
+  p.ntask = (int)ht.size();
+  auto up = [&](auto& vec, auto** dptr) -> int {
+    using T = typename std::decay<decltype(vec[0])>::type;
+    QD_CUDA(cudaMalloc(dptr, std::max<size_t>(1, vec.size()) * sizeof(T)));
+    if (!vec.empty()) QD_CUDA(cudaMemcpy(*dptr, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
+    L->ws_bytes += (i64)(vec.size() * sizeof(T));
+    return QD_OK;
+  };
+  int rc;
+  if ((rc = up(ht, &p.d_task)) || (rc = up(meta, &p.d_meta)) || (rc = up(sub, &p.d_sub)) ||
+      (rc = up(cell, &p.d_cell)) || (rc = up(sbase, &p.d_sbase)))
+    return rc;
+  QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)std::max(1, p.nfent)));
+  L->ws_bytes += (i64)sizeof(double2) * 2 * p.nfent;
   if (!p.buckets.empty()) {
-    const int lim = (int)SMEM_MAX_ATTR_122;
-    QD_CUDA(cudaFuncSetAttribute(k_122_bra<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    QD_CUDA(cudaFuncSetAttribute(k_122_ket<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    QD_CUDA(cudaFuncSetAttribute(k_122_bra<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    QD_CUDA(cudaFuncSetAttribute(k_122_ket<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    int rc2 = p.gmax <= 10 ? set_attr_122<10>() : set_attr_122<16>();
+    if (rc2) return rc2;
   }
   plans()[L] = p;
   *out = &plans()[L];
@@ -359,8 +492,9 @@ void drop_122_plan(const qd_layout* L) {
   std::lock_guard<std::mutex> lock(g_plan_mutex);
   auto it = plans().find(L);
   if (it == plans().end()) return;
-  for (void* ptr : {(void*)it->second.d_bra, (void*)it->second.d_ket, (void*)it->second.d_legstart,
-                    (void*)it->second.d_legs, (void*)it->second.d_ftab})
+  const Plan122& p = it->second;
+  for (void* ptr : {(void*)p.d_task, (void*)p.d_meta, (void*)p.d_sub, (void*)p.d_cell, (void*)p.d_sbase,
+                    (void*)p.d_ftab})
     if (ptr) cudaFree(ptr);
   plans().erase(it);
 }
@@ -369,35 +503,18 @@ int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   Plan122* p;
   int rc = plan_122(L, &p);
   if (rc) return rc;
-  if (p->nbra == 0) return QD_OK;
+  if (p->ntask == 0) return QD_OK;
   const int nf = L->m * p->gmax;
-  k_ftab<<<(nf + 127) / 128, 128, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d, (double)B->herm, p->d_ftab,
-                                                  p->gmax);
-  for (const Bucket122& b : p->buckets) {
-    const Task122* tb = p->d_bra + b.first;
-    if (b.tj == 8)
-      k_122_bra<8><<<b.count, T122, b.smem, L->stream>>>(L->dev, tb, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
-                                                          B->zero_mask, C);
-    else
-      k_122_bra<4><<<b.count, T122, b.smem, L->stream>>>(L->dev, tb, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
-                                                          B->zero_mask, C);
-    ++L->nlaunch;
+  k_ftab<<<(nf + 127) / 128, 128, 0, L->stream>>>(L->dev, p->d_sbase, A->d, (double)A->herm, B->d,
+                                                  (double)B->herm, p->d_ftab, p->gmax, p->nfent);
+  ++L->nlaunch;
+  if (p->gmax <= 10) {
+    pass_122<10, 0>(p, L, A, B, C);
+    pass_122<10, 1>(p, L, A, B, C);
+  } else {
+    pass_122<16, 0>(p, L, A, B, C);
+    pass_122<16, 1>(p, L, A, B, C);
   }
-  for (const Bucket122& b : p->buckets) {
-    const Task122* tk = p->d_ket + b.first;
-    if (b.tj == 8)
-      k_122_ket<8><<<b.count, T122, b.smem, L->stream>>>(L->dev, tk, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
-                                                          B->zero_mask, C);
-    else
-      k_122_ket<4><<<b.count, T122, b.smem, L->stream>>>(L->dev, tk, p->d_legstart, p->d_legs, p->d_ftab, p->gmax,
-                                                          A->d, (double)A->herm, A->zero_mask, B->d, (double)B->herm,
-                                                          B->zero_mask, C);
-    ++L->nlaunch;
-  }
-  L->nlaunch += 1;
   QD_CUDA(cudaGetLastError());
   return QD_OK;
 }
