@@ -299,6 +299,19 @@ int qd_mlp_grad(qd_mlp* mlp, const float* d_X, const float* d_T, int64_t n, floa
 int qd_mlp_train_step(qd_mlp* mlp, const float* d_X, const float* d_T, int64_t n, float lr, float* loss,
                       void* stream);
 
+/* Split-precision FP64 product with dgemm's argument meaning (column-major;
+ * transa/transb 'N' or 'T'): C = alpha op(A) op(B) + beta C on device arrays,
+ * on the tcgen05 tensor cores.  Replaces the dgemm calls of matrix_mult222
+ * (src/commutators.f90:987-1132) and construct_cc_ints
+ * (src/ME_general.f90:923-952) in the split form.  Each row of op(A) and
+ * column of op(B) is scaled by a power of two and cut into `slices` (1..8)
+ * 7-bit integer BF16 slices; the slice products with s + t <= slices + 1 are
+ * accumulated exactly in FP32 (TMEM) over K chunks and summed in FP64.  The
+ * truncation error is about 2^(-7 slices) of max|row| max|column| K per
+ * entry; slices = 8 reaches FP64 accuracy.  Synchronous on `stream`.       */
+int qd_gemm_split(int device, void* stream, char transa, char transb, int M, int N, int K, double alpha,
+                  const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc, int slices);
+
 #ifdef __cplusplus
 }
 #endif

@@ -438,3 +438,31 @@ def v_int(qi, qj, qk, ql, hw: float = 1.0, quad: bool = False) -> float:
     arrs = [(C.c_int * 3)(*[int(x) for x in q]) for q in (qi, qj, qk, ql)]
     fn = lib().qd_v_int_quad if quad else lib().qd_v_int
     return float(fn(*arrs, float(hw)))
+
+
+def gemm_split(A, B, C=None, alpha: float = 1.0, beta: float = 0.0, trans_a: bool = False, trans_b: bool = False,
+               slices: int = 8, device: int = 0, stream=None):
+    """C = alpha op(A) op(B) + beta C in the split form (qd_gemm_split) on
+    row-major float64 CUDA tensors (torch); op(X) = X.T when trans_x.
+    Returns C (allocated when not given)."""
+    import torch
+
+    for X in (A, B):
+        if X.dtype != torch.float64 or not X.is_cuda or not X.is_contiguous() or X.dim() != 2:
+            raise ValueError("gemm_split: A and B must be contiguous 2-D float64 CUDA tensors")
+    m, k = (A.shape[1], A.shape[0]) if trans_a else (A.shape[0], A.shape[1])
+    k2, n = (B.shape[1], B.shape[0]) if trans_b else (B.shape[0], B.shape[1])
+    if k != k2:
+        raise ValueError(f"gemm_split: inner dimensions {k} and {k2} differ")
+    if C is None:
+        C = torch.zeros((m, n), dtype=torch.float64, device=A.device)
+        beta = 0.0
+    elif C.shape != (m, n) or not C.is_contiguous() or C.dtype != torch.float64:
+        raise ValueError("gemm_split: C must be a contiguous float64 tensor of shape (m, n)")
+    st = stream if stream is not None else torch.cuda.current_stream(A.device).cuda_stream
+    # row-major X is the column-major X^T: C^T = alpha op(B)^T op(A)^T + beta C^T
+    tb, ta = (b"T" if trans_b else b"N"), (b"T" if trans_a else b"N")
+    check(lib().qd_gemm_split(int(device), st, tb, ta, n, m, k, float(alpha),
+                              B.data_ptr(), B.shape[1], A.data_ptr(), A.shape[1], float(beta), C.data_ptr(), n,
+                              int(slices)))
+    return C

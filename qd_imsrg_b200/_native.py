@@ -118,6 +118,8 @@ SIGNATURES = {
     "qd_mlp_forward": (C.c_int, [_vp, _vp, _vp, _i64, _vp]),
     "qd_mlp_grad": (C.c_int, [_vp, _vp, _vp, _i64, _vp, C.POINTER(C.c_float), _vp]),
     "qd_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i64, C.c_float, C.POINTER(C.c_float), _vp]),
+    "qd_gemm_split": (C.c_int, [C.c_int, _vp, C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, _vp,
+                                C.c_int, _vp, C.c_int, C.c_double, _vp, C.c_int, C.c_int]),
     "qd_tbme_write": (C.c_int, [C.c_int, C.c_char_p, C.c_int, C.c_uint]),
     "qd_hf_hamiltonian": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int, C.c_double, C.c_uint,
                                     _dp, _dp, _i64, _ip]),
