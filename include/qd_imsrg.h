@@ -75,6 +75,14 @@ int qd_layout_offsets(const qd_layout* L, int64_t* off6);
 int qd_layout_pairs(const qd_layout* L, int q, int kind, int* out, int* count);
 /* CUDA stream (cudaStream_t) used for this layout; NULL = library-owned    */
 int qd_layout_set_stream(qd_layout* L, void* stream);
+/* Precision of the block contractions (the dgemm calls of matrix_mult222,
+ * construct_cc_ints, commutator_221 and commutator_111) on this layout:
+ * slices = 0 plain FP64 (the reference's arithmetic), 1..8 the split form of
+ * qd_gemm_split with that many BF16 slices per operand.  Everything else
+ * (one-body, 122, 121, 221 traces, Pandya gathers, E0, norms, BCH sums, HF)
+ * stays FP64.  No reference counterpart (the reference is FP64 only).       */
+int qd_layout_set_split(qd_layout* L, int slices);
+int qd_layout_get_split(const qd_layout* L, int* slices);
 int qd_layout_synchronize(qd_layout* L);
 /* device bytes currently held by the layout's work arena                    */
 int qd_layout_workspace_bytes(const qd_layout* L, int64_t* bytes);

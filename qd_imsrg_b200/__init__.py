@@ -84,6 +84,17 @@ class Layout:
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib().qd_layout_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
+    @property
+    def split(self) -> int:
+        """Slices of the split form of the block contractions (0 = plain FP64)."""
+        v = C.c_int()
+        check(lib().qd_layout_get_split(self.h, C.byref(v)))
+        return v.value
+
+    @split.setter
+    def split(self, slices: int) -> None:
+        check(lib().qd_layout_set_split(self.h, int(slices)))
+
     def profile(self, enable: bool = True) -> None:
         """Start (and reset) or stop per-stage CUDA-event timing."""
         check(lib().qd_layout_profile(self.h, int(enable)))

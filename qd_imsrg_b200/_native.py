@@ -60,6 +60,8 @@ SIGNATURES = {
     "qd_layout_offsets": (C.c_int, [_vp, _lp]),
     "qd_layout_pairs": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _ip]),
     "qd_layout_set_stream": (C.c_int, [_vp, _vp]),
+    "qd_layout_set_split": (C.c_int, [_vp, C.c_int]),
+    "qd_layout_get_split": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "qd_layout_synchronize": (C.c_int, [_vp]),
     "qd_layout_workspace_bytes": (C.c_int, [_vp, _lp]),
     "qd_layout_profile": (C.c_int, [_vp, C.c_int]),

@@ -444,6 +444,19 @@ int qd_layout_set_stream(qd_layout* L, void* stream) {
   return QD_OK;
 }
 
+int qd_layout_set_split(qd_layout* L, int slices) {
+  CHECK(L, QD_ERR_ARG, "null layout");
+  CHECK(slices >= 0 && slices <= 8, QD_ERR_ARG, "qd_layout_set_split: slices must be 0..8");
+  L->split_slices = slices;
+  return QD_OK;
+}
+
+int qd_layout_get_split(const qd_layout* L, int* slices) {
+  CHECK(L && slices, QD_ERR_ARG, "null argument");
+  *slices = L->split_slices;
+  return QD_OK;
+}
+
 int qd_layout_synchronize(qd_layout* L) {
   CHECK(L, QD_ERR_ARG, "null layout");
   TRY(use_device(L));

@@ -576,6 +576,7 @@ int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double 
                 unsigned maskB) {
   int rc = build_programs(L);
   if (rc) return rc;
+  if (L->split_slices > 0) return run_program_split(L, P, bufs, hv0, hv1, maskA, maskB);
   GTask* d_tasks = nullptr;
   int nt = 0;
   if ((rc = get_tasks(L, P, maskA, maskB, &d_tasks, &nt))) return rc;

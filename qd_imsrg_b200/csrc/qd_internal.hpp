@@ -156,6 +156,9 @@ struct qd_layout {
   // GEMM programs
   qd::GemmProgram prog_ladder, prog_221, prog_111, prog_pandya;
   bool programs_built = false;
+  // split form of the GEMM programs: slices per operand (0 = plain FP64)
+  int split_slices = 0;
+  void* split = nullptr;  // plans and workspaces (split_gemm.cu)
 };
 
 struct qd_op {
@@ -215,5 +218,8 @@ int launch_pandya_gather(qd_layout* L, const double* Z, double* C);
 int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
                 unsigned maskB);
 void fill_random(const qd_layout* L, int herm, uint64_t seed, double sigma, int conserve, double* out);
+int run_program_split(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
+                      unsigned maskB);
+void split_free(qd_layout* L);
 
 }  // namespace qd

@@ -46,27 +46,33 @@ constexpr size_t SG_BTILE = (size_t)SG_BN * SG_BK * 2;  // bytes per B slice til
 constexpr long long SG_SPIN = 1LL << 22;                // mbarrier polls before giving up
 
 // Operand role: the slices of one op(A) (rows i = m) or op(B) (rows i = n),
-// K-major: slice s of row i at sl[((s * rpad) + i) * kpad + k]; ex[i] = e_i.
+// K-major, in a shared workspace: slice s of row i at
+// slbase[S * unit + (s * rpad + i) * kpad + k] (unit = the sum of rpad * kpad
+// over the roles before it); e_i at exbase[ex_off + i].  The slicer reads the role
+// from source buffer src: x(i,k) = src[off + i * si + k * sk].
 struct SRole {
-  const __nv_bfloat16* sl;
-  const int* ex;
-  int rpad, kpad;
+  i64 unit;
+  int ex_off, rpad, kpad, R, K, src;
+  i64 off, si, sk;
 };
-struct SSeg {
-  int ra, rb;    // roles of op(A) and op(B)
-  int K;
-  double alpha;
+struct SSeg {  // acc += c * hv0^pa * hv1^pb * op(A) op(B)
+  int ra, rb, K;
+  signed char pa, pb, pad0, pad1;
+  double c;
 };
 struct SProb {
-  int M, N, ldc, seg0, nseg, mode;  // mode: 0 SET, 1 ACC, 2 C = V + beta C
+  int M, N, ldc, seg0, nseg, mode, outbuf, pad;  // mode: 0 SET, 1 ACC, 2 C = V + beta C
   i64 offC;
-  double* C;
   double beta;
 };
 struct STask {
   int prob;
   short ti, tj;
 };
+struct SPtrs {
+  const double* p[8];
+};
+constexpr int SG_NBUF = 8;
 
 // K chunk over which every diagonal's FP32 sums stay exact
 __host__ __device__ inline int split_kchunk(int S) {
@@ -86,25 +92,31 @@ __host__ __device__ inline int split_tmem_cols(int S) {
 // ---------------------------------------------------------------------------
 // slicing: role (x(i,k) = X[i*si + k*sk]) -> exponents and S slices
 // ---------------------------------------------------------------------------
-// one warp per row i: max |x(i,k)| over k, then the slices of the row
-__global__ void k_split_slice(const double* __restrict__ X, i64 si, i64 sk, int R, int K, int S, int rpad, int kpad,
-                              __nv_bfloat16* __restrict__ sl, int* __restrict__ ex) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= rpad) return;
-  const int i = warp;
+// one warp per (role, row i): max |x(i,k)| over k, then the slices of the row;
+// rows beyond R (padding) get zero slices
+__global__ void k_split_slice(const SRole* __restrict__ roles, const i64* __restrict__ rowstart, int nroles,
+                              SPtrs src, int S, __nv_bfloat16* __restrict__ slbase, int* __restrict__ exbase) {
+  const i64 w = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= rowstart[nroles]) return;
+  const int r = find_seg(rowstart, nroles, w);
+  const SRole ro = roles[r];
+  const int i = (int)(w - rowstart[r]);
+  const double* X = src.p[ro.src] + ro.off;
   double mx = 0.0;
-  if (i < R)
-    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(X[i * si + k * sk]));
+  if (i < ro.R)
+    for (int k = lane; k < ro.K; k += 32) mx = fmax(mx, fabs(X[i * ro.si + k * ro.sk]));
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   const int e = mx > 0.0 ? ilogb(mx) + 1 : 0;
-  if (lane == 0 && i < R) ex[i] = e;
-  for (int k = lane; k < kpad; k += 32) {
-    double r = (i < R && k < K) ? scalbn(X[i * si + k * sk], -e) : 0.0;
-    for (int s = 0; s < S; ++s) {
-      const double t = r * 128.0;
+  if (lane == 0) exbase[ro.ex_off + i] = e;
+  __nv_bfloat16* out = slbase + (i64)S * ro.unit + (i64)i * ro.kpad;
+  for (int k = lane; k < ro.kpad; k += 32) {
+    double x = (i < ro.R && k < ro.K) ? scalbn(X[i * ro.si + k * ro.sk], -e) : 0.0;
+    for (int sl = 0; sl < S; ++sl) {
+      const double t = x * 128.0;
       const double d = rint(t);
-      r = t - d;
-      sl[((i64)s * rpad + i) * kpad + k] = __float2bfloat16_rn((float)d);
+      x = t - d;
+      out[(i64)sl * ro.rpad * ro.kpad + k] = __float2bfloat16_rn((float)d);
     }
   }
 }
@@ -171,13 +183,13 @@ __device__ __forceinline__ void cp16(unsigned saddr, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
 }
 
-// stage rows [row0, row0+rows) x K [k0, k0+64) of slice s of role r into a
-// swizzled tile: 16-byte chunk c of row i lands at i*128 + ((c ^ (i & 7)) * 16)
-__device__ __forceinline__ void stage_tile(unsigned sbase, const SRole& ro, int s, int row0, int rows, int k0) {
-  const __nv_bfloat16* g = ro.sl + ((i64)s * ro.rpad + row0) * ro.kpad + k0;
+// stage rows [row0, row0+rows) x K [k0, k0+64) of one slice (rows kpad
+// apart) into a swizzled tile: 16-byte chunk c of row i lands at
+// i*128 + ((c ^ (i & 7)) * 16)
+__device__ __forceinline__ void stage_tile(unsigned sbase, const __nv_bfloat16* g, int kpad, int rows) {
   for (int e = threadIdx.x; e < rows * 8; e += SG_THREADS) {
     const int i = e >> 3, c = e & 7;
-    cp16(sbase + i * 128 + ((c ^ (i & 7)) << 4), g + (i64)i * ro.kpad + c * 8);
+    cp16(sbase + i * 128 + ((c ^ (i & 7)) << 4), g + (i64)i * kpad + c * 8);
   }
 }
 
@@ -186,7 +198,8 @@ __device__ __forceinline__ void stage_tile(unsigned sbase, const SRole& ro, int 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SG_THREADS, 1)
     k_split_gemm(const STask* __restrict__ tasks, const SProb* __restrict__ probs, const SSeg* __restrict__ segs,
-                 const SRole* __restrict__ roles, int S, int* __restrict__ err) {
+                 const SRole* __restrict__ roles, int S, const __nv_bfloat16* __restrict__ slbase,
+                 const int* __restrict__ exbase, SPtrs outs, double hv0, double hv1, int* __restrict__ err) {
   extern __shared__ uint8_t smraw[];
   __shared__ uint64_t bar;
   __shared__ unsigned tslot;
@@ -228,16 +241,20 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
   for (int sg = 0; sg < P.nseg && !fail; ++sg) {
     const SSeg G = segs[P.seg0 + sg];
     const SRole RA = roles[G.ra], RB = roles[G.rb];
-    if (threadIdx.x < SG_BN) fx[threadIdx.x] = (col0 + threadIdx.x < P.N) ? RB.ex[col0 + threadIdx.x] : 0;
-    const int em = m < P.M ? RA.ex[m] : 0;
+    const double alpha = G.c * (G.pa ? hv0 : 1.0) * (G.pb ? hv1 : 1.0);
+    const __nv_bfloat16* slA = slbase + (i64)S * RA.unit + (i64)row0 * RA.kpad;
+    const __nv_bfloat16* slB = slbase + (i64)S * RB.unit + (i64)col0 * RB.kpad;
+    const i64 sstrA = (i64)RA.rpad * RA.kpad, sstrB = (i64)RB.rpad * RB.kpad;
+    if (threadIdx.x < SG_BN) fx[threadIdx.x] = (col0 + threadIdx.x < P.N) ? exbase[RB.ex_off + col0 + threadIdx.x] : 0;
+    const int em = m < P.M ? exbase[RA.ex_off + m] : 0;
     const int ksteps = (G.K + SG_BK - 1) / SG_BK;
     for (int c0 = 0; c0 < ksteps && !fail; c0 += kc / SG_BK) {
       const int c1 = min(ksteps, c0 + kc / SG_BK);
       unsigned init = 0;  // diagonals written in this chunk
       for (int ks = c0; ks < c1; ++ks) {
         for (int s = 0; s < S; ++s) {
-          stage_tile(sA + s * (unsigned)SG_ATILE, RA, s, row0, SG_BM, ks * SG_BK);
-          stage_tile(sB + s * (unsigned)SG_BTILE, RB, s, col0, SG_BN, ks * SG_BK);
+          stage_tile(sA + s * (unsigned)SG_ATILE, slA + s * sstrA + ks * SG_BK, RA.kpad, SG_BM);
+          stage_tile(sB + s * (unsigned)SG_BTILE, slB + s * sstrB + ks * SG_BK, RB.kpad, SG_BN);
         }
         asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -268,7 +285,7 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
       tc_fence_after();
       // read the diagonals of this chunk and add them in FP64
       for (int d = 0; d < S; ++d) {
-        const double rs = ldexp(G.alpha, em - 7 * (d + 2));
+        const double rs = ldexp(alpha, em - 7 * (d + 2));
 #pragma unroll
         for (int q = 0; q < SG_BN / 16; ++q) {
           float v[16];
@@ -285,7 +302,7 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
   if (fail && threadIdx.x == 0) atomicExch(err, 1);
   // epilogue: thread = row m, columns col0.. (consecutive rows per column)
   if (!fail && m < P.M) {
-    double* out = P.C + P.offC + m;
+    double* out = const_cast<double*>(outs.p[P.outbuf]) + P.offC + m;
     const int nn = min(SG_BN, P.N - col0);
 #pragma unroll
     for (int j = 0; j < SG_BN; ++j) {
@@ -309,16 +326,304 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
 
 size_t split_gemm_smem(int S) { return (size_t)S * (SG_ATILE + SG_BTILE) + 1024; }
 
+// pair modes: C = (C +) V + sigma V^T from the product V (M x M scratch)
+struct SPair {
+  int M, ldc, outbuf, acc;
+  i64 offV, offC;
+  double sc;
+  int spa, spb;
+};
+struct SPairTask {
+  int pair;
+  short ti, tj;
+};
+__global__ void k_split_pair(const SPairTask* __restrict__ tasks, const SPair* __restrict__ pairs,
+                             const double* __restrict__ V, SPtrs outs, double hv0, double hv1) {
+  __shared__ double t[32][33];
+  const SPairTask tk = tasks[blockIdx.x];
+  const SPair P = pairs[tk.pair];
+  const double sigma = P.sc * (P.spa ? hv0 : 1.0) * (P.spb ? hv1 : 1.0);
+  const double* v = V + P.offV;
+  double* C = const_cast<double*>(outs.p[P.outbuf]) + P.offC;
+  const int r0 = tk.ti * 32, c0 = tk.tj * 32, M = P.M;
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {  // t[i][j] = V(c0+i, r0+j)
+    const int i = e & 31, j = e >> 5;
+    t[i][j] = (c0 + i < M && r0 + j < M) ? v[(c0 + i) + (i64)(r0 + j) * M] : 0.0;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    const int a = e & 31, b = e >> 5, r = r0 + a, c = c0 + b;
+    if (r < M && c < M) {
+      const double val = v[r + (i64)c * M] + sigma * t[b][a];
+      double* p = C + r + (i64)c * P.ldc;
+      *p = P.acc ? *p + val : val;
+    }
+  }
+}
+
+__global__ void k_scale2d(double* __restrict__ C, int ldc, int M, i64 n, double beta) {
+  const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) C[(e % M) + (e / M) * ldc] *= beta;
+}
+
+// ---------------------------------------------------------------------------
+// host side: split plans of the grouped GEMM programs
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SplitPlan {
+  std::vector<SRole> roles;
+  i64 units = 0, exn = 0, vsize = 0, rows = 0;
+  SRole* d_roles = nullptr;
+  i64* d_rowstart = nullptr;
+  SSeg* d_segs = nullptr;
+  SProb* d_probs = nullptr;
+  STask* d_tasks = nullptr;
+  SPair* d_pairs = nullptr;
+  SPairTask* d_ptasks = nullptr;
+  int ntask = 0, nptask = 0;
+};
+
+struct SplitState {
+  std::map<std::tuple<const void*, unsigned, unsigned>, SplitPlan> plans;
+  __nv_bfloat16* sl = nullptr;
+  size_t sl_n = 0;
+  int* ex = nullptr;
+  size_t ex_n = 0;
+  double* V = nullptr;
+  size_t v_n = 0;
+  int* err = nullptr;
+};
+
+template <class T>
+int upload(const std::vector<T>& h, T** d) {
+  QD_CUDA(cudaMalloc((void**)d, std::max<size_t>(1, h.size()) * sizeof(T)));
+  if (!h.empty()) QD_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return QD_OK;
+}
+
+bool seg_live(const GSeg& s, unsigned mA, unsigned mB) {
+  auto dead = [&](int src, int dep) {
+    if (dep < 0) return false;
+    unsigned m = src == 0 ? mA : (src == 1 ? mB : 0u);
+    return ((m >> dep) & 1u) != 0;
+  };
+  return s.K > 0 && !dead(s.srcA, s.depA) && !dead(s.srcB, s.depB);
+}
+
+constexpr int SG_VBUF = 7;  // output slot of the pair-mode scratch
+
+int build_plan(const GemmProgram& G, unsigned mA, unsigned mB, SplitPlan& sp) {
+  std::map<std::tuple<int, i64, i64, i64, int, int>, int> rk;
+  auto role = [&](int src, i64 off, i64 si, i64 sk, int R, int K) {
+    auto key = std::make_tuple(src, off, si, sk, R, K);
+    auto it = rk.find(key);
+    if (it != rk.end()) return it->second;
+    SRole r;
+    r.R = R;
+    r.K = K;
+    r.rpad = (R + SG_BM - 1) / SG_BM * SG_BM;
+    r.kpad = std::max(SG_BK, (K + SG_BK - 1) / SG_BK * SG_BK);
+    r.unit = sp.units;
+    r.ex_off = (int)sp.exn;
+    r.src = src;
+    r.off = off;
+    r.si = si;
+    r.sk = sk;
+    sp.units += (i64)r.rpad * r.kpad;
+    sp.exn += r.rpad;
+    sp.roles.push_back(r);
+    rk[key] = (int)sp.roles.size() - 1;
+    return (int)sp.roles.size() - 1;
+  };
+  std::vector<SSeg> segs;
+  std::vector<SProb> probs;
+  std::vector<SPair> pairs;
+  std::vector<std::pair<double, STask>> tv;
+  for (const GProb& g : G.probs) {
+    const bool pair = g.mode == GM_ACC_PAIR || g.mode == GM_SET_PAIR;
+    const bool set = g.mode == GM_SET || g.mode == GM_SET_PAIR;
+    SProb p;
+    std::memset(&p, 0, sizeof(p));
+    p.M = g.M;
+    p.N = g.N;
+    p.seg0 = (int)segs.size();
+    double cost = 1.0;
+    for (int k = 0; k < g.nseg; ++k) {
+      const GSeg& s = G.segs[g.seg0 + k];
+      if (!seg_live(s, mA, mB)) continue;
+      SSeg q;
+      std::memset(&q, 0, sizeof(q));
+      q.ra = role(s.srcA, s.offA, s.tA ? s.lda : 1, s.tA ? 1 : s.lda, g.M, s.K);
+      q.rb = role(s.srcB, s.offB, s.tB ? 1 : s.ldb, s.tB ? s.ldb : 1, g.N, s.K);
+      q.K = s.K;
+      q.c = s.c;
+      q.pa = s.pa;
+      q.pb = s.pb;
+      segs.push_back(q);
+      cost += (s.K + SG_BK - 1) / SG_BK;
+    }
+    p.nseg = (int)segs.size() - p.seg0;
+    if (p.nseg == 0 && !set) continue;
+    if (pair) {
+      SPair pr;
+      std::memset(&pr, 0, sizeof(pr));
+      pr.M = g.M;
+      pr.ldc = g.ldc;
+      pr.outbuf = g.outbuf;
+      pr.acc = g.mode == GM_ACC_PAIR;
+      pr.offV = sp.vsize;
+      pr.offC = g.offC;
+      pr.sc = g.sc;
+      pr.spa = g.spa;
+      pr.spb = g.spb;
+      pairs.push_back(pr);
+      p.mode = 0;
+      p.outbuf = SG_VBUF;
+      p.offC = sp.vsize;
+      p.ldc = g.M;
+      sp.vsize += (i64)g.M * g.M;
+    } else {
+      p.mode = set ? 0 : 1;
+      p.outbuf = g.outbuf;
+      p.offC = g.offC;
+      p.ldc = g.ldc;
+    }
+    probs.push_back(p);
+    const int tm = (g.M + SG_BM - 1) / SG_BM, tn = (g.N + SG_BN - 1) / SG_BN;
+    for (int i = 0; i < tm; ++i)
+      for (int j = 0; j < tn; ++j) tv.push_back({cost, STask{(int)probs.size() - 1, (short)i, (short)j}});
+  }
+  std::stable_sort(tv.begin(), tv.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<STask> tasks(tv.size());
+  for (size_t i = 0; i < tv.size(); ++i) tasks[i] = tv[i].second;
+  std::vector<SPairTask> pt;
+  for (size_t k = 0; k < pairs.size(); ++k) {
+    const int t = (pairs[k].M + 31) / 32;
+    for (int i = 0; i < t; ++i)
+      for (int j = 0; j < t; ++j) pt.push_back(SPairTask{(int)k, (short)i, (short)j});
+  }
+  std::vector<i64> rowstart(sp.roles.size() + 1, 0);
+  for (size_t r = 0; r < sp.roles.size(); ++r) rowstart[r + 1] = rowstart[r] + sp.roles[r].rpad;
+  sp.rows = rowstart.back();
+  int rc;
+  if ((rc = upload(sp.roles, &sp.d_roles)) || (rc = upload(rowstart, &sp.d_rowstart)) ||
+      (rc = upload(segs, &sp.d_segs)) || (rc = upload(probs, &sp.d_probs)) || (rc = upload(tasks, &sp.d_tasks)) ||
+      (rc = upload(pairs, &sp.d_pairs)) || (rc = upload(pt, &sp.d_ptasks)))
+    return rc;
+  sp.ntask = (int)tasks.size();
+  sp.nptask = (int)pt.size();
+  return QD_OK;
+}
+
+void free_plan(SplitPlan& sp) {
+  for (void* p : {(void*)sp.d_roles, (void*)sp.d_rowstart, (void*)sp.d_segs, (void*)sp.d_probs, (void*)sp.d_tasks,
+                  (void*)sp.d_pairs, (void*)sp.d_ptasks})
+    if (p) cudaFree(p);
+}
+
+// slices, products and pair combines of one plan on `st`; workspaces grown on demand
+int run_plan(SplitState& ss, const SplitPlan& sp, int S, SPtrs bufs, double hv0, double hv1, cudaStream_t st,
+             i64* ws_bytes) {
+  auto grow = [&](auto*& ptr, size_t& have, size_t need, size_t elem) -> int {
+    if (need <= have) return QD_OK;
+    if (ptr) {
+      QD_CUDA(cudaStreamSynchronize(st));
+      QD_CUDA(cudaFree(ptr));
+    }
+    ptr = nullptr;
+    QD_CUDA(cudaMalloc((void**)&ptr, need * elem));
+    if (ws_bytes) *ws_bytes += (i64)((need - have) * elem);
+    have = need;
+    return QD_OK;
+  };
+  int rc;
+  if ((rc = grow(ss.sl, ss.sl_n, (size_t)S * sp.units, 2)) || (rc = grow(ss.ex, ss.ex_n, (size_t)sp.exn, 4)) ||
+      (rc = grow(ss.V, ss.v_n, (size_t)std::max<i64>(1, sp.vsize), 8)))
+    return rc;
+  if (!ss.err) {
+    QD_CUDA(cudaMalloc((void**)&ss.err, sizeof(int)));
+    QD_CUDA(cudaMemsetAsync(ss.err, 0, sizeof(int), st));
+  }
+  if (sp.rows > 0) {
+    const i64 threads = sp.rows * 32;
+    k_split_slice<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(sp.d_roles, sp.d_rowstart,
+                                                                    (int)sp.roles.size(), bufs, S, ss.sl, ss.ex);
+  }
+  SPtrs outs = bufs;
+  outs.p[SG_VBUF] = ss.V;
+  if (sp.ntask > 0) {
+    const size_t smem = split_gemm_smem(S);
+    QD_CUDA(cudaFuncSetAttribute(k_split_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_split_gemm<<<sp.ntask, SG_THREADS, smem, st>>>(sp.d_tasks, sp.d_probs, sp.d_segs, sp.d_roles, S, ss.sl, ss.ex,
+                                                     outs, hv0, hv1, ss.err);
+  }
+  if (sp.nptask > 0) k_split_pair<<<sp.nptask, 256, 0, st>>>(sp.d_ptasks, sp.d_pairs, ss.V, outs, hv0, hv1);
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+int check_err(SplitState& ss, cudaStream_t st) {
+  if (!ss.err) return QD_OK;
+  int h = 0;
+  QD_CUDA(cudaMemcpyAsync(&h, ss.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  QD_CUDA(cudaStreamSynchronize(st));
+  if (h) {
+    set_error("split product: tensor-core wait timed out");
+    return QD_ERR_CUDA;
+  }
+  return QD_OK;
+}
+
+void free_state(SplitState* ss) {
+  if (!ss) return;
+  for (auto& kv : ss->plans) free_plan(kv.second);
+  for (void* p : {(void*)ss->sl, (void*)ss->ex, (void*)ss->V, (void*)ss->err})
+    if (p) cudaFree(p);
+  delete ss;
+}
+
+}  // namespace
+
+// the commutator's GEMM programs in the split form (L->split_slices slices)
+int run_program_split(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
+                      unsigned maskB) {
+  SplitState*& ss = reinterpret_cast<SplitState*&>(L->split);
+  if (!ss) ss = new SplitState();
+  auto key = std::make_tuple((const void*)&P, maskA, maskB);
+  auto it = ss->plans.find(key);
+  if (it == ss->plans.end()) {
+    SplitPlan sp;
+    int rc = build_plan(P, maskA, maskB, sp);
+    if (rc) {
+      free_plan(sp);
+      return rc;
+    }
+    it = ss->plans.emplace(key, sp).first;
+  }
+  SPtrs b;
+  for (int i = 0; i < SG_NBUF; ++i) b.p[i] = i < 7 ? bufs[i] : nullptr;
+  int rc = run_plan(*ss, it->second, L->split_slices, b, hv0, hv1, L->stream, &L->ws_bytes);
+  L->nlaunch += 3;
+  return rc;
+}
+
+void split_free(qd_layout* L) {
+  free_state(reinterpret_cast<SplitState*>(L->split));
+  L->split = nullptr;
+}
+
 }  // namespace qd
 
 using namespace qd;
 
+extern "C" {
+
 // ---------------------------------------------------------------------------
 // C ABI: one split-precision product with dgemm's argument meaning
 // ---------------------------------------------------------------------------
-extern "C" int qd_gemm_split(int device, void* stream, char transa, char transb, int M, int N, int K, double alpha,
-                             const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc,
-                             int slices) {
+int qd_gemm_split(int device, void* stream, char transa, char transb, int M, int N, int K, double alpha,
+                  const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc, int slices) {
   const bool ta = transa == 'T' || transa == 't', tb = transb == 'T' || transb == 't';
   if (!(ta || transa == 'N' || transa == 'n') || !(tb || transb == 'N' || transb == 'n') || M < 0 || N < 0 ||
       K < 0 || slices < 1 || slices > SG_MAXS || (M > 0 && N > 0 && (!C || ldc < M)) ||
@@ -335,60 +640,55 @@ extern "C" int qd_gemm_split(int device, void* stream, char transa, char transb,
   QD_CUDA(cudaSetDevice(device));
   cudaStream_t st = (cudaStream_t)stream;
   if (M == 0 || N == 0) return QD_OK;
-  const int S = slices;
-  const int mpad = (M + SG_BM - 1) / SG_BM * SG_BM, npad = (N + SG_BN - 1) / SG_BN * SG_BN;
-  const int kpad = std::max(SG_BK, (K + SG_BK - 1) / SG_BK * SG_BK);
-  const size_t bytesA = (size_t)S * mpad * kpad * 2, bytesB = (size_t)S * npad * kpad * 2;
-  uint8_t* ws = nullptr;
-  const size_t off_ex = bytesA + bytesB, off_err = off_ex + sizeof(int) * (mpad + npad);
-  const size_t off_meta = (off_err + sizeof(int) + 255) & ~(size_t)255;
-  const int ntask = (mpad / SG_BM) * (npad / SG_BN);
-  const size_t bytes = off_meta + sizeof(SRole) * 2 + sizeof(SSeg) + sizeof(SProb) + sizeof(STask) * ntask + 64;
-  QD_CUDA(cudaMallocAsync((void**)&ws, bytes, st));
-  __nv_bfloat16* slA = (__nv_bfloat16*)ws;
-  __nv_bfloat16* slB = (__nv_bfloat16*)(ws + bytesA);
-  int* exA = (int*)(ws + off_ex);
-  int* exB = exA + mpad;
-  int* d_err = (int*)(ws + off_err);
-  QD_CUDA(cudaMemsetAsync(exA, 0, sizeof(int) * (mpad + npad) + sizeof(int), st));
-  // op(A)(m,k) = ta ? A[k + m lda] : A[m + k lda]; op(B)(k,n) = tb ? B[n + k ldb] : B[k + n ldb]
-  const double* Ab = K > 0 ? A : C;
-  const double* Bb = K > 0 ? B : C;
-  k_split_slice<<<(mpad * 32 + 255) / 256, 256, 0, st>>>(Ab, ta ? lda : 1, ta ? 1 : lda, M, K, S, mpad, kpad, slA,
-                                                        exA);
-  k_split_slice<<<(npad * 32 + 255) / 256, 256, 0, st>>>(Bb, tb ? 1 : ldb, tb ? ldb : 1, N, K, S, npad, kpad, slB,
-                                                        exB);
-  // one problem, one segment, every tile
-  uint8_t* hmeta = (uint8_t*)malloc(bytes - off_meta);
-  SRole* hr = (SRole*)hmeta;
-  hr[0] = SRole{slA, exA, mpad, kpad};
-  hr[1] = SRole{slB, exB, npad, kpad};
-  SSeg* hs = (SSeg*)(hr + 2);
-  *hs = SSeg{0, 1, K, alpha};
-  SProb* hp = (SProb*)(hs + 1);
-  *hp = SProb{M, N, ldc, 0, K > 0 ? 1 : 0, 2, 0, C, beta};
-  STask* ht = (STask*)(hp + 1);
-  for (int i = 0, k = 0; i < mpad / SG_BM; ++i)
-    for (int j = 0; j < npad / SG_BN; ++j, ++k) ht[k] = STask{0, (short)i, (short)j};
-  uint8_t* dmeta = ws + off_meta;
-  QD_CUDA(cudaMemcpyAsync(dmeta, hmeta, bytes - off_meta, cudaMemcpyHostToDevice, st));
-  QD_CUDA(cudaStreamSynchronize(st));
-  free(hmeta);
-  const size_t smem = split_gemm_smem(S);
-  QD_CUDA(cudaFuncSetAttribute(k_split_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const SRole* dr = (const SRole*)dmeta;
-  const SSeg* ds = (const SSeg*)(dr + 2);
-  const SProb* dp = (const SProb*)(ds + 1);
-  const STask* dt = (const STask*)(dp + 1);
-  k_split_gemm<<<ntask, SG_THREADS, smem, st>>>(dt, dp, ds, dr, S, d_err);
-  QD_CUDA(cudaGetLastError());
-  int herr = 0;
-  QD_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  QD_CUDA(cudaStreamSynchronize(st));
-  QD_CUDA(cudaFreeAsync(ws, st));
-  if (herr) {
-    set_error("qd_gemm_split: tensor-core wait timed out");
-    return QD_ERR_CUDA;
+  // a one-problem program: buffers 0 = A, 1 = B, 4 = C
+  GemmProgram G;
+  GProb g;
+  std::memset(&g, 0, sizeof(g));
+  g.M = M;
+  g.N = N;
+  g.ldc = ldc;
+  g.mode = GM_ACC;
+  g.outbuf = 4;
+  g.nseg = K > 0 ? 1 : 0;
+  G.probs.push_back(g);
+  if (K > 0) {
+    GSeg s;
+    std::memset(&s, 0, sizeof(s));
+    s.lda = lda;
+    s.ldb = ldb;
+    s.K = K;
+    s.srcA = 0;
+    s.srcB = 1;
+    s.tA = ta;
+    s.tB = tb;
+    s.depA = s.depB = -1;
+    s.c = alpha;
+    G.segs.push_back(s);
   }
-  return QD_OK;
+  // C = V + beta C: scale C first (beta = 0 overwrites, as dgemm), then accumulate
+  if (beta == 0.0) {
+    QD_CUDA(cudaMemset2DAsync(C, sizeof(double) * ldc, 0, sizeof(double) * M, N, st));
+  } else if (beta != 1.0) {
+    const i64 n = (i64)M * N;
+    k_scale2d<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(C, ldc, M, n, beta);
+  }
+  SplitState ss;
+  SplitPlan sp;
+  int rc = build_plan(G, 0u, 0u, sp);
+  if (!rc) {
+    SPtrs b;
+    for (int i = 0; i < SG_NBUF; ++i) b.p[i] = nullptr;
+    b.p[0] = A;
+    b.p[1] = B;
+    b.p[4] = C;
+    rc = run_plan(ss, sp, slices, b, 1.0, 1.0, st, nullptr);
+    if (!rc) rc = check_err(ss, st);
+  }
+  cudaStreamSynchronize(st);
+  free_plan(sp);
+  for (void* p : {(void*)ss.sl, (void*)ss.ex, (void*)ss.V, (void*)ss.err})
+    if (p) cudaFree(p);
+  return rc;
 }
+
+}  // extern "C"
