@@ -72,6 +72,9 @@ def parse():
                     help="warmstart: target s as fractions of the training flows' median final s; the first "
                          "is the headline, the others are reported beside it")
     ap.add_argument("--workload", choices=["flow", "commutator", "batch", "warmstart"], default="flow")
+    ap.add_argument("--split", type=int, default=0,
+                    help="flow/commutator: block contractions in the split form with this many BF16 slices "
+                         "(0 = plain FP64)")
     ap.add_argument("--hw", type=float, default=0.5)
     ap.add_argument("--pandya", action="store_true", help="flow: add the particle-hole channel")
     ap.add_argument("--hf-mix", type=float, default=0.5, help="flow: HF density mixing (1 = plain iteration)")
@@ -197,10 +200,19 @@ def measured_dgemm_tflops(torch, device) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_peak: float) -> dict:
+def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_peak: float, split: int = 0) -> dict:
     """Roofline of the stage with the largest device time."""
     name, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
     per_launch_s = (ms / max(cnt, 1)) / 1e3
+    if split and name in ("ladder_gemm", "pandya_gemm"):
+        # the split form runs slice_pairs(split) BF16 products per FP64 product
+        f = flops["ladder"] if name == "ladder_gemm" else flops["pandya"] / 2
+        return {"kernel": "k_split_gemm (%s, %d slices)" % (name, split), "bound": "tensor",
+                "achieved": f * slice_pairs(split) / per_launch_s / 1e12, "peak": bf16_peak_tflops(),
+                "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured, burst)",
+                "algorithmic_per_launch": f * slice_pairs(split),
+                "note": "BF16 slice-product FLOPs = FP64-algorithm FLOPs x %d slice pairs; the stage time "
+                        "includes slicing the operands" % slice_pairs(split)}
     if name == "ladder_gemm":
         return {"kernel": "k_grouped_gemm (ladders of commutator_222)", "bound": "tensor",
                 "achieved": flops["ladder"] / per_launch_s / 1e12, "peak": dgemm_peak, "unit": "TFLOP/s",
@@ -243,6 +255,23 @@ def hbm_peak_gbs() -> float:
             return float(json.load(fh)["hbm_gbs"])
     except Exception:
         return 6650.0
+
+
+def bf16_peak_tflops() -> float:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
+def form_name(split: int) -> str:
+    return ("split: block contractions as %d BF16 slices per operand (tcgen05, exact FP32 chunks, FP64 sum)"
+            % split) if split else "plain FP64"
+
+
+def slice_pairs(split: int) -> int:
+    return split * (split + 1) // 2
 
 
 def cpu_baseline_full(a: np.ndarray, b: np.ndarray, flops_total: float) -> dict:
@@ -310,6 +339,36 @@ def run_reference(args, world, rank):
             "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def split_errors(P, got, ref) -> dict:
+    """Relative Frobenius error per stored part (and E0) of a split-form
+    result against the FP64 result of the same inputs."""
+    n, mp = P.nbody, P.msp - P.nbody
+    parts = {"E0": [np.array([0])]}
+    o = 1
+    for name, sz in (("fhh", n * n), ("fpp", mp * mp), ("fph", mp * n)):
+        parts[name] = [np.arange(o, o + sz)]
+        o += sz
+    names = ["Vhhhh", "Vpppp", "Vpphh", "Vphph", "Vppph", "Vphhh"]
+    for nm in names:
+        parts[nm] = []
+    for q in range(P.nblock):
+        nh, nb, npp = (int(x) for x in P.dims[q, :3])
+        for k, sz in enumerate((nh * nh, npp * npp, npp * nh, nb * nb, npp * nb, nb * nh)):
+            if sz:
+                st = int(P.offs[q, k])
+                parts[names[k]].append(np.arange(st, st + sz))
+    out = {}
+    for nm, ix in parts.items():
+        if not ix:
+            continue
+        ix = np.concatenate(ix)
+        d = np.linalg.norm(got[ix] - ref[ix])
+        r = np.linalg.norm(ref[ix])
+        out[nm] = float(d / r) if r > 0 else float(d)
+    out["max"] = max(out.values())
+    return out
 
 
 def sample_flops(P, stride):
@@ -401,6 +460,13 @@ def run_flow(args, world, rank, local):
     def flow():
         return qd.magnus_flow(H, HS, pandya=args.pandya, full_norm=True, max_iter=1000)
 
+    fp64 = None
+    if args.split:
+        # the plain FP64 flow on the same Hamiltonian, for the error of the split form
+        _, r0 = flow()
+        fp64 = {"E_gs": float(r0.E0), "flow_steps": int(r0.iterations), "commutators": int(r0.commutators)}
+        P.split = args.split
+
     for _ in range(max(1, args.warmup)):
         tr, res = flow()
     clocks = ClockSampler(local)
@@ -457,7 +523,9 @@ def run_flow(args, world, rank, local):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
-                "config": {"workload": flow_desc(args), "form": "plain FP64", "E_HF": float(vec[0]),
+                "config": {"workload": flow_desc(args), "form": form_name(args.split), "E_HF": float(vec[0]),
+                           "fp64_flow": fp64,
+                           "dE_vs_fp64": (abs(float(res.E0) - fp64["E_gs"]) if fp64 else None),
                            "E_gs": float(res.E0), "flow_steps": int(res.iterations), "rejected": int(res.rejected),
                            "commutators": comms, "s_final": float(res.s), "hf_setup_s": setup_s,
                            "hf_iterations": hf_it, "hf_mix": args.hf_mix, "tbme": args.tbme,
@@ -724,6 +792,16 @@ def main():
     a = qd.random_operator(P, -1, SEED_OMEGA)
     b = qd.random_operator(P, 1, SEED_H)
     A, B, C = qd.FullHam(P, -1, a), qd.FullHam(P, 1, b), qd.FullHam(P, 1)
+    err = None
+    if args.split:
+        # error of the split form against the plain FP64 engine on the same inputs
+        qd.commutator(A, B, C, pandya=True)
+        ref = C.download()
+        P.split = args.split
+        qd.commutator(A, B, C, pandya=True)
+        got = C.download()
+        err = split_errors(P, got, ref)
+    P.split = args.split
 
     for _ in range(args.warmup):
         qd.commutator(A, B, C, pandya=True)
@@ -774,7 +852,7 @@ def main():
     e2e = {"value": world * fl["total"] / e2e_sec / 1e12, "unit": "TFLOP/s",
            "h2d_bytes_per_step": 2 * 8 * neq, "d2h_bytes_per_step": 8 * neq, "ms_per_step": 1e3 * e2e_sec}
 
-    roof = stage_roofline(prof, fl, neq2b, dgemm_peak, hbm_peak_gbs())
+    roof = stage_roofline(prof, fl, neq2b, dgemm_peak, hbm_peak_gbs(), args.split)
     roof["frac"] = roof["achieved"] / roof["peak"]
     stage = max(prof.items(), key=lambda kv: kv[1][0])[0]
     roof["traffic"] = NCU_TRAFFIC[stage] * neq / NCU_NEQ if stage in NCU_TRAFFIC else None
@@ -792,6 +870,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox operators)",
             "config": {"workload": "FP64 commutator [Omega,H], N=%d R=%d (%d spin-orbitals), random "
                                    "(anti)Hermitian operators, Pandya channel on" % (n, P.emax, P.msp),
+                       "form": form_name(args.split), "error_vs_fp64": err,
                        "n_electrons": n, "shells": P.emax, "neq_per_operator": neq,
                        "flops_per_step": fl["total"], "flops_breakdown": fl,
                        "l2": "inputs larger than L2 (two 495.6 MB operators read per step)",
