@@ -96,45 +96,68 @@ __global__ void k_ftab(DevLayout L, const int* __restrict__ sbase, const double*
   F[nfent + pos] = make_double2(fak, fbk);
 }
 
-// One direction of one group pair, by one warp.  DIR 0: fibers are the
-// columns k2 of the cell grid (length N = |G_g|, F_g); DIR 1: the rows k1
-// (length N = |G_h|, F_h).  Lane (slot, r) keeps row r of F in registers and,
-// for the fibers (and staged columns j) of its slot, forms
-// sum_k F(r,k) (FA * VB - FB * VA)(cell k) into the fiber's cell r: DIR 0
-// assigns (it reaches every cell once), DIR 1 adds.  The lanes of a slot read
-// the same cells (shared-memory broadcast).
+__device__ __forceinline__ void dmma122(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// One direction of one group pair, by one warp, on the FP64 tensor pipe:
+// Y(r, col) = sum_k F(r,k) (FA * VB - FB * VA)(k, col) as m8n8k4 products.
+// DIR 0: F = F_g (N = |G_g|), columns col = (k2, j), cell (k, col) =
+// base + k n2 + k2 (assigns: it reaches every cell once); DIR 1: F = F_h
+// (N = |G_h|), columns col = (k1, j), cell = base + k1 n2 + k (adds).
+// Fragments (m8n8k4): A row lane/4, k lane%4; B k lane%4, column lane/4;
+// D row lane/4, columns 2 (lane%4) + {0,1}.  Out-of-range rows, k and
+// columns are selected to zero (never multiplied with shared-memory data).
 template <int N, int TJ, int DIR>
 __device__ __forceinline__ void pair_dir(int base, int n1, int n2, int fofs, int lane, const double2* __restrict__ Vc,
                                          double* __restrict__ Yc, const double2* __restrict__ F) {
-  constexpr int NSLOT = 32 / N;
-  const int slot = lane / N, r = lane - slot * N;
-  if (slot >= NSLOT) return;
-  double2 f[N];
+  constexpr int MT = (N + 7) / 8, KS = (N + 3) / 4;
+  double fa[MT][KS], fb[MT][KS];
 #pragma unroll
-  for (int k = 0; k < N; ++k) f[k] = __ldg(&F[fofs + r * N + k]);
-  const int nfib = (DIR ? n1 : n2) * TJ;
-  const int step = (DIR ? 1 : n2) * TJ;  // between the fiber's cells, in staged elements
-  for (int it = slot; it < nfib; it += NSLOT) {
-    const int fi = it / TJ, j = it % TJ;
-    const int e0 = (DIR ? base + fi * n2 : base + fi) * TJ + j;
-    const double2* v = Vc + e0;
-    double y0 = 0.0, y1 = 0.0;
+  for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-    for (int k = 0; k < N; ++k) {
-      const double2 x = v[k * step];
-      if (k & 1) {
-        y1 = fma(f[k].x, x.y, y1);
-        y1 = fma(-f[k].y, x.x, y1);
-      } else {
-        y0 = fma(f[k].x, x.y, y0);
-        y0 = fma(-f[k].y, x.x, y0);
+    for (int ks = 0; ks < KS; ++ks) {
+      const int r = 8 * mt + (lane >> 2), k = 4 * ks + (lane & 3);
+      double2 f = make_double2(0.0, 0.0);
+      if (r < N && k < N) f = __ldg(&F[fofs + r * N + k]);
+      fa[mt][ks] = f.x;
+      fb[mt][ks] = -f.y;
+    }
+  const int ncol = (DIR ? n1 : n2) * TJ;
+  auto cell = [&](int k, int col) -> int {  // staged element of (k, col)
+    return DIR ? (base + (col / TJ) * n2 + k) * TJ + (col % TJ) : (base + k * n2) * TJ + col;
+  };
+  for (int c0 = 0; c0 < ncol; c0 += 8) {
+    double d[MT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) d[mt][0] = d[mt][1] = 0.0;
+    const int bcol = c0 + (lane >> 2);
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+      const int k = 4 * ks + (lane & 3);
+      double2 v = make_double2(0.0, 0.0);
+      if (k < N && bcol < ncol) v = Vc[cell(k, bcol)];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        dmma122(d[mt][0], d[mt][1], fa[mt][ks], v.y);
+        dmma122(d[mt][0], d[mt][1], fb[mt][ks], v.x);
       }
     }
-    double* yo = Yc + e0 + r * step;
-    if (DIR)
-      *yo += y0 + y1;
-    else
-      *yo = y0 + y1;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = 8 * mt + (lane >> 2), c = c0 + 2 * (lane & 3) + e;
+        if (r < N && c < ncol) {
+          double* y = Yc + cell(r, c);
+          if (DIR)
+            *y += d[mt][e];
+          else
+            *y = d[mt][e];
+        }
+      }
   }
 }
 
