@@ -246,7 +246,7 @@ NCU_TRAFFIC = {"ladder_gemm": 794.761728e6 + 162.643712e6, "pandya_gemm": 200.46
 # the N=20, R=18 capture (29,618,726 entries per operator): scaled to the
 # flow's basis by entries per operator
 NCU_FLOW_NEQ = 29618726
-NCU_FLOW_TRAFFIC = {"c122": 718.3e6 + 224.9e6}
+NCU_FLOW_TRAFFIC = {"c122": 712.7e6 + 232.8e6}
 
 
 def hbm_peak_gbs() -> float:
@@ -512,8 +512,8 @@ def run_flow(args, world, rank, local):
             "note": "stage with the most device time, per launch = per commutator; bytes = read A, B and "
                     "write C two-body parts once",
             "traffic": NCU_FLOW_TRAFFIC[name] * P.neq / NCU_FLOW_NEQ if name in NCU_FLOW_TRAFFIC else None,
-            "traffic_source": "ncu dram bytes of the k_122 launches of one commutator at N=20 R=18, scaled by "
-                              "entries per operator" if name in NCU_FLOW_TRAFFIC else None}
+            "traffic_source": "ncu dram bytes of the k_122_pass launches of one commutator at N=20 R=18, "
+                              "scaled by entries per operator" if name in NCU_FLOW_TRAFFIC else None}
     roof["frac"] = roof["achieved"] / roof["peak"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
