@@ -22,12 +22,14 @@
 // scale 2^(e_m + f_n - 7d).  The only rounding is the truncation of the
 // slice series and the FP64 summation.
 //
-// Kernel.  One CTA (128 threads) per 128 x 64 output tile; per 64-wide K
-// step the S slices of the A tile (128 x 64) and of the B tile (64 x 64) are
-// staged in shared memory in the K-major 128-byte-swizzled layout (cp.async),
-// one thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M=128,
-// N=64, K=16) for every slice pair of the triangle and commits to an
-// mbarrier; accumulators live in TMEM (S diagonals x 64 columns).
+// Kernel.  Persistent CTAs (one per SM) walk the 128 x 64 output tiles.  Per
+// 64-wide K step a producer warp bulk-copies the S slices of the A tile
+// (128 x 64) and of the B tile (64 x 64), stored pre-swizzled, into one of
+// NST shared-memory stages; an MMA warp issues tcgen05.mma (kind::f16,
+// BF16 x BF16 -> FP32, M=128, N=64, K=16) for every slice pair of the
+// triangle into TMEM (S diagonals x 64 columns, two buffers when they fit)
+// and commits to mbarriers; four epilogue warps read each finished chunk
+// with tcgen05.ld and accumulate it in FP64 while the next chunk runs.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -39,7 +41,7 @@
 
 namespace qd {
 
-constexpr int SG_BM = 128, SG_BN = 64, SG_BK = 64, SG_THREADS = 128;
+constexpr int SG_BM = 128, SG_BN = 64, SG_BK = 64;
 constexpr int SG_MAXS = 8;
 constexpr size_t SG_ATILE = (size_t)SG_BM * SG_BK * 2;  // bytes per A slice tile
 constexpr size_t SG_BTILE = (size_t)SG_BN * SG_BK * 2;  // bytes per B slice tile
@@ -92,6 +94,15 @@ __host__ __device__ inline int split_tmem_cols(int S) {
 // ---------------------------------------------------------------------------
 // slicing: role (x(i,k) = X[i*si + k*sk]) -> exponents and S slices
 // ---------------------------------------------------------------------------
+// Slices are stored pre-tiled: per role and slice, 128-row x 64-K tiles of
+// 16 KB, row-tile major, each tile already in the K-major 128-byte-swizzled
+// shared-memory layout (row r at r*128 bytes, 16-byte chunk c at
+// (c ^ (r & 7))*16), so one bulk copy moves a whole tile (or a 64-row half).
+__device__ __forceinline__ i64 tiled_off(int i, int k, int kpad) {
+  const int r = i & 127, kk = k & 63;
+  return ((i64)(i >> 7) * (kpad >> 6) + (k >> 6)) * 8192 + r * 64 + ((((kk >> 3) ^ (r & 7)) << 3) | (kk & 7));
+}
+
 // one warp per (role, row i): max |x(i,k)| over k, then the slices of the row;
 // rows beyond R (padding) get zero slices
 __global__ void k_split_slice(const SRole* __restrict__ roles, const i64* __restrict__ rowstart, int nroles,
@@ -109,14 +120,16 @@ __global__ void k_split_slice(const SRole* __restrict__ roles, const i64* __rest
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   const int e = mx > 0.0 ? ilogb(mx) + 1 : 0;
   if (lane == 0) exbase[ro.ex_off + i] = e;
-  __nv_bfloat16* out = slbase + (i64)S * ro.unit + (i64)i * ro.kpad;
+  __nv_bfloat16* out = slbase + (i64)S * ro.unit;
+  const i64 sstride = (i64)ro.rpad * ro.kpad;
   for (int k = lane; k < ro.kpad; k += 32) {
     double x = (i < ro.R && k < ro.K) ? scalbn(X[i * ro.si + k * ro.sk], -e) : 0.0;
+    const i64 o = tiled_off(i, k, ro.kpad);
     for (int sl = 0; sl < S; ++sl) {
       const double t = x * 128.0;
       const double d = rint(t);
       x = t - d;
-      out[(i64)sl * ro.rpad * ro.kpad + k] = __float2bfloat16_rn((float)d);
+      out[sl * sstride + o] = __float2bfloat16_rn((float)d);
     }
   }
 }
@@ -179,46 +192,58 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ void cp16(unsigned saddr, const void* g) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
-
-// stage rows [row0, row0+rows) x K [k0, k0+64) of one slice (rows kpad
-// apart) into a swizzled tile: 16-byte chunk c of row i lands at
-// i*128 + ((c ^ (i & 7)) * 16)
-__device__ __forceinline__ void stage_tile(unsigned sbase, const __nv_bfloat16* g, int kpad, int rows) {
-  for (int e = threadIdx.x; e < rows * 8; e += SG_THREADS) {
-    const int i = e >> 3, c = e & 7;
-    cp16(sbase + i * 128 + ((c ^ (i & 7)) << 4), g + (i64)i * kpad + c * 8);
-  }
+__device__ __forceinline__ void mbar_init_n(uint64_t* bar, unsigned n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // ---------------------------------------------------------------------------
-// the grouped split GEMM
+// the grouped split GEMM: warp-specialised pipeline
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SG_THREADS, 1)
-    k_split_gemm(const STask* __restrict__ tasks, const SProb* __restrict__ probs, const SSeg* __restrict__ segs,
-                 const SRole* __restrict__ roles, int S, const __nv_bfloat16* __restrict__ slbase,
-                 const int* __restrict__ exbase, SPtrs outs, double hv0, double hv1, int* __restrict__ err) {
+// warps 0-3: epilogue (TMEM lanes 32w.., FP64 accumulation, output);
+// warp 4: producer (bulk copies of the slice tiles into NST stages);
+// warp 5: MMA issuer (tcgen05.mma into NB TMEM accumulator buffers).
+// Barriers: full/empty per stage, accf/acce per accumulator buffer; every
+// wait is bounded and a timeout sets `fail` (all roles then stop).
+constexpr int SG_WARPS = 6, SG_THREADS_P = SG_WARPS * 32, SG_MAXST = 4;
+
+template <int S>
+__global__ void __launch_bounds__(SG_THREADS_P, 1)
+    k_split_gemm(const STask* __restrict__ tasks, int ntask, const SProb* __restrict__ probs,
+                 const SSeg* __restrict__ segs, const SRole* __restrict__ roles, int NST, int NB,
+                 const __nv_bfloat16* __restrict__ slbase, const int* __restrict__ exbase, SPtrs outs, double hv0,
+                 double hv1, int* __restrict__ err) {
   extern __shared__ uint8_t smraw[];
-  __shared__ uint64_t bar;
+  __shared__ uint64_t full[SG_MAXST], empty[SG_MAXST], accf[2], acce[2];
   __shared__ unsigned tslot;
-  __shared__ int fx[SG_BN];
-  __shared__ int fail;
-  // 1024-byte aligned tiles: A slices then B slices
-  const unsigned sraw = smem_u32(smraw);
-  const unsigned sA = (sraw + 1023u) & ~1023u;
-  const unsigned sB = sA + (unsigned)(S * SG_ATILE);
+  __shared__ double fsc[SG_BN];  // 2^(column exponent) of the current segment
+  __shared__ volatile int fail;
+  const unsigned sbase = (smem_u32(smraw) + 1023u) & ~1023u;
+  const unsigned stage_bytes = (unsigned)(S * (SG_ATILE + SG_BTILE));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ncols = split_tmem_cols(S);
-
-  const STask t = tasks[blockIdx.x];
-  const SProb P = probs[t.prob];
-  const int row0 = t.ti * SG_BM, col0 = t.tj * SG_BN;
-  const int m = row0 + threadIdx.x;  // this thread's output row (TMEM lane)
+  const int ncols = split_tmem_cols(NB * S);
+  const int kcs = split_kchunk(S) / SG_BK;  // K steps per exact chunk
 
   if (threadIdx.x == 0) {
-    mbar_init(&bar);
+    for (int i = 0; i < NST; ++i) {
+      mbar_init_n(&full[i], 1);
+      mbar_init_n(&empty[i], 1);
+    }
+    for (int i = 0; i < NB; ++i) {
+      mbar_init_n(&accf[i], 1);
+      mbar_init_n(&acce[i], 128);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fail = 0;
   }
   if (warp == 0) {
@@ -231,100 +256,160 @@ __global__ void __launch_bounds__(SG_THREADS, 1)
   __syncthreads();
   tc_fence_after();
   const unsigned tbase = tslot;
-  const int kc = split_kchunk(S);
 
-  double acc[SG_BN];
-#pragma unroll
-  for (int j = 0; j < SG_BN; ++j) acc[j] = 0.0;
-  unsigned phase = 0;
-
-  for (int sg = 0; sg < P.nseg && !fail; ++sg) {
-    const SSeg G = segs[P.seg0 + sg];
-    const SRole RA = roles[G.ra], RB = roles[G.rb];
-    const double alpha = G.c * (G.pa ? hv0 : 1.0) * (G.pb ? hv1 : 1.0);
-    const __nv_bfloat16* slA = slbase + (i64)S * RA.unit + (i64)row0 * RA.kpad;
-    const __nv_bfloat16* slB = slbase + (i64)S * RB.unit + (i64)col0 * RB.kpad;
-    const i64 sstrA = (i64)RA.rpad * RA.kpad, sstrB = (i64)RB.rpad * RB.kpad;
-    if (threadIdx.x < SG_BN) fx[threadIdx.x] = (col0 + threadIdx.x < P.N) ? exbase[RB.ex_off + col0 + threadIdx.x] : 0;
-    const int em = m < P.M ? exbase[RA.ex_off + m] : 0;
-    const int ksteps = (G.K + SG_BK - 1) / SG_BK;
-    for (int c0 = 0; c0 < ksteps && !fail; c0 += kc / SG_BK) {
-      const int c1 = min(ksteps, c0 + kc / SG_BK);
-      unsigned init = 0;  // diagonals written in this chunk
-      for (int ks = c0; ks < c1; ++ks) {
-        for (int s = 0; s < S; ++s) {
-          stage_tile(sA + s * (unsigned)SG_ATILE, slA + s * sstrA + ks * SG_BK, RA.kpad, SG_BM);
-          stage_tile(sB + s * (unsigned)SG_BTILE, slB + s * sstrB + ks * SG_BK, RB.kpad, SG_BN);
-        }
-        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          tc_fence_after();
-#pragma unroll 1
-          for (int k16 = 0; k16 < SG_BK / 16; ++k16)
-            for (int s = 0; s < S; ++s)
-              for (int u = 0; u + s < S; ++u) {  // slice pair (s+1, u+1), diagonal s+u+2
-                const int d = s + u;
-                const uint64_t ad = umma_desc(sA + s * (unsigned)SG_ATILE + k16 * 32);
-                const uint64_t bd = umma_desc(sB + u * (unsigned)SG_BTILE + k16 * 32);
-                umma_bf16(tbase + d * SG_BN, ad, bd, (init >> d) & 1u);
-                init |= 1u << d;
-              }
-          umma_commit(&bar);
-        }
-        // the tiles are reused by the next step: wait for the MMAs
-        if (!mbar_wait(&bar, phase)) {
-          if (lane == 0) atomicExch(&fail, 1);
-        }
-        phase ^= 1u;
-        __syncthreads();
-        if (fail) break;
-      }
-      if (fail) break;
-      tc_fence_after();
-      // read the diagonals of this chunk and add them in FP64
-      for (int d = 0; d < S; ++d) {
-        const double rs = ldexp(alpha, em - 7 * (d + 2));
-#pragma unroll
-        for (int q = 0; q < SG_BN / 16; ++q) {
-          float v[16];
-          tmem_ld16(tbase + ((unsigned)(warp * 32) << 16) + d * SG_BN + q * 16, v);
-#pragma unroll
-          for (int j = 0; j < 16; ++j) acc[q * 16 + j] = fma((double)v[j], ldexp(rs, fx[q * 16 + j]), acc[q * 16 + j]);
+  if (warp == 4) {
+    // ---- producer
+    if (lane == 0) {
+      int it = 0;
+      for (int tk = blockIdx.x; tk < ntask && !fail; tk += gridDim.x) {
+      const STask t = tasks[tk];
+      const SProb P = probs[t.prob];
+      const int col0 = t.tj * SG_BN;
+      for (int sg = 0; sg < P.nseg && !fail; ++sg) {
+        const SSeg G = segs[P.seg0 + sg];
+        const SRole RA = roles[G.ra], RB = roles[G.rb];
+        const int ksteps = (G.K + SG_BK - 1) / SG_BK;
+        const __nv_bfloat16* a0 = slbase + (i64)S * RA.unit + (i64)t.ti * (RA.kpad >> 6) * 8192;
+        const __nv_bfloat16* b0 =
+            slbase + (i64)S * RB.unit + (i64)(col0 >> 7) * (RB.kpad >> 6) * 8192 + ((col0 >> 6) & 1) * 4096;
+        const i64 sa = (i64)RA.rpad * RA.kpad, sb = (i64)RB.rpad * RB.kpad;
+        for (int ks = 0; ks < ksteps; ++ks, ++it) {
+          const int st = it % NST;
+          if (!mbar_wait(&empty[st], ((it / NST) & 1) ^ 1)) {
+            fail = 1;
+            break;
+          }
+          mbar_expect(&full[st], stage_bytes);
+          const unsigned sA = sbase + st * stage_bytes, sB = sA + S * (unsigned)SG_ATILE;
+          for (int s = 0; s < S; ++s) {
+            bulk_g2s(sA + s * (unsigned)SG_ATILE, a0 + s * sa + (i64)ks * 8192, (unsigned)SG_ATILE, &full[st]);
+            bulk_g2s(sB + s * (unsigned)SG_BTILE, b0 + s * sb + (i64)ks * 8192, (unsigned)SG_BTILE, &full[st]);
+          }
         }
       }
-      tc_fence_before();
-      __syncthreads();
+      }
     }
-    __syncthreads();  // fx is rewritten by the next segment
-  }
-  if (fail && threadIdx.x == 0) atomicExch(err, 1);
-  // epilogue: thread = row m, columns col0.. (consecutive rows per column)
-  if (!fail && m < P.M) {
-    double* out = const_cast<double*>(outs.p[P.outbuf]) + P.offC + m;
-    const int nn = min(SG_BN, P.N - col0);
+  } else if (warp == 5) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      int it = 0, ch = 0;
+      for (int tk = blockIdx.x; tk < ntask && !fail; tk += gridDim.x) {
+      const SProb P = probs[tasks[tk].prob];
+      for (int sg = 0; sg < P.nseg && !fail; ++sg) {
+        const int ksteps = (segs[P.seg0 + sg].K + SG_BK - 1) / SG_BK;
+        for (int c0 = 0; c0 < ksteps && !fail; c0 += kcs, ++ch) {
+          const int b = ch % NB;
+          if (!mbar_wait(&acce[b], ((ch / NB) & 1) ^ 1)) {
+            fail = 1;
+            break;
+          }
+          tc_fence_after();
+          const unsigned dbase = tbase + b * S * SG_BN;
+          const int c1 = min(ksteps, c0 + kcs);
+          for (int ks = c0; ks < c1; ++ks, ++it) {
+            const int st = it % NST;
+            if (!mbar_wait(&full[st], (it / NST) & 1)) {
+              fail = 1;
+              break;
+            }
+            tc_fence_after();
+            const unsigned sA = sbase + st * stage_bytes, sB = sA + S * (unsigned)SG_ATILE;
+            // descriptors advance by (byte offset >> 4) within the stage
+            const uint64_t dA = umma_desc(sA), dB = umma_desc(sB);
+            const unsigned first = ks == c0 ? 0u : 1u;
 #pragma unroll
-    for (int j = 0; j < SG_BN; ++j) {
-      if (j >= nn) break;
-      double* p = out + (i64)(col0 + j) * P.ldc;
-      if (P.mode == 0)
-        *p = acc[j];
-      else if (P.mode == 1)
-        *p += acc[j];
-      else
-        *p = acc[j] + (P.beta == 0.0 ? 0.0 : P.beta * *p);
+            for (int k16 = 0; k16 < SG_BK / 16; ++k16)
+#pragma unroll
+              for (int s = 0; s < S; ++s)
+#pragma unroll
+                for (int u = 0; u + s < S; ++u)  // slice pair (s+1, u+1), diagonal s+u+2
+                  umma_bf16(dbase + (s + u) * SG_BN, dA + ((s * (unsigned)SG_ATILE + k16 * 32) >> 4),
+                            dB + ((u * (unsigned)SG_BTILE + k16 * 32) >> 4),
+                            (k16 | s) ? 1u : first);  // each diagonal starts at (k16, s) = (0, 0)
+            umma_commit(&empty[st]);  // the stage is free once these MMAs complete
+          }
+          umma_commit(&accf[b]);  // the chunk's diagonals are complete
+        }
+      }
+      }
+    }
+  } else {
+    // ---- epilogue: thread = output row m (TMEM lane)
+    int ch = 0;
+    for (int tk = blockIdx.x; tk < ntask; tk += gridDim.x) {
+    const STask t = tasks[tk];
+    const SProb P = probs[t.prob];
+    const int row0 = t.ti * SG_BM, col0 = t.tj * SG_BN;
+    const int m = row0 + threadIdx.x;
+    double acc[SG_BN];
+#pragma unroll
+    for (int j = 0; j < SG_BN; ++j) acc[j] = 0.0;
+    // the four epilogue warps run every segment (their named barriers must
+    // match); after a failed wait they skip the waits and reads
+    for (int sg = 0; sg < P.nseg; ++sg) {
+      const SSeg G = segs[P.seg0 + sg];
+      const SRole RA = roles[G.ra], RB = roles[G.rb];
+      const double alpha = G.c * (G.pa ? hv0 : 1.0) * (G.pb ? hv1 : 1.0);
+      const int em = m < P.M ? exbase[RA.ex_off + m] : 0;
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // fsc of the previous segment is no longer read
+      if (threadIdx.x < SG_BN)
+        fsc[threadIdx.x] = ldexp(1.0, (col0 + threadIdx.x < P.N) ? exbase[RB.ex_off + col0 + threadIdx.x] : 0);
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      const int ksteps = (G.K + SG_BK - 1) / SG_BK;
+      for (int c0 = 0; c0 < ksteps; c0 += kcs, ++ch) {
+        const int b = ch % NB;
+        if (fail) continue;
+        if (!mbar_wait(&accf[b], (ch / NB) & 1)) {
+          fail = 1;
+          continue;
+        }
+        tc_fence_after();
+        const unsigned dbase = tbase + ((unsigned)(warp * 32) << 16) + b * S * SG_BN;
+        for (int d = 0; d < S; ++d) {
+          const double rs = ldexp(alpha, em - 7 * (d + 2));
+#pragma unroll
+          for (int q = 0; q < SG_BN / 16; ++q) {
+            float v[16];
+            tmem_ld16(dbase + d * SG_BN + q * 16, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[q * 16 + j] = fma((double)v[j] * rs, fsc[q * 16 + j], acc[q * 16 + j]);
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acce[b]);
+      }
+    }
+    if (!fail && m < P.M) {
+      double* out = const_cast<double*>(outs.p[P.outbuf]) + P.offC + m;
+      const int nn = min(SG_BN, P.N - col0);
+#pragma unroll
+      for (int j = 0; j < SG_BN; ++j) {
+        if (j >= nn) break;
+        double* p = out + (i64)(col0 + j) * P.ldc;
+        if (P.mode == 0)
+          *p = acc[j];
+        else if (P.mode == 1)
+          *p += acc[j];
+        else
+          *p = acc[j] + (P.beta == 0.0 ? 0.0 : P.beta * *p);
+      }
+    }
     }
   }
   tc_fence_before();
   __syncthreads();
+  if (fail && threadIdx.x == 0) atomicExch(err, 1);
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(ncols) : "memory");
   }
 }
 
-size_t split_gemm_smem(int S) { return (size_t)S * (SG_ATILE + SG_BTILE) + 1024; }
+// pipeline shape for S slices: stages of S A tiles and S B tiles (24 KB per
+// slice) within 192 KB; two TMEM accumulator sets when they fit 512 columns
+int split_stages(int S) { return std::max(1, std::min(SG_MAXST, (192 * 1024) / (S * (int)(SG_ATILE + SG_BTILE)))); }
+int split_nbuf(int S) { return 2 * S * SG_BN <= 512 ? 2 : 1; }
+size_t split_gemm_smem(int S) { return (size_t)split_stages(S) * S * (SG_ATILE + SG_BTILE) + 1024; }
 
 // pair modes: C = (C +) V + sigma V^T from the product V (M x M scratch)
 struct SPair {
@@ -554,9 +639,25 @@ int run_plan(SplitState& ss, const SplitPlan& sp, int S, SPtrs bufs, double hv0,
   outs.p[SG_VBUF] = ss.V;
   if (sp.ntask > 0) {
     const size_t smem = split_gemm_smem(S);
-    QD_CUDA(cudaFuncSetAttribute(k_split_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_split_gemm<<<sp.ntask, SG_THREADS, smem, st>>>(sp.d_tasks, sp.d_probs, sp.d_segs, sp.d_roles, S, ss.sl, ss.ex,
-                                                     outs, hv0, hv1, ss.err);
+    int dev = 0, nsm = 148;
+    QD_CUDA(cudaGetDevice(&dev));
+    QD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = std::min(sp.ntask, nsm);  // one CTA per SM (the stages fill shared memory)
+    switch (S) {
+#define QD_SPLIT_LAUNCH(SS)                                                                                       \
+  case SS:                                                                                                        \
+    QD_CUDA(cudaFuncSetAttribute(k_split_gemm<SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));      \
+    k_split_gemm<SS><<<grid, SG_THREADS_P, smem, st>>>(sp.d_tasks, sp.ntask, sp.d_probs, sp.d_segs, sp.d_roles,  \
+                                                       split_stages(SS), split_nbuf(SS), ss.sl, ss.ex, outs, hv0, \
+                                                       hv1, ss.err);                                              \
+    break;
+      QD_SPLIT_LAUNCH(1) QD_SPLIT_LAUNCH(2) QD_SPLIT_LAUNCH(3) QD_SPLIT_LAUNCH(4)
+      QD_SPLIT_LAUNCH(5) QD_SPLIT_LAUNCH(6) QD_SPLIT_LAUNCH(7) QD_SPLIT_LAUNCH(8)
+#undef QD_SPLIT_LAUNCH
+      default:
+        set_error("split product: slices must be 1..8");
+        return QD_ERR_ARG;
+    }
   }
   if (sp.nptask > 0) k_split_pair<<<sp.nptask, 256, 0, st>>>(sp.d_ptasks, sp.d_pairs, ss.V, outs, hv0, hv1);
   QD_CUDA(cudaGetLastError());
