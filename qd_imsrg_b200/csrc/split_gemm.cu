@@ -103,34 +103,81 @@ __device__ __forceinline__ i64 tiled_off(int i, int k, int kpad) {
   return ((i64)(i >> 7) * (kpad >> 6) + (k >> 6)) * 8192 + r * 64 + ((((kk >> 3) ^ (r & 7)) << 3) | (kk & 7));
 }
 
-// one warp per (role, row i): max |x(i,k)| over k, then the slices of the row;
-// rows beyond R (padding) get zero slices
-__global__ void k_split_slice(const SRole* __restrict__ roles, const i64* __restrict__ rowstart, int nroles,
-                              SPtrs src, int S, __nv_bfloat16* __restrict__ slbase, int* __restrict__ exbase) {
-  const i64 w = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= rowstart[nroles]) return;
-  const int r = find_seg(rowstart, nroles, w);
+// One CTA (256 threads) per (role, block of 32 rows): the rows' maxima, then
+// per 64-wide K tile a coalesced load into shared memory (along the index that
+// is contiguous in the source) and the slices, 8 digits of a row per 16-byte
+// store.  Rows beyond R and K beyond the role's K get zero slices.
+constexpr int SL_ROWS = 32, SL_THREADS = 256;
+__global__ void __launch_bounds__(SL_THREADS) k_split_slice(const SRole* __restrict__ roles,
+                                                            const i64* __restrict__ blkstart, int nroles, SPtrs src,
+                                                            int S, __nv_bfloat16* __restrict__ slbase,
+                                                            int* __restrict__ exbase) {
+  __shared__ double T[SL_ROWS][65];
+  __shared__ double red[SL_THREADS / 32][SL_ROWS];
+  __shared__ int ex[SL_ROWS];
+  const int r = find_seg(blkstart, nroles, blockIdx.x);
   const SRole ro = roles[r];
-  const int i = (int)(w - rowstart[r]);
+  const int i0 = (int)(blockIdx.x - blkstart[r]) * SL_ROWS;
   const double* X = src.p[ro.src] + ro.off;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const bool rowc = ro.si == 1;  // consecutive rows are adjacent in memory
+  // maxima
   double mx = 0.0;
-  if (i < ro.R)
-    for (int k = lane; k < ro.K; k += 32) mx = fmax(mx, fabs(X[i * ro.si + k * ro.sk]));
-  for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  const int e = mx > 0.0 ? ilogb(mx) + 1 : 0;
-  if (lane == 0) exbase[ro.ex_off + i] = e;
+  if (rowc) {  // lane = row, warps stride over k
+    const int i = i0 + lane;
+    if (i < ro.R)
+      for (int k = w; k < ro.K; k += SL_THREADS / 32) mx = fmax(mx, fabs(X[i + (i64)k * ro.sk]));
+    red[w][lane] = mx;
+  } else {  // warp per row, lanes over k
+    for (int rr = w; rr < SL_ROWS; rr += SL_THREADS / 32) {
+      const int i = i0 + rr;
+      double m2 = 0.0;
+      if (i < ro.R)
+        for (int k = lane; k < ro.K; k += 32) m2 = fmax(m2, fabs(X[(i64)i * ro.si + (i64)k * ro.sk]));
+      for (int o = 16; o; o >>= 1) m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+      if (lane == 0) red[0][rr] = m2;
+    }
+  }
+  __syncthreads();
+  if (t < SL_ROWS) {
+    double m2 = red[0][t];
+    if (rowc)
+      for (int g = 1; g < SL_THREADS / 32; ++g) m2 = fmax(m2, red[g][t]);
+    const int e = m2 > 0.0 ? ilogb(m2) + 1 : 0;
+    ex[t] = e;
+    exbase[ro.ex_off + i0 + t] = e;
+  }
+  __syncthreads();
   __nv_bfloat16* out = slbase + (i64)S * ro.unit;
   const i64 sstride = (i64)ro.rpad * ro.kpad;
-  for (int k = lane; k < ro.kpad; k += 32) {
-    double x = (i < ro.R && k < ro.K) ? scalbn(X[i * ro.si + k * ro.sk], -e) : 0.0;
-    const i64 o = tiled_off(i, k, ro.kpad);
-    for (int sl = 0; sl < S; ++sl) {
-      const double t = x * 128.0;
-      const double d = rint(t);
-      x = t - d;
-      out[sl * sstride + o] = __float2bfloat16_rn((float)d);
+  for (int k0 = 0; k0 < ro.kpad; k0 += 64) {
+    // tile x(i0 + rr, k0 + c), rr < 32, c < 64
+    for (int e = t; e < SL_ROWS * 64; e += SL_THREADS) {
+      const int rr = rowc ? (e & 31) : (e >> 6), c = rowc ? (e >> 5) : (e & 63);
+      const int i = i0 + rr, k = k0 + c;
+      T[rr][c] = (i < ro.R && k < ro.K) ? X[(i64)i * ro.si + (i64)k * ro.sk] : 0.0;
     }
+    __syncthreads();
+    {  // thread = (row rr, 8-wide chunk cc)
+      const int rr = t >> 3, cc = t & 7;
+      const int e = ex[rr];
+      double x[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) x[q] = scalbn(T[rr][cc * 8 + q], -e);
+      const i64 o = tiled_off(i0 + rr, k0 + cc * 8, ro.kpad);  // 8 consecutive k share one 16-byte chunk
+      for (int sl = 0; sl < S; ++sl) {
+        __align__(16) __nv_bfloat16 d8[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const double tq = x[q] * 128.0;
+          const double dq = rint(tq);
+          x[q] = tq - dq;
+          d8[q] = __float2bfloat16_rn((float)dq);
+        }
+        *reinterpret_cast<uint4*>(out + sl * sstride + o) = *reinterpret_cast<const uint4*>(d8);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -588,8 +635,8 @@ int build_plan(const GemmProgram& G, unsigned mA, unsigned mB, SplitPlan& sp) {
     for (int i = 0; i < t; ++i)
       for (int j = 0; j < t; ++j) pt.push_back(SPairTask{(int)k, (short)i, (short)j});
   }
-  std::vector<i64> rowstart(sp.roles.size() + 1, 0);
-  for (size_t r = 0; r < sp.roles.size(); ++r) rowstart[r + 1] = rowstart[r] + sp.roles[r].rpad;
+  std::vector<i64> rowstart(sp.roles.size() + 1, 0);  // slicer blocks of SL_ROWS rows per role
+  for (size_t r = 0; r < sp.roles.size(); ++r) rowstart[r + 1] = rowstart[r] + sp.roles[r].rpad / SL_ROWS;
   sp.rows = rowstart.back();
   int rc;
   if ((rc = upload(sp.roles, &sp.d_roles)) || (rc = upload(rowstart, &sp.d_rowstart)) ||
@@ -630,11 +677,9 @@ int run_plan(SplitState& ss, const SplitPlan& sp, int S, SPtrs bufs, double hv0,
     QD_CUDA(cudaMalloc((void**)&ss.err, sizeof(int)));
     QD_CUDA(cudaMemsetAsync(ss.err, 0, sizeof(int), st));
   }
-  if (sp.rows > 0) {
-    const i64 threads = sp.rows * 32;
-    k_split_slice<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(sp.d_roles, sp.d_rowstart,
-                                                                    (int)sp.roles.size(), bufs, S, ss.sl, ss.ex);
-  }
+  if (sp.rows > 0)
+    k_split_slice<<<(unsigned)sp.rows, SL_THREADS, 0, st>>>(sp.d_roles, sp.d_rowstart, (int)sp.roles.size(), bufs,
+                                                            S, ss.sl, ss.ex);
   SPtrs outs = bufs;
   outs.p[SG_VBUF] = ss.V;
   if (sp.ntask > 0) {
