@@ -307,6 +307,21 @@ int qd_mlp_grad(qd_mlp* mlp, const float* d_X, const float* d_T, int64_t n, floa
 int qd_mlp_train_step(qd_mlp* mlp, const float* d_X, const float* d_T, int64_t n, float lr, float* loss,
                       void* stream);
 
+/* ---- on-disk Hamiltonian: export_hamiltonian / import_hamiltonian --------
+ * Replaces src/ME_general.f90:207-361.  The reference's Fortran unformatted
+ * sequential file: one record per FP64 entry framed by 4-byte markers (8),
+ * in its loop order (E0, fhh, fph, fpp row by row, then per block Vhhhh,
+ * Vpppp, Vpphh, Vphph, Vphhh, Vppph row by row); no header.  The reference
+ * prefixes '../hamiltonians/' to the name; `path` here is the full path.
+ * qd_hamiltonian_write/read convert a host array in vectorize order (they
+ * work on QD_HOST_ONLY layouts); qd_export/import_hamiltonian move a device
+ * operator (download + write, read + upload).  A file whose size or record
+ * markers do not match the layout is rejected with QD_ERR_ARG.             */
+int qd_hamiltonian_write(const qd_layout* L, const double* vec, const char* path);
+int qd_hamiltonian_read(const qd_layout* L, double* vec, const char* path);
+int qd_export_hamiltonian(const qd_op* H, const char* path);
+int qd_import_hamiltonian(qd_op* H, const char* path);
+
 /* Split-precision FP64 product with dgemm's argument meaning (column-major;
  * transa/transb 'N' or 'T'): C = alpha op(A) op(B) + beta C on device arrays,
  * on the tcgen05 tensor cores.  Replaces the dgemm calls of matrix_mult222

@@ -20,6 +20,7 @@ layout; host arrays are exchanged in the reference's vectorize order.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -449,6 +450,31 @@ def v_int(qi, qj, qk, ql, hw: float = 1.0, quad: bool = False) -> float:
     arrs = [(C.c_int * 3)(*[int(x) for x in q]) for q in (qi, qj, qk, ql)]
     fn = lib().qd_v_int_quad if quad else lib().qd_v_int
     return float(fn(*arrs, float(hw)))
+
+
+def hamiltonian_write(layout: Layout, vec: np.ndarray, path: str) -> None:
+    """Write a vectorize-order operator in the reference's export_hamiltonian
+    file format (ME_general.f90:207-282)."""
+    v = np.ascontiguousarray(vec, np.float64)
+    if v.size != layout.neq:
+        raise ValueError("hamiltonian_write: %d entries given, layout has %d" % (v.size, layout.neq))
+    check(lib().qd_hamiltonian_write(layout.h, v.ctypes.data_as(_dp), os.fsencode(path)))
+
+
+def hamiltonian_read(layout: Layout, path: str) -> np.ndarray:
+    """Read a file of the reference's import_hamiltonian format
+    (ME_general.f90:284-361) into a vectorize-order array."""
+    v = np.empty(layout.neq, np.float64)
+    check(lib().qd_hamiltonian_read(layout.h, v.ctypes.data_as(_dp), os.fsencode(path)))
+    return v
+
+
+def export_hamiltonian(H: "FullHam", path: str) -> None:
+    check(lib().qd_export_hamiltonian(H.h, os.fsencode(path)))
+
+
+def import_hamiltonian(H: "FullHam", path: str) -> None:
+    check(lib().qd_import_hamiltonian(H.h, os.fsencode(path)))
 
 
 def gemm_split(A, B, C=None, alpha: float = 1.0, beta: float = 0.0, trans_a: bool = False, trans_b: bool = False,
