@@ -176,6 +176,14 @@ int qd_commutator_222(const qd_op* r1, const qd_op* r2, qd_op* r3, qd_op* w1, co
  * makes the initial eta norm ~1e-16, so run_magnus rejects every step.      */
 #define QD_FULL_NORM 2u
 int qd_commutator(const qd_op* A, const qd_op* B, qd_op* C, unsigned flags);
+/* dGam, src/gs_IMSRG.f90:223-273: the derivative of the ODE form of the flow,
+ * the right-hand side the host's Adams integrator (adams_ode) evaluates.
+ * ETA = build_white(H) on a zeroed generator (herm -1), HCC = calc_cc(H),
+ * ETACC = calc_cc(ETA), DER = [ETA, H] with all terms including the
+ * particle-hole channel.  HCC / ETACC are filled as in the reference (NULL:
+ * library workspaces).  The reference's vectorize(DER, yp) is
+ * qd_op_download(DER, yp, neq); its repackage(H, y) is qd_op_upload.        */
+int qd_dgam(const qd_op* H, qd_op* DER, qd_cc* HCC, qd_cc* ETACC);
 
 /* ---- cross-coupled (Pandya) matrices ----------------------------------------
  * calc_cc src/commutators.f90:1135-1159, copy_cc src/IMSRG_tools.f90:437-461 */

@@ -261,6 +261,12 @@ def commutator(A: FullHam, B: FullHam, Cop: FullHam, pandya: bool = True) -> Non
     check(lib().qd_commutator(A.h, B.h, Cop.h, QD_PANDYA if pandya else 0))
 
 
+def dgam(H: FullHam, DER: FullHam, HCC: CCMat | None = None, ETACC: CCMat | None = None) -> None:
+    """dGam (gs_IMSRG.f90:223-273): DER = [build_white(H), H] with every term,
+    the ODE flow's derivative; fills HCC = calc_cc(H), ETACC = calc_cc(eta)."""
+    check(lib().qd_dgam(H.h, DER.h, HCC.h if HCC is not None else None, ETACC.h if ETACC is not None else None))
+
+
 def calc_cc(H: FullHam, HCC: CCMat) -> None:
     check(lib().qd_calc_cc(H.h, HCC.h))
 

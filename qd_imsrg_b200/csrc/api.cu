@@ -32,6 +32,7 @@ struct Workspace {
   // OCC, allocated by the first flow on the layout and kept
   qd_op* flow[11] = {nullptr};
   qd_cc* flow_cc[2] = {nullptr};
+  qd_op* eta = nullptr;  // dGam's generator
 };
 std::map<const qd_layout*, Workspace>& workspaces() {
   static std::map<const qd_layout*, Workspace> m;
@@ -304,6 +305,7 @@ void drop_ws(const qd_layout* L) {
   cc_free(w.cb);
   for (qd_op* o : w.flow) op_free(o);
   for (qd_cc* c : w.flow_cc) cc_free(c);
+  op_free(w.eta);
 }
 
 const double kCof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666, 0.0083333333333333333,
@@ -684,6 +686,28 @@ int qd_commutator(const qd_op* A, const qd_op* B, qd_op* C, unsigned flags) {
   Workspace* w;
   TRY(get_ws(L, &w));
   return commutator_seq(L, A, B, C, w->w1, w->w2, w->ca, w->cb, (flags & QD_PANDYA) != 0);
+}
+
+// dGam (src/gs_IMSRG.f90:223-273): ETA = build_white(H) on a zeroed
+// operator, HCC = calc_cc(H) (herm +1), ETACC = calc_cc(ETA) (herm -1),
+// DER = [ETA, H] with every term: 110+220 into E0, 111, 121, 221, 122, 222
+// with the particle-hole channel (the reference's order).
+int qd_dgam(const qd_op* H, qd_op* DER, qd_cc* HCC, qd_cc* ETACC) {
+  TRY(same_layout(H, DER));
+  CHECK(H != DER, QD_ERR_ARG, "qd_dgam: DER aliases H");
+  qd_layout* L = H->L;
+  CHECK((!HCC || HCC->L == L) && (!ETACC || ETACC->L == L), QD_ERR_ARG, "qd_dgam: cross-coupled matrix of another layout");
+  TRY(use_device(L));
+  Workspace* w;
+  TRY(get_ws(L, &w));
+  if (!w->eta) TRY(op_new(L, -1, &w->eta));
+  qd_op* eta = w->eta;
+  eta->herm = -1;
+  QD_CUDA(cudaMemsetAsync(eta->d, 0, sizeof(double) * L->neq, L->stream));
+  eta->zero_mask = ALL_PARTS;
+  TRY(qd_build_white(eta, H));
+  TRY(commutator_seq(L, eta, H, DER, w->w1, w->w2, ETACC ? ETACC : w->ca, HCC ? HCC : w->cb, true));
+  return QD_OK;
 }
 
 int qd_cc_create(qd_layout* L, double herm, qd_cc** out) {
