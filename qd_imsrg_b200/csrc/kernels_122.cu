@@ -46,6 +46,13 @@ constexpr int GMAX122 = 16;                        // largest (m_l,m_s) group (f
 constexpr size_t SMEM_MAX_ATTR_122 = 227 * 1024;   // opt-in shared memory per CTA on sm_100
 constexpr size_t SMEM_TARGET_122 = 74 * 1024;      // per-CTA staging goal: three CTAs per SM
 constexpr size_t SMEM_STATIC_122 = 1024;           // bound on the pass kernels' static shared memory
+// Per-pass TJ rule (measured on the N=20 R=20 flow, 122 ms per flow): both
+// passes at TJ >= 2 within 74 KB, 592; the ket pass at TJ >= 4 within 112 or
+// 150 KB (whole 32-byte sectors, fewer CTAs), 812-820; TJ = 1 on the largest
+// blocks of either pass, 637-808.  Parallelism beats sector efficiency here.
+constexpr size_t KET_SMEM_TARGET_122 = 74 * 1024;   // ket pass: three CTAs per SM
+constexpr int KET_MIN_TJ_122 = 2;
+constexpr int BRA_MIN_TJ_122 = 2;
 
 struct Task122 {
   int q;
@@ -311,7 +318,7 @@ namespace {
 // Tasks are grouped in buckets by TJ; each bucket is one launch per pass
 // whose dynamic shared memory fits its largest block.
 struct Bucket122 {
-  int tj;       // 2, 4, 8 or 16
+  int tj;       // 1, 2, 4, 8 or 16
   int first;    // range in the task array
   int count;
   size_t smem;
@@ -324,7 +331,7 @@ struct Plan122 {
   int* d_sbase = nullptr;
   double2* d_ftab = nullptr;
   int ntask = 0, gmax = 0, nfent = 0;
-  std::vector<Bucket122> buckets;
+  std::vector<Bucket122> buckets[2];  // bra pass, ket pass
 };
 std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
@@ -343,10 +350,11 @@ size_t smem_122(int cells, int npair, int tj) {
 // built concurrently for other layouts can never lower it below a need
 template <int GM>
 static int set_attr_122() {
-  const void* fns[8] = {(const void*)k_122_pass<16, 0, GM>, (const void*)k_122_pass<16, 1, GM>,
-                        (const void*)k_122_pass<8, 0, GM>,  (const void*)k_122_pass<8, 1, GM>,
-                        (const void*)k_122_pass<4, 0, GM>,  (const void*)k_122_pass<4, 1, GM>,
-                        (const void*)k_122_pass<2, 0, GM>,  (const void*)k_122_pass<2, 1, GM>};
+  const void* fns[10] = {(const void*)k_122_pass<16, 0, GM>, (const void*)k_122_pass<16, 1, GM>,
+                         (const void*)k_122_pass<8, 0, GM>,  (const void*)k_122_pass<8, 1, GM>,
+                         (const void*)k_122_pass<4, 0, GM>,  (const void*)k_122_pass<4, 1, GM>,
+                         (const void*)k_122_pass<2, 0, GM>,  (const void*)k_122_pass<2, 1, GM>,
+                         (const void*)k_122_pass<1, 0, GM>,  (const void*)k_122_pass<1, 1, GM>};
   for (const void* fn : fns) {
     cudaFuncAttributes fa;
     QD_CUDA(cudaFuncGetAttributes(&fa, fn));  // static + dynamic shared memory <= the limit
@@ -359,7 +367,7 @@ static int set_attr_122() {
 template <int GM, int KET>
 static void pass_122(const Plan122* p, qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   const double2* ft = p->d_ftab + (KET ? p->nfent : 0);
-  for (const Bucket122& b : p->buckets) {
+  for (const Bucket122& b : p->buckets[KET]) {
 #define QD_122_LAUNCH(TJ)                                                                                          \
   k_122_pass<TJ, KET, GM><<<b.count, T122, b.smem, L->stream>>>(L->dev, p->d_task + b.first, p->d_meta, p->d_sub, \
                                                                 p->d_cell, ft, A->d, (double)A->herm,             \
@@ -369,7 +377,8 @@ static void pass_122(const Plan122* p, qd_layout* L, const qd_op* A, const qd_op
       case 16: QD_122_LAUNCH(16); break;
       case 8: QD_122_LAUNCH(8); break;
       case 4: QD_122_LAUNCH(4); break;
-      default: QD_122_LAUNCH(2); break;
+      case 2: QD_122_LAUNCH(2); break;
+      default: QD_122_LAUNCH(1); break;
     }
 #undef QD_122_LAUNCH
     ++L->nlaunch;
@@ -451,42 +460,49 @@ static int plan_122(qd_layout* L, Plan122** out) {
     sub.insert(sub.end(), sv.begin(), sv.end());
   }
 
-  // tasks: TJ = the largest power of two (2..16) whose staging fits the
-  // per-CTA goal; larger blocks first within a bucket
-  const int tjs[4] = {16, 8, 4, 2};
+  // tasks per pass: TJ = the largest power of two (min_tj..16) whose staging
+  // fits the pass's per-CTA goal; larger blocks first within a bucket.  The
+  // ket pass stages rows of column-major parts in TJ-long runs, so its TJ
+  // starts at KET_MIN_TJ_122 (whole 32-byte sectors).
   std::vector<Task122> ht;
-  for (int bkt = 0; bkt < 4; ++bkt) {
-    const int tj = tjs[bkt];
-    std::vector<std::pair<int, Task122>> v;
-    int cmax = 0;
-    for (int q = 0; q < L->nblock; ++q) {
-      const int nc = meta[q].x;
-      if (L->blk[q].w == 0) continue;
-      int want = 2;
-      for (int t : tjs)
-        if (smem_122(nc, L->blk[q].w, t) <= SMEM_TARGET_122) {
-          want = t;
-          break;
+  for (int pass = 0; pass < 2; ++pass) {
+    const size_t target = pass ? KET_SMEM_TARGET_122 : SMEM_TARGET_122;
+    const int min_tj = pass ? KET_MIN_TJ_122 : BRA_MIN_TJ_122;
+    const int tjs[5] = {16, 8, 4, 2, 1};
+    for (int bkt = 0; bkt < 5; ++bkt) {
+      const int tj = tjs[bkt];
+      if (tj < min_tj) continue;
+      std::vector<std::pair<int, Task122>> v;
+      int cmax = 0;
+      for (int q = 0; q < L->nblock; ++q) {
+        const int nc = meta[q].x;
+        if (L->blk[q].w == 0) continue;
+        int want = min_tj;
+        for (int t : tjs)
+          if (t >= min_tj && smem_122(nc, L->blk[q].w, t) <= target) {
+            want = t;
+            break;
+          }
+        if (want != tj) continue;
+        if (smem_122(nc, L->blk[q].w, tj) > SMEM_MAX_ATTR_122 - SMEM_STATIC_122) {
+          set_error("commutator_122: block of %d cells exceeds shared memory", nc);
+          return QD_ERR_ARG;
         }
-      if (want != tj) continue;
-      if (smem_122(nc, L->blk[q].w, tj) > SMEM_MAX_ATTR_122 - SMEM_STATIC_122) {
-        set_error("commutator_122: block of %d cells exceeds shared memory", nc);
-        return QD_ERR_ARG;
+        cmax = std::max(cmax, (int)smem_122(nc, L->blk[q].w, tj));
+        const int cnt[3] = {L->blk[q].x, L->blk[q].y, L->blk[q].z};
+        for (int c = 0; c < 3; ++c)
+          for (int f = 0; f < cnt[c]; f += tj) v.push_back({nc, Task122{q, (short)c, 0, f}});
       }
-      cmax = std::max(cmax, (int)smem_122(nc, L->blk[q].w, tj));
-      const int cnt[3] = {L->blk[q].x, L->blk[q].y, L->blk[q].z};
-      for (int c = 0; c < 3; ++c)
-        for (int f = 0; f < cnt[c]; f += tj) v.push_back({nc, Task122{q, (short)c, 0, f}});
+      if (v.empty()) continue;
+      std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+      Bucket122 bk;
+      bk.tj = tj;
+      bk.first = (int)ht.size();
+      bk.count = (int)v.size();
+      bk.smem = (size_t)cmax;
+      for (auto& x : v) ht.push_back(x.second);
+      p.buckets[pass].push_back(bk);
     }
-    if (v.empty()) continue;
-    std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-    Bucket122 bk;
-    bk.tj = tj;
-    bk.first = (int)ht.size();
-    bk.count = (int)v.size();
-    bk.smem = (size_t)cmax;
-    for (auto& x : v) ht.push_back(x.second);
-    p.buckets.push_back(bk);
   }
   p.ntask = (int)ht.size();
   auto up = [&](auto& vec, auto** dptr) -> int {
@@ -502,7 +518,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
     return rc;
   QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)std::max(1, p.nfent)));
   L->ws_bytes += (i64)sizeof(double2) * 2 * p.nfent;
-  if (!p.buckets.empty()) {
+  if (!p.buckets[0].empty() || !p.buckets[1].empty()) {
     int rc2 = p.gmax <= 10 ? set_attr_122<10>() : set_attr_122<16>();
     if (rc2) return rc2;
   }
