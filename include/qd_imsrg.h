@@ -82,6 +82,13 @@ int qd_layout_set_stream(qd_layout* L, void* stream);
  * (one-body, 122, 121, 221 traces, Pandya gathers, E0, norms, BCH sums, HF)
  * stays FP64.  No reference counterpart (the reference is FP64 only).       */
 int qd_layout_set_split(qd_layout* L, int slices);
+/* BCH terms (qd_bch_expand, and the flows built on it) as CUDA graphs: a
+ * term seen before with the same buffers, zero-part masks, herm, flags and
+ * coefficient is captured once and replayed with one launch (default on;
+ * the stage profiler bypasses it).  Results are identical either way.
+ * qd_layout_graph_stats: graphs captured and replays so far.               */
+int qd_layout_set_graphs(qd_layout* L, int enable);
+int qd_layout_graph_stats(const qd_layout* L, int64_t* captured, int64_t* replays);
 int qd_layout_get_split(const qd_layout* L, int* slices);
 int qd_layout_synchronize(qd_layout* L);
 /* device bytes currently held by the layout's work arena                    */

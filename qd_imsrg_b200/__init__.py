@@ -96,6 +96,16 @@ class Layout:
     def split(self, slices: int) -> None:
         check(lib().qd_layout_set_split(self.h, int(slices)))
 
+    def set_graphs(self, enable: bool) -> None:
+        """Replay BCH terms as CUDA graphs (default on)."""
+        check(lib().qd_layout_set_graphs(self.h, int(enable)))
+
+    def graph_stats(self) -> tuple[int, int]:
+        """(graphs captured, replays) of this layout so far."""
+        a, b = C.c_int64(), C.c_int64()
+        check(lib().qd_layout_graph_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def profile(self, enable: bool = True) -> None:
         """Start (and reset) or stop per-stage CUDA-event timing."""
         check(lib().qd_layout_profile(self.h, int(enable)))

@@ -61,6 +61,8 @@ SIGNATURES = {
     "qd_layout_pairs": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _ip]),
     "qd_layout_set_stream": (C.c_int, [_vp, _vp]),
     "qd_layout_set_split": (C.c_int, [_vp, C.c_int]),
+    "qd_layout_set_graphs": (C.c_int, [_vp, C.c_int]),
+    "qd_layout_graph_stats": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "qd_layout_get_split": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "qd_layout_synchronize": (C.c_int, [_vp]),
     "qd_layout_workspace_bytes": (C.c_int, [_vp, _lp]),

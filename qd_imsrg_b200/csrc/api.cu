@@ -453,6 +453,24 @@ int qd_layout_set_split(qd_layout* L, int slices) {
   return QD_OK;
 }
 
+int qd_layout_set_graphs(qd_layout* L, int enable) {
+  CHECK(L, QD_ERR_ARG, "null layout");
+  if (!enable && L->graphs) {
+    TRY(use_device(L));
+    QD_CUDA(cudaStreamSynchronize(L->stream));
+    graphs_free(L);
+  }
+  L->use_graphs = enable != 0;
+  return QD_OK;
+}
+
+int qd_layout_graph_stats(const qd_layout* L, int64_t* captured, int64_t* replays) {
+  CHECK(L, QD_ERR_ARG, "null layout");
+  if (captured) *captured = L->graphs_captured;
+  if (replays) *replays = L->graph_replays;
+  return QD_OK;
+}
+
 int qd_layout_get_split(const qd_layout* L, int* slices) {
   CHECK(L && slices, QD_ERR_ARG, "null argument");
   *slices = L->split_slices;
@@ -778,6 +796,108 @@ int qd_hf_e2(qd_op* H, double* out) {
   return QD_OK;
 }
 
+// ---- one BCH term, replayed as a CUDA graph --------------------------------
+// A term is INT2 = [G, AD], HS += cof INT2 with |HS| and |INT2| into
+// red_slot(1) and their copy to h_red[1..2].  Its launches depend only on the
+// buffers, the zero-part masks, herm, the flags, the slice count and cof, so
+// a term seen before on the same key is captured once (thread-local capture
+// mode, after an eager run has built every plan and workspace) and replayed
+// with one cudaGraphLaunch.  A capture that fails leaves the key eager.
+namespace {
+struct TermKey {
+  const void* p[8];  // G, AD, INT2, HS, w1, w2, OCC, HCC data
+  unsigned mg, mad, mhs;
+  int gh, term, flags, split;
+  bool operator<(const TermKey& o) const { return std::memcmp(this, &o, sizeof(TermKey)) < 0; }
+};
+struct TermGraph {
+  int seen = 0;
+  bool failed = false;
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;
+};
+using TermGraphs = std::map<TermKey, TermGraph>;
+
+int bch_term(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd_op* w1, qd_op* w2, qd_cc* HCC,
+             qd_cc* OCC, bool pandya, bool full, double cof) {
+  if (pandya) {
+    TRY(commutator_seq(L, G, AD, INT2, w1, w2, OCC, HCC, true));
+  } else {
+    TRY(commutator_seq(L, G, AD, INT2, w1, w2, nullptr, nullptr, false));
+  }
+  {
+    StageTimer tm(L, S_GLUE);
+    TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, full ? 1 : 0, red_slot(L, 1)));
+  }
+  QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+  return QD_OK;
+}
+}  // namespace
+
+static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd_op* w1, qd_op* w2,
+                          qd_cc* HCC, qd_cc* OCC, bool pandya, bool full, int term, double cof) {
+  if (!L->use_graphs || L->prof.on) return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+  if (!L->graphs) L->graphs = new TermGraphs();
+  TermKey k;
+  std::memset(&k, 0, sizeof(k));
+  k.p[0] = G->d;
+  k.p[1] = AD->d;
+  k.p[2] = INT2->d;
+  k.p[3] = HS->d;
+  k.p[4] = w1->d;
+  k.p[5] = w2->d;
+  k.p[6] = OCC ? OCC->d : nullptr;
+  k.p[7] = HCC ? HCC->d : nullptr;
+  k.mg = G->zero_mask;
+  k.mad = AD->zero_mask;
+  k.mhs = HS->zero_mask;
+  k.gh = G->herm;
+  k.term = term;
+  k.flags = (pandya ? 1 : 0) | (full ? 2 : 0);
+  k.split = L->split_slices;
+  TermGraph& tg = (*reinterpret_cast<TermGraphs*>(L->graphs))[k];
+  if (tg.exec) {
+    QD_CUDA(cudaGraphLaunch(tg.exec, L->stream));
+    L->nlaunch += tg.launches;
+    ++L->graph_replays;
+    INT2->zero_mask = 0;  // what the captured commutator_seq leaves on the host side
+    if (pandya) {
+      OCC->filled = true;
+      OCC->herm = G->herm;
+      HCC->filled = true;
+      HCC->herm = AD->herm;
+    }
+    return QD_OK;
+  }
+  if (tg.failed || tg.seen == 0) {
+    ++tg.seen;
+    return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+  }
+  // second sight: capture, instantiate, launch
+  const long long n0 = L->nlaunch;
+  cudaGraph_t graph = nullptr;
+  int rc = QD_OK;
+  cudaError_t e = cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+    e = cudaStreamEndCapture(L->stream, &graph);
+  }
+  if (e == cudaSuccess && rc == QD_OK && graph) e = cudaGraphInstantiate(&tg.exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess || rc != QD_OK || !tg.exec) {
+    (void)cudaGetLastError();
+    if (tg.exec) cudaGraphExecDestroy(tg.exec);
+    tg.exec = nullptr;
+    tg.failed = true;
+    L->nlaunch = n0;
+    return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+  }
+  tg.launches = L->nlaunch - n0;
+  ++L->graphs_captured;
+  QD_CUDA(cudaGraphLaunch(tg.exec, L->stream));
+  return QD_OK;
+}
+
 int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op* INT2, qd_op* AD, qd_op* w1,
                   qd_op* w2, qd_cc* HCC, qd_cc* OCC, unsigned flags, int* nterms) {
   TRY(same_layout(HS, G));
@@ -801,19 +921,10 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   for (int i = 2; i <= 12; ++i) {
     std::swap(INT2->d, AD->d);  // AD = previous term; INT2 becomes the output buffer
     std::swap(INT2->zero_mask, AD->zero_mask);
-    if (pandya) {
-      TRY(commutator_seq(L, G, AD, INT2, w1, w2, OCC, HCC, true));
-    } else {
-      TRY(commutator_seq(L, G, AD, INT2, w1, w2, nullptr, nullptr, false));
-    }
-    ++count;
     const double cof = kCof[i - 2];
-    {  // HS += cof * INT2 with |INT1| = |HS| before the update and |INT2| in the same pass
-      StageTimer tm(L, S_GLUE);
-      TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, (flags & QD_FULL_NORM) ? 1 : 0, red_slot(L, 1)));
-    }
+    TRY(bch_term_graph(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, (flags & QD_FULL_NORM) != 0, i, cof));
+    ++count;
     HS->zero_mask &= INT2->zero_mask;
-    QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     QD_CUDA(cudaStreamSynchronize(L->stream));
     const double n1 = L->h_red[1], n2 = L->h_red[2];
     if (n2 * cof / n1 < conv) break;
@@ -1085,3 +1196,14 @@ int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, u
 }
 
 }  // extern "C"
+
+namespace qd {
+void graphs_free(qd_layout* L) {
+  auto* m = reinterpret_cast<TermGraphs*>(L->graphs);
+  if (!m) return;
+  for (auto& kv : *m)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  delete m;
+  L->graphs = nullptr;
+}
+}  // namespace qd

@@ -299,6 +299,7 @@ void layout_free_device(qd_layout* L) {
   L->prog_111.clear_device();
   L->prog_pandya.clear_device();
   split_free(L);
+  graphs_free(L);
   if (L->d_z) cudaFree(L->d_z);
   if (L->d_red) cudaFree(L->d_red);
   if (L->d_axn) cudaFree(L->d_axn);

@@ -159,6 +159,10 @@ struct qd_layout {
   // split form of the GEMM programs: slices per operand (0 = plain FP64)
   int split_slices = 0;
   void* split = nullptr;  // plans and workspaces (split_gemm.cu)
+  // BCH terms replayed as CUDA graphs (api.cu)
+  bool use_graphs = true;
+  void* graphs = nullptr;
+  long long graphs_captured = 0, graph_replays = 0;
 };
 
 struct qd_op {
@@ -221,5 +225,6 @@ void fill_random(const qd_layout* L, int herm, uint64_t seed, double sigma, int 
 int run_program_split(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
                       unsigned maskB);
 void split_free(qd_layout* L);
+void graphs_free(qd_layout* L);
 
 }  // namespace qd
