@@ -191,6 +191,16 @@ int qd_commutator(const qd_op* A, const qd_op* B, qd_op* C, unsigned flags);
  * library workspaces).  The reference's vectorize(DER, yp) is
  * qd_op_download(DER, yp, neq); its repackage(H, y) is qd_op_upload.        */
 int qd_dgam(const qd_op* H, qd_op* DER, qd_cc* HCC, qd_cc* ETACC);
+/* EOM matrix-vector product for the scalar target (M_L, M_S) = (0, 0):
+ * matvec_prod (src/EOM_IMSRG.f90:551-649) with HQ_comm_1b / HQ_comm_2b
+ * (src/commutators.f90:1162-1272).  Q's fph and Vpphh hold the 1p1h and 2p2h
+ * amplitudes (its other parts are ignored); HQ receives fph = HQ_comm_1b and
+ * Vpphh = HQ_comm_2b, every other part zero.  Computed as the particle-hole
+ * and pphh parts of ([H, Q+] + [H, Q-]) / 2 with Q+- the amplitudes as
+ * herm +-1 operators (particle-hole channel on).  The Lanczos driver
+ * (ARPACK dsaupd) stays on the host, as in the reference; its vector maps to
+ * Q through the host's unwrap/rewrap.  Non-scalar targets are not covered. */
+int qd_eom_matvec(const qd_op* H, const qd_op* Q, qd_op* HQ);
 
 /* ---- cross-coupled (Pandya) matrices ----------------------------------------
  * calc_cc src/commutators.f90:1135-1159, copy_cc src/IMSRG_tools.f90:437-461 */

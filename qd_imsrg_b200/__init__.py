@@ -277,6 +277,13 @@ def dgam(H: FullHam, DER: FullHam, HCC: CCMat | None = None, ETACC: CCMat | None
     check(lib().qd_dgam(H.h, DER.h, HCC.h if HCC is not None else None, ETACC.h if ETACC is not None else None))
 
 
+def eom_matvec(H: FullHam, Q: FullHam, HQ: FullHam) -> None:
+    """EOM matrix-vector product (matvec_prod / HQ_comm_1b,2b) for the
+    scalar target: HQ's fph and Vpphh = the ph and pphh parts of [H, Q] for
+    the excitation amplitudes in Q's fph and Vpphh; other parts zero."""
+    check(lib().qd_eom_matvec(H.h, Q.h, HQ.h))
+
+
 def calc_cc(H: FullHam, HCC: CCMat) -> None:
     check(lib().qd_calc_cc(H.h, HCC.h))
 

@@ -33,6 +33,8 @@ struct Workspace {
   qd_op* flow[11] = {nullptr};
   qd_cc* flow_cc[2] = {nullptr};
   qd_op* eta = nullptr;  // dGam's generator
+  qd_op* eomq = nullptr;  // EOM matvec: excitation operator, second commutator
+  qd_op* eomt = nullptr;
 };
 std::map<const qd_layout*, Workspace>& workspaces() {
   static std::map<const qd_layout*, Workspace> m;
@@ -306,6 +308,8 @@ void drop_ws(const qd_layout* L) {
   for (qd_op* o : w.flow) op_free(o);
   for (qd_cc* c : w.flow_cc) cc_free(c);
   op_free(w.eta);
+  op_free(w.eomq);
+  op_free(w.eomt);
 }
 
 const double kCof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666, 0.0083333333333333333,
@@ -725,6 +729,39 @@ int qd_dgam(const qd_op* H, qd_op* DER, qd_cc* HCC, qd_cc* ETACC) {
   eta->zero_mask = ALL_PARTS;
   TRY(qd_build_white(eta, H));
   TRY(commutator_seq(L, eta, H, DER, w->w1, w->w2, ETACC ? ETACC : w->ca, HCC ? HCC : w->cb, true));
+  return QD_OK;
+}
+
+// EOM matrix-vector product (matvec_prod, src/EOM_IMSRG.f90:551-649, with
+// HQ_comm_1b/2b, src/commutators.f90:1162-1272) for the scalar target
+// (M_L, M_S) = (0, 0): the particle-hole and pphh parts of [H, Q] for the
+// excitation operator Q (its fph and Vpphh).  The layout stores each
+// operator with herm = +-1, so Q = (Q+ + Q-)/2, Q+- the same amplitudes as
+// herm +-1 operators, and [H, Q] is the average of two full commutators with
+// the particle-hole channel; every other part of HQ is zero.
+int qd_eom_matvec(const qd_op* H, const qd_op* Q, qd_op* HQ) {
+  TRY(same_layout(H, Q));
+  TRY(same_layout(H, HQ));
+  CHECK(HQ != H && HQ != Q, QD_ERR_ARG, "qd_eom_matvec: HQ aliases an input");
+  qd_layout* L = H->L;
+  TRY(use_device(L));
+  Workspace* w;
+  TRY(get_ws(L, &w));
+  if (!w->eomq) TRY(op_new(L, 1, &w->eomq));
+  if (!w->eomt) TRY(op_new(L, 1, &w->eomt));
+  const unsigned exc = (1u << P_FPH) | (1u << P_PPHH);
+  qd_op* X = w->eomq;
+  QD_CUDA(cudaMemcpyAsync(X->d, Q->d, sizeof(double) * L->neq, cudaMemcpyDeviceToDevice, L->stream));
+  TRY(launch_keep_parts(L, X->d, exc));
+  X->zero_mask = (ALL_PARTS & ~exc) | (Q->zero_mask & exc);
+  X->herm = 1;
+  TRY(commutator_seq(L, H, X, HQ, w->w1, w->w2, w->cb, w->ca, true));
+  X->herm = -1;
+  TRY(commutator_seq(L, H, X, w->eomt, w->w1, w->w2, w->cb, w->ca, true));
+  TRY(launch_axpy(L, HQ->d, 0.5, w->eomt->d, 0.5, HQ->d, L->neq));
+  TRY(launch_keep_parts(L, HQ->d, exc));
+  HQ->herm = 1;
+  HQ->zero_mask = ALL_PARTS & ~exc;
   return QD_OK;
 }
 

@@ -28,6 +28,32 @@ __global__ void k_axpy2(const double2* __restrict__ a, double sa, const double2*
   }
 }
 
+// zero every entry of op outside the parts in `keep` (bit P_* per part, bit
+// P_COUNT for E0)
+__global__ void k_keep_parts(DevLayout L, double* __restrict__ op, unsigned keep) {
+  const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= L.neq) return;
+  int part;
+  if (e < L.o_fhh)
+    part = P_COUNT;
+  else if (e < L.o_fpp)
+    part = P_FHH;
+  else if (e < L.o_fph)
+    part = P_FPP;
+  else if (e < L.o2)
+    part = P_FPH;
+  else
+    part = P_HHHH + (__ldg(L.s2id + find_seg(L.s2off, L.ns2, e)) & 7);
+  if (!((keep >> part) & 1u)) op[e] = 0.0;
+}
+
+int launch_keep_parts(qd_layout* L, double* op, unsigned keep) {
+  if (L->neq > 0) k_keep_parts<<<(unsigned)((L->neq + 255) / 256), 256, 0, L->stream>>>(L->dev, op, keep);
+  ++L->nlaunch;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
 int launch_axpy(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, i64 n) {
   const int threads = 256, blocks = 148 * 8;
   if ((((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15) == 0) {

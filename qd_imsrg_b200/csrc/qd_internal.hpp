@@ -213,6 +213,7 @@ int reduce_norm1b(qd_layout* L, const double* a, double* dout);
 int reduce_norm_full(qd_layout* L, const double* a, double* dout);
 double* red_slot(qd_layout* L, int k);
 int launch_white(qd_layout* L, double* gen, const double* h, int herm);
+int launch_keep_parts(qd_layout* L, double* op, unsigned keep);
 int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
 int launch_221_trace(qd_layout* L, const qd_op* A, const qd_op* B, const qd_op* w1, const qd_op* w2, double* C);
 int launch_221_fused(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
