@@ -23,8 +23,9 @@
 // and C(pair) = (orientation sign) * Y(cell).  The ket legs are the same with
 // F' and V transposed.  Each product runs along "fibers": a fixed k2 (F_g,
 // length |G_g|) or a fixed k1 (F_h, length |G_h|).  A warp takes one group
-// pair and direction at a time; each lane keeps one row of F in registers
-// and the lanes of a fiber read its cells as shared-memory broadcasts.
+// pair and direction at a time and forms the product on the FP64 tensor pipe
+// (mma.sync m8n8k4): F as A fragments held in registers, the staged cells as
+// B fragments, FA * VB and -FB * VA into one accumulator.
 //
 // Pass 1 (bra, SET): a CTA stages TJ columns of V_A and V_B (all ntot rows,
 // upper classes through herm) in shared memory in cell order, runs the k1

@@ -206,10 +206,6 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
 // wait for the phase with parity `ph`; false if it did not complete in time
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned ph) {
   for (long long it = 0; it < SG_SPIN; ++it) {
