@@ -523,7 +523,11 @@ def run_flow(args, world, rank, local):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
-                "config": {"workload": flow_desc(args), "form": form_name(args.split), "E_HF": float(vec[0]),
+                "config": {"workload": flow_desc(args), "form": form_name(args.split),
+                           "chosen_form": "plain FP64 block contractions, BCH terms replayed as CUDA graphs: on "
+                                          "this ladders-only flow the split form (--split S) and the learned "
+                                          "warm start (--workload warmstart) measure slower",
+                           "E_HF": float(vec[0]),
                            "fp64_flow": fp64,
                            "dE_vs_fp64": (abs(float(res.E0) - fp64["E_gs"]) if fp64 else None),
                            "E_gs": float(res.E0), "flow_steps": int(res.iterations), "rejected": int(res.rejected),
