@@ -209,7 +209,7 @@ def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_p
         f = flops["ladder"] if name == "ladder_gemm" else flops["pandya"] / 2
         return {"kernel": "k_split_gemm (%s, %d slices)" % (name, split), "bound": "tensor",
                 "achieved": f * slice_pairs(split) / per_launch_s / 1e12, "peak": bf16_peak_tflops(),
-                "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured, burst)",
+                "unit": "TFLOP/s", "peak_source": bf16_source(),
                 "algorithmic_per_launch": f * slice_pairs(split),
                 "note": "BF16 slice-product FLOPs = FP64-algorithm FLOPs x %d slice pairs; the stage time "
                         "includes slicing the operands" % slice_pairs(split)}
@@ -227,11 +227,11 @@ def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_p
     if name == "c122":
         byts = 3.0 * 8 * neq2b  # read A, B two-body, write C two-body
         return {"kernel": "k_122 (commutator_122)", "bound": "hbm", "achieved": byts / per_launch_s / 1e9,
-                "peak": hbm_peak, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                "peak": hbm_peak, "unit": "GB/s", "peak_source": hbm_source(),
                 "algorithmic_per_launch": byts}
     byts = 3.0 * 8 * neq2b
     return {"kernel": name, "bound": "hbm", "achieved": byts / per_launch_s / 1e9, "peak": hbm_peak,
-            "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs", "algorithmic_per_launch": byts}
+            "unit": "GB/s", "peak_source": hbm_source(), "algorithmic_per_launch": byts}
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
@@ -247,6 +247,20 @@ NCU_TRAFFIC = {"ladder_gemm": 794.761728e6 + 162.643712e6, "pandya_gemm": 200.46
 # flow's basis by entries per operator
 NCU_FLOW_NEQ = 29618726
 NCU_FLOW_TRAFFIC = {"c122": 712.7e6 + 232.8e6}
+
+
+def _peaks_present() -> bool:
+    return os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json"))
+
+
+def hbm_source() -> str:
+    return ("MEASURED_PEAKS.json hbm_gbs (of measured)" if _peaks_present()
+            else "fallback 6650 GB/s: MEASURED_PEAKS.json absent (of fallback)")
+
+
+def bf16_source() -> str:
+    return ("MEASURED_PEAKS.json bf16_tflops (of measured, burst)" if _peaks_present()
+            else "fallback 1590 TFLOP/s: MEASURED_PEAKS.json absent (of fallback)")
 
 
 def hbm_peak_gbs() -> float:
@@ -508,7 +522,7 @@ def run_flow(args, world, rank, local):
     per = (ms / max(cnt, 1)) / 1e3
     byts = 3.0 * 8 * neq2b
     roof = {"kernel": name, "bound": "hbm", "achieved": byts / per / 1e9, "peak": hbm_peak_gbs(), "unit": "GB/s",
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)", "algorithmic_per_launch": byts,
+            "peak_source": hbm_source(), "algorithmic_per_launch": byts,
             "note": "stage with the most device time, per launch = per commutator; bytes = read A, B and "
                     "write C two-body parts once",
             "traffic": NCU_FLOW_TRAFFIC[name] * P.neq / NCU_FLOW_NEQ if name in NCU_FLOW_TRAFFIC else None,
