@@ -50,7 +50,8 @@ constexpr size_t SMEM_STATIC_122 = 1024;           // bound on the pass kernels'
 // Per-pass TJ rule (measured on the N=20 R=20 flow, 122 ms per flow): both
 // passes at TJ >= 2 within 74 KB, 592; the ket pass at TJ >= 4 within 112 or
 // 150 KB (whole 32-byte sectors, fewer CTAs), 812-820; TJ = 1 on the largest
-// blocks of either pass, 637-808.  Parallelism beats sector efficiency here.
+// blocks of either pass, 637-808; 8 staging loads in flight per thread
+// instead of 4 (U122), 611.  Parallelism beats sector efficiency here.
 constexpr size_t KET_SMEM_TARGET_122 = 74 * 1024;   // ket pass: three CTAs per SM
 constexpr int KET_MIN_TJ_122 = 2;
 constexpr int BRA_MIN_TJ_122 = 2;
