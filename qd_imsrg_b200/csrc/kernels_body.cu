@@ -157,7 +157,11 @@ int launch_221_trace(qd_layout* L, const qd_op* A, const qd_op* B, const qd_op* 
 // qd_commutator_221 keeps the reference's visible w1/w2.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double w221_stored(const DevLayout& L, int which, int q, int sl, int r, int c,
-                                              const double* __restrict__ A, const double* __restrict__ B) {
+                                              const double* __restrict__ A, const double* __restrict__ B,
+                                              unsigned zA, unsigned zB) {
+  // an operand part known to be zero makes the element an exact zero
+  auto zero = [&](unsigned za, unsigned zb) { return ((zA & za) | (zB & zb)) != 0u; };
+  const unsigned pphh = 1u << P_PPHH, ppph = 1u << P_PPPH, phhh = 1u << P_PHHH;
   const int4 bd = __ldg(&L.blk[q]);
   const int nh = bd.x, nb = bd.y, np = bd.z;
   const i64* o = L.boff + 6 * q;
@@ -166,30 +170,35 @@ __device__ __forceinline__ double w221_stored(const DevLayout& L, int which, int
   if (which == 1) {
     switch (sl) {
       case 0: {  // Bpphh^T Apphh
+        if (zero(pphh, pphh)) break;
         const double* u = B + __ldg(o + 2) + (i64)r * np;
         const double* v = A + __ldg(o + 2) + (i64)c * np;
         for (int k = 0; k < np; ++k) s += u[k] * v[k];
         break;
       }
       case 1: {  // Apphh Bpphh^T
+        if (zero(pphh, pphh)) break;
         const double* u = A + __ldg(o + 2) + r;
         const double* v = B + __ldg(o + 2) + c;
         for (int k = 0; k < nh; ++k) s += u[(i64)k * np] * v[(i64)k * np];
         break;
       }
       case 3: {  // Bppph^T Appph
+        if (zero(ppph, ppph)) break;
         const double* u = B + __ldg(o + 4) + (i64)r * np;
         const double* v = A + __ldg(o + 4) + (i64)c * np;
         for (int k = 0; k < np; ++k) s += u[k] * v[k];
         break;
       }
       case 5: {  // Bppph^T Apphh
+        if (zero(pphh, ppph)) break;
         const double* u = B + __ldg(o + 4) + (i64)r * np;
         const double* v = A + __ldg(o + 2) + (i64)c * np;
         for (int k = 0; k < np; ++k) s += u[k] * v[k];
         break;
       }
       case 4: {  // Apphh Bphhh^T
+        if (zero(pphh, phhh)) break;
         const double* u = A + __ldg(o + 2) + r;
         const double* v = B + __ldg(o + 5) + c;
         for (int k = 0; k < nh; ++k) s += u[(i64)k * np] * v[(i64)k * nb];
@@ -200,18 +209,21 @@ __device__ __forceinline__ double w221_stored(const DevLayout& L, int which, int
   } else {
     switch (sl) {
       case 3: {  // Aphhh Bphhh^T
+        if (zero(phhh, phhh)) break;
         const double* u = A + __ldg(o + 5) + r;
         const double* v = B + __ldg(o + 5) + c;
         for (int k = 0; k < nh; ++k) s += u[(i64)k * nb] * v[(i64)k * nb];
         break;
       }
       case 5: {  // Appph^T Bpphh
+        if (zero(ppph, pphh)) break;
         const double* u = A + __ldg(o + 4) + (i64)r * np;
         const double* v = B + __ldg(o + 2) + (i64)c * np;
         for (int k = 0; k < np; ++k) s += u[k] * v[k];
         break;
       }
       case 4: {  // Bpphh Aphhh^T
+        if (zero(phhh, pphh)) break;
         const double* u = B + __ldg(o + 2) + r;
         const double* v = A + __ldg(o + 5) + c;
         for (int k = 0; k < nh; ++k) s += u[(i64)k * np] * v[(i64)k * nb];
@@ -225,7 +237,8 @@ __device__ __forceinline__ double w221_stored(const DevLayout& L, int which, int
 
 // v_elem(w, a, b, c, d) of intermediate w (herm +1) through w221_stored
 __device__ __forceinline__ double w221(const DevLayout& L, int which, const double* __restrict__ A,
-                                       const double* __restrict__ B, int a, int b, int c, int d) {
+                                       const double* __restrict__ B, unsigned zA, unsigned zB, int a, int b, int c,
+                                       int d) {
   if (a == b || c == d) return 0.0;
   const int e1 = __ldg(&L.ptab[a * L.m + b]);
   const int e2 = __ldg(&L.ptab[c * L.m + d]);
@@ -241,14 +254,15 @@ __device__ __forceinline__ double w221(const DevLayout& L, int which, const doub
   if (c1 == 0) sl = 0;
   else if (c1 == 1) sl = c2 == 0 ? 5 : 3;
   else sl = c2 == 0 ? 2 : (c2 == 1 ? 4 : 1);
-  return sgn * w221_stored(L, which, q, sl, i1, i2, A, B);
+  return sgn * w221_stored(L, which, q, sl, i1, i2, A, B, zA, zB);
 }
 
 constexpr int T221 = 128;
 
 __global__ void __launch_bounds__(T221) k_221_fused(DevLayout L, const int* __restrict__ targets, double hA,
                                                     double hB, const double* __restrict__ A,
-                                                    const double* __restrict__ B, double* __restrict__ C) {
+                                                    const double* __restrict__ B, unsigned zA, unsigned zB,
+                                                    double* __restrict__ C) {
   __shared__ double sh[T221 / 32];
   const int n = L.n, mp = L.mp, m = L.m;
   const i64 nhh = (i64)n * n, npp = (i64)mp * mp;
@@ -258,14 +272,14 @@ __global__ void __launch_bounds__(T221) k_221_fused(DevLayout L, const int* __re
   double s = 0.0;
   for (int u = threadIdx.x; u < m; u += T221) {
     if (t < nhh) {  // fhh(h,h2): x = h, y = h2
-      if (u < n) s += hA * w221(L, 1, A, B, u, y, u, x) - hB * w221(L, 1, A, B, u, x, u, y);
-      else s += -hA * w221(L, 2, A, B, u, y, u, x) + hB * w221(L, 2, A, B, u, x, u, y);
+      if (u < n) s += hA * w221(L, 1, A, B, zA, zB, u, y, u, x) - hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
+      else s += -hA * w221(L, 2, A, B, zA, zB, u, y, u, x) + hB * w221(L, 2, A, B, zA, zB, u, x, u, y);
     } else if (t < nhh + npp) {  // fpp(p,p2)
-      if (u < n) s += hA * w221(L, 1, A, B, u, y, u, x) - hB * w221(L, 1, A, B, u, x, u, y);
-      else s += -hA * w221(L, 1, A, B, u, y, u, x) + hB * w221(L, 1, A, B, u, x, u, y);
+      if (u < n) s += hA * w221(L, 1, A, B, zA, zB, u, y, u, x) - hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
+      else s += -hA * w221(L, 1, A, B, zA, zB, u, y, u, x) + hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
     } else {  // fph(p,h)
-      if (u < n) s += hA * w221(L, 2, A, B, u, x, u, y) - hB * w221(L, 1, A, B, u, x, u, y);
-      else s += -hA * w221(L, 2, A, B, u, x, u, y) + hB * w221(L, 1, A, B, u, x, u, y);
+      if (u < n) s += hA * w221(L, 2, A, B, zA, zB, u, x, u, y) - hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
+      else s += -hA * w221(L, 2, A, B, zA, zB, u, x, u, y) + hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
     }
   }
   s = block_sum<T221>(s, sh);
@@ -290,7 +304,7 @@ int launch_221_fused(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   }
   if (L->ntgt221 > 0) {
     k_221_fused<<<L->ntgt221, T221, 0, L->stream>>>(L->dev, L->d_tgt221, (double)A->herm, (double)B->herm, A->d,
-                                                   B->d, C);
+                                                   B->d, A->zero_mask, B->zero_mask, C);
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());
