@@ -45,8 +45,15 @@ __global__ void k_ccflag(DevLayout L, const double* __restrict__ A, const double
   if (A[f] != 0.0 || B[f] != 0.0) flag[__ldg(&L.ccmap[i * L.m + a]).x] = 1;
 }
 
+// stored part holding pairs of classes c1, c2 (0 hh, 1 ph, 2 pp), as a P_* bit
+__device__ __forceinline__ unsigned part_bit_of(int c1, int c2) {
+  const int hi = c1 > c2 ? c1 : c2, lo = c1 > c2 ? c2 : c1;
+  const int part = hi == 0 ? P_HHHH : (hi == 1 ? (lo == 0 ? P_PHHH : P_PHPH) : (lo == 0 ? P_PPHH : (lo == 1 ? P_PPPH : P_PPPP)));
+  return 1u << part;
+}
+
 __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, const double* __restrict__ B, double hB,
-                      const int* __restrict__ flag, double* __restrict__ C) {
+                      unsigned zA, unsigned zB, const int* __restrict__ flag, double* __restrict__ C) {
   const i64 n1 = (i64)L.n * L.n + (i64)L.mp * L.mp + (i64)L.mp * L.n;
   i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n1) return;
@@ -56,6 +63,12 @@ __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, cons
   const int q1 = __ldg(&L.ccmap[x * L.m + y]).x, q2 = __ldg(&L.ccmap[y * L.m + x]).x;
   const bool on1 = __ldg(flag + q1) != 0, on2 = __ldg(flag + q2) != 0;
   if (!on1 && !on2) return;
+  // the two-body elements of each sum lie in one part fixed by the target's
+  // hole/particle types: a part known to be zero makes its terms exact zeros
+  const bool px = x >= n, py = y >= n;
+  const unsigned part1 = part_bit_of(px ? 2 : 1, py ? 1 : 0);  // <a x|i y>, a particle, i hole
+  const unsigned part2 = part_bit_of(px ? 1 : 0, py ? 2 : 1);  // <i x|a y>
+  const bool b1 = !(zB & part1), a1 = !(zA & part1), b2 = !(zB & part2), a2 = !(zA & part2);
   double s = 0.0;
   if (on1) {
     int base = __ldg(&L.cchp_base[q1]), nb = __ldg(&L.ccdim[q1]).y;
@@ -63,7 +76,9 @@ __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, cons
       int2 ia = __ldg(&L.cchp[base + k]);
       const int i = ia.x, a = ia.y;
       double fa = A[L.o_fph + (a - n) + (i64)i * mp], fb = B[L.o_fph + (a - n) + (i64)i * mp];
-      s += fa * hA * dv_elem(L, B, hB, a, x, i, y) - fb * hB * dv_elem(L, A, hA, a, x, i, y);
+      const double tb = b1 ? fa * hA * dv_elem(L, B, hB, a, x, i, y) : 0.0;
+      const double ta = a1 ? fb * hB * dv_elem(L, A, hA, a, x, i, y) : 0.0;
+      s += tb - ta;
     }
   }
   if (on2) {
@@ -72,7 +87,9 @@ __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, cons
       int2 ia = __ldg(&L.cchp[base + k]);
       const int i = ia.x, a = ia.y;
       double fa = A[L.o_fph + (a - n) + (i64)i * mp], fb = B[L.o_fph + (a - n) + (i64)i * mp];
-      s += -fa * dv_elem(L, B, hB, i, x, a, y) + fb * dv_elem(L, A, hA, i, x, a, y);
+      const double tb = b2 ? -fa * dv_elem(L, B, hB, i, x, a, y) : 0.0;
+      const double ta = a2 ? fb * dv_elem(L, A, hA, i, x, a, y) : 0.0;
+      s += tb + ta;
     }
   }
   C[L.o_fhh + t] += s;
@@ -94,6 +111,7 @@ int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
     ++L->nlaunch;
   }
   k_121<<<(unsigned)((n1 + 127) / 128), 128, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d, (double)B->herm,
+                                                             A->zero_mask, B->zero_mask,
                                                              L->d_ccflag, C);
   ++L->nlaunch;
   QD_CUDA(cudaGetLastError());
