@@ -33,6 +33,8 @@ __all__ = [
     "commutator_122", "commutator_222", "commutator", "calc_cc", "build_white", "add_arrays",
     "copy_arrays", "set_to_zero", "mat_2_norm", "mbpt2", "hf_e2", "bch_expand", "magnus_expand",
     "euler_step", "magnus_flow", "random_operator", "tbme_write", "hf_hamiltonian", "v_int",
+    "Flow", "magnus_flow_batch", "dgam", "eom_matvec", "gemm_split", "hamiltonian_write", "hamiltonian_read",
+    "export_hamiltonian", "import_hamiltonian",
 ]
 
 _dp = C.POINTER(C.c_double)
