@@ -456,9 +456,7 @@ def flow_desc(args):
 def run_flow(args, world, rank, local):
     """Seconds to a converged ground-state energy: Hartree-Fock on the host,
     then the Magnus flow on the device to |MBPT2(H(s))| <= 1e-9, one flow per
-    step.  The one- plus two-body norm drives the BCH truncation and the step
-    rejection (the reference's one-body norm never accepts a step on a
-    Hartree-Fock Hamiltonian)."""
+    step."""
     import torch
 
     import qd_imsrg_b200 as qd
@@ -472,7 +470,7 @@ def run_flow(args, world, rank, local):
     H, HS = qd.FullHam(P, 1, vec), qd.FullHam(P, 1)
 
     def flow():
-        return qd.magnus_flow(H, HS, pandya=args.pandya, full_norm=True, max_iter=1000)
+        return qd.magnus_flow(H, HS, pandya=args.pandya, max_iter=1000)
 
     fp64 = None
     if args.split:
@@ -588,7 +586,7 @@ def run_batch(args, world, rank, local):
         inst.append({"N": nb, "hw": hw, "R": R, "P": P, "H": qd.FullHam(P, 1, vec), "HS": qd.FullHam(P, 1),
                      "E_HF": float(vec[0])})
     setup_s = time.perf_counter() - t0
-    kw = dict(pandya=args.pandya, full_norm=True, max_iter=args.batch_max_iter)
+    kw = dict(pandya=args.pandya, max_iter=args.batch_max_iter)
     # one after another (also allocates every layout's flow workspaces)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
@@ -752,8 +750,7 @@ def run_reference_flow(args, world, rank):
         import oracle
 
         O = oracle.Layout(args.nbody, args.emax, eig=eig)
-        tr, _ = oracle.magnus_flow(oracle.Op(O, 1, vec), oracle.Op(O, 1), pandya=args.pandya, max_iter=1000,
-                                   full_norm=True)
+        tr, _ = oracle.magnus_flow(oracle.Op(O, 1, vec), oracle.Op(O, 1), pandya=args.pandya, max_iter=1000)
         comms, how = int(np.abs(tr[:, 6]).sum()), "counted by running the CPU flow"
     vals = []
     for k in range(args.warmup + args.steps):

@@ -7,8 +7,8 @@
  * Hartree-Fock, TBME generation and EOM; it hands the normal-ordered
  * Hamiltonian to this library in the reference's own flat "vectorize" order
  * (src/ME_general.f90:1871-1989) and calls the commutator / BCH / Magnus
- * routines on device-resident operators.  INTEGRATION.md shows the
- * iso_c_binding interface module a Fortran caller would add.
+ * routines on device-resident operators, through an iso_c_binding interface
+ * module on the Fortran side.
  *
  * Conventions
  *   - Every function returns an int status: QD_OK (0) or a QD_ERR_* code;
@@ -132,28 +132,36 @@ int qd_random_operator(const qd_layout* L, int herm, uint64_t seed, double sigma
 int qd_add_arrays(const qd_op* r1, double s1, const qd_op* r2, double s2, qd_op* r3); /* r3=s1*r1+s2*r2 */
 int qd_copy_arrays(const qd_op* r1, qd_op* r2);                                        /* r2 = r1      */
 int qd_set_to_zero(qd_op* r1);
-/* mat_2_norm: as the reference, the one-body parts only (its block loop is
- * empty): sqrt(sum fph^2 + sum fpp^2 + sum fhh^2)                            */
+/* mat_2_norm (:2112-2138): sqrt of the sum of squares of every stored one-
+ * and two-body entry, E0 excluded: fph, fpp, fhh and, per block, Vhhhh,
+ * Vpppp, Vpphh, Vphph, Vphhh, Vppph.  Synchronous.                          */
 int qd_mat_2_norm(const qd_op* r, double* out);
 
-/* Allocation-free one-body norm, for callers that must not allocate device
+/* Allocation-free mat_2_norm, for callers that must not allocate device
  * memory while they run (a host that reserves its device-memory budget up
  * front and forbids allocation inside its flow loop, or one whose memory is
  * held by another allocator, where cudaMalloc may fail or synchronise the
- * device).  No counterpart in the reference.
- *   d_op   device array of one operator in vectorize order (e.g. from
- *          qd_op_device_ptr); d_norm: device double receiving the norm;
- *   stream cudaStream_t to run on (NULL: legacy default stream); the call is
- *          asynchronous: the result is in d_norm once the stream reaches it.
+ * device).  Same value as qd_mat_2_norm (every stored one- and two-body
+ * entry); no counterpart in the reference.
+ *   d_op   device array of one operator of layout L in vectorize order (e.g.
+ *          from qd_op_device_ptr); d_norm: device double receiving the norm;
+ *   stream cudaStream_t to run on.  NULL: the layout's own stream, so the
+ *          call is ordered after every earlier call on the layout and before
+ *          every later one.  A caller's stream must be ordered against the
+ *          layout's stream by the caller (qd_layout_synchronize, or events).
+ *          The call is asynchronous: d_norm holds the norm once the stream
+ *          reaches it.
  * Nothing is allocated: the partial sums live in a static device array of
  * QD_NOALLOC_MAX_PARTIALS doubles (32 KiB, held by every GPU that loads the
- * library until exit).  Layouts with more than QD_NOALLOC_MAX_ENTRIES
- * one-body entries are rejected with QD_ERR_ARG.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array, so calls that
+ * library until exit).  Layouts with more than QD_NOALLOC_MAX_ENTRIES one-
+ * and two-body entries (1 GiB per operator) are rejected with QD_ERR_ARG.
+ * The kernels run on the layout's device; the calling thread's current
+ * device is restored before returning.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array, so calls that
  * overlap on the GPU race.                                                   */
 #define QD_NOALLOC_MAX_PARTIALS 4096
-#define QD_NOALLOC_MAX_ENTRIES (4096LL * 2048LL)
+#define QD_NOALLOC_MAX_ENTRIES (4096LL * 32768LL)
 int qd_mat_2_norm_noalloc(const qd_layout* L, const double* d_op, double* d_norm, void* stream);
 
 /* ---- commutators (src/commutators.f90) ------------------------------------- */
@@ -176,12 +184,6 @@ int qd_commutator_222(const qd_op* r1, const qd_op* r2, qd_op* r3, qd_op* w1, co
  * matrices first (as dGam, src/gs_IMSRG.f90:243-250); without it the
  * particle-hole channel is skipped (X = 0, as run_magnus).                  */
 #define QD_PANDYA 1u
-/* For qd_bch_expand / qd_magnus_flow: take the BCH truncation norm and the
- * eta norm of the step rejection over every stored one- and two-body entry.
- * The reference's mat_2_norm sums the one-body parts only (its block loop is
- * empty); on a Hartree-Fock Hamiltonian, whose ph Fock block vanishes, that
- * makes the initial eta norm ~1e-16, so run_magnus rejects every step.      */
-#define QD_FULL_NORM 2u
 int qd_commutator(const qd_op* A, const qd_op* B, qd_op* C, unsigned flags);
 /* dGam, src/gs_IMSRG.f90:223-273: the derivative of the ODE form of the flow,
  * the right-hand side the host's Adams integrator (adams_ode) evaluates.
@@ -247,11 +249,14 @@ double qd_v_int_quad(const int* qi, const int* qj, const int* qk, const int* ql,
 
 /* ---- BCH / Magnus (src/magnus_IMSRG.f90) ----------------------------------- */
 /* BCH_EXPAND :253-318: HS = sum_k ad_G^k(H) cof(k) with the reference's
- * truncated cof table and exit test |INT2|*cof/|INT1| < 1e-5 (one-body norm).
- * INT1, INT2, AD, w1, w2 are caller workspaces (contents unspecified on
- * return); HCC/OCC as in the reference (never filled -> no ph channel) unless
- * flags has QD_PANDYA, which refills them from AD and G before each 222.
- * *nterms receives the number of commutators evaluated.                      */
+ * truncated cof table and exit test mat_2_norm(INT2)*cof/mat_2_norm(INT1)
+ * < 1e-5.  INT2, AD, w1, w2 are caller workspaces (contents unspecified on
+ * return).  INT1 is not written: the reference copies HS into it before
+ * every term (:290) only to take its norm, which is taken here from HS in
+ * the same pass as the update; a caller that reads INT1 afterwards must copy
+ * HS itself.  HCC/OCC as in the reference (never filled -> no ph channel)
+ * unless flags has QD_PANDYA, which refills them from AD and G before each
+ * 222.  *nterms receives the number of commutators evaluated.               */
 int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op* INT2, qd_op* AD,
                   qd_op* w1, qd_op* w2, qd_cc* HCC, qd_cc* OCC, unsigned flags, int* nterms);
 /* MAGNUS_EXPAND :321-369: the reference returns after DG = ETA.              */

@@ -83,7 +83,6 @@ def lib():
             "orc_copy_arrays": (None, [_vp, _vp]),
             "orc_set_to_zero": (None, [_vp]),
             "orc_mat_2_norm": (C.c_double, [_vp]),
-            "orc_mat_2_norm_full": (C.c_double, [_vp]),
             "orc_mbpt2": (C.c_double, [_vp]),
             "orc_hf_e2": (C.c_double, [_vp]),
             "orc_bch_expand": (C.c_int, [_vp, _vp, _vp, C.c_int]),
@@ -318,16 +317,8 @@ def hf_e2(r) -> float:
     return float(lib().orc_hf_e2(r.h))
 
 
-def mat_2_norm_full(r) -> float:
-    return float(lib().orc_mat_2_norm_full(r.h))
-
-
-def _flags(pandya: bool, full_norm: bool) -> int:
-    return (1 if pandya else 0) | (2 if full_norm else 0)
-
-
-def bch_expand(HS: Op, G: Op, H: Op, pandya: bool = False, full_norm: bool = False) -> int:
-    return int(lib().orc_bch_expand(HS.h, G.h, H.h, _flags(pandya, full_norm)))
+def bch_expand(HS: Op, G: Op, H: Op, pandya: bool = False) -> int:
+    return int(lib().orc_bch_expand(HS.h, G.h, H.h, 1 if pandya else 0))
 
 
 class Sampler:
@@ -351,11 +342,11 @@ class Sampler:
             self.h = None
 
 
-def magnus_flow(HAM: Op, HS: Op, pandya: bool = False, max_iter: int = 500, full_norm: bool = False):
+def magnus_flow(HAM: Op, HS: Op, pandya: bool = False, max_iter: int = 500):
     """s_evolve(build_white); returns (trace[rows,7], s)."""
     trace = np.zeros((max_iter, 7), np.float64)
     s = C.c_double(0.0)
-    rows = int(lib().orc_magnus_flow(HAM.h, HS.h, _flags(pandya, full_norm), int(max_iter), _dptr(trace),
+    rows = int(lib().orc_magnus_flow(HAM.h, HS.h, 1 if pandya else 0, int(max_iter), _dptr(trace),
                                      C.byref(s)))
     if rows < 0:
         raise RuntimeError("oracle Magnus flow did not converge within %d iterations" % max_iter)

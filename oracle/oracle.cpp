@@ -391,27 +391,30 @@ void add_arrays(Op& r1, double s1, Op& r2, double s2, Op& r3) {
 void copy_arrays(Op& r1, Op& r2) { r2.v = r1.v; }
 void set_to_zero(Op& r1) { std::fill(r1.v.begin(), r1.v.end(), 0.0); }
 
-// mat_2_norm, ME_general.f90:2112-2138: the block loop of the reference is
-// empty, so only the one-body parts enter: od = 0 + sum(fph**2) + sum(fpp**2)
-// + sum(fhh**2).
+// mat_2_norm, ME_general.f90:2112-2138: the square root of the sum of
+// squares of every stored one- and two-body entry (E0 excluded), in the
+// reference's order: od = od + sum(fph**2) + sum(fpp**2) + sum(fhh**2)
+// (:2125), then per block q (:2127-2133)
+// od = od + sum(Vhhhh**2) + sum(Vpppp**2) + sum(Vpphh**2) + sum(Vphph**2)
+//         + sum(Vphhh**2) + sum(Vppph**2), each line summed left to right.
+namespace {
+double sumsq(const double* x, i64 n) {
+  double s = 0.0;
+  for (i64 i = 0; i < n; ++i) s += x[i] * x[i];
+  return s;
+}
+}  // namespace
 double mat_2_norm(Op& r) {
   const Layout& L = *r.L;
-  int n = L.n, mp = L.m - L.n;
-  double sph = 0, spp = 0, shh = 0;
-  for (i64 i = 0; i < (i64)mp * n; ++i) { double x = r.v[L.o_fph + i]; sph += x * x; }
-  for (i64 i = 0; i < (i64)mp * mp; ++i) { double x = r.v[L.o_fpp + i]; spp += x * x; }
-  for (i64 i = 0; i < (i64)n * n; ++i) { double x = r.v[L.o_fhh + i]; shh += x * x; }
+  const i64 n = L.n, mp = L.m - L.n;
   double od = 0.0;
-  od = od + sph + spp + shh;
-  return std::sqrt(od);
-}
-
-// The norm mat_2_norm's name intends: every stored one- and two-body entry
-// (E0 excluded).  Used only when a caller asks for it (flag 2 of the BCH and
-// flow drivers); the reference's own mat_2_norm is the one-body-only one.
-double mat_2_norm_full(Op& r) {
-  double od = 0.0;
-  for (i64 i = 1; i < r.L->neq; ++i) od += r.v[i] * r.v[i];
+  od = od + sumsq(&r.v[L.o_fph], mp * n) + sumsq(&r.v[L.o_fpp], mp * mp) + sumsq(&r.v[L.o_fhh], n * n);
+  for (int q = 1; q <= L.nblock; ++q) {
+    const Blk& b = L.blk[q - 1];
+    const i64 nh = b.nhh, nb = b.nph, np = b.npp;
+    od = od + sumsq(r.Vhhhh(q), nh * nh) + sumsq(r.Vpppp(q), np * np) + sumsq(r.Vpphh(q), np * nh) +
+         sumsq(r.Vphph(q), nb * nb) + sumsq(r.Vphhh(q), nb * nh) + sumsq(r.Vppph(q), np * nb);
+  }
   return std::sqrt(od);
 }
 
@@ -1056,11 +1059,8 @@ struct Sampler {
 // flags bit 0: calc_cc on G and AD before every commutator_222 (run_magnus
 //              never fills the cross-coupled X, so without it the ph channel
 //              is absent, as in the reference);
-// flags bit 1: truncation test with the one- plus two-body norm instead of
-//              the reference's one-body mat_2_norm.
 int BCH_EXPAND(Op& HS, Op& G, Op& H, Op& INT1, Op& INT2, Op& AD, Op& w1, Op& w2, CC& HCC, CC& OCC, int flags) {
   const int pandya = flags & 1;
-  double (*nrm)(Op&) = (flags & 2) ? mat_2_norm_full : mat_2_norm;
   const double conv = 1e-5;
   const double cof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666, 0.0083333333333333333,
                           .001388888888888, 1.984126984e-4, 2.48015873e-5, 2.755731922e-6, 2.755731922e-7,
@@ -1096,7 +1096,7 @@ int BCH_EXPAND(Op& HS, Op& G, Op& H, Op& INT1, Op& INT2, Op& AD, Op& w1, Op& w2,
     commutator_222(G, AD, INT2, w1, HCC, OCC);
     ++count;
     add_arrays(INT1, 1.0, INT2, cof[i - 2], HS);
-    if (nrm(INT2) * cof[i - 2] / nrm(INT1) < convd) break;
+    if (mat_2_norm(INT2) * cof[i - 2] / mat_2_norm(INT1) < convd) break;
   }
   return count;
 }
@@ -1274,7 +1274,6 @@ void orc_add_arrays(void* r1, double s1, void* r2, double s2, void* r3) {
 void orc_copy_arrays(void* r1, void* r2) { copy_arrays(*(Op*)r1, *(Op*)r2); }
 void orc_set_to_zero(void* r1) { set_to_zero(*(Op*)r1); }
 double orc_mat_2_norm(void* r) { return mat_2_norm(*(Op*)r); }
-double orc_mat_2_norm_full(void* r) { return mat_2_norm_full(*(Op*)r); }
 double orc_mbpt2(void* r) { return MBPT2(*(Op*)r); }
 double orc_hf_e2(void* r) { return HF_E2(*(Op*)r); }
 
@@ -1291,8 +1290,7 @@ int orc_bch_expand(void* HS, void* G, void* H, int flags) {
 // s_evolve with build_white, magnus_IMSRG.f90:194-248 (TDA/spectrum
 // diagnostics omitted; they do not feed back into the flow).  HAM is the
 // normal-ordered HF Hamiltonian (herm=+1), HS receives the evolved one.
-// flags as BCH_EXPAND (bit 1 also switches the eta-norm of the step
-// rejection to the one- plus two-body norm).
+// flags as BCH_EXPAND.
 // trace: per accepted-or-rejected iteration, 7 doubles:
 //   iteration, s, E0, nrm1, nrm2, crit, bch_terms (negative when rejected)
 // Returns the number of trace rows written, or -1 if max_iter was reached.
@@ -1309,9 +1307,8 @@ int orc_magnus_flow(void* HAMp, void* HSp, int flags, int max_iter, double* trac
   double s = 0.0, stp = (double)0.7f;  // "stp=.7" is a real(4) literal
   copy_arrays(HAM, HS);
   HS.herm = 1;
-  double (*nrm)(Op&) = (flags & 2) ? mat_2_norm_full : mat_2_norm;
   build_white(ETA, HS);
-  double nrm1 = nrm(ETA);
+  double nrm1 = mat_2_norm(ETA);
   double crit = std::fabs(MBPT2(HAM));
   int iteration = 0, rows = 0, loops = 0;
   while (crit > conv_criteria) {
@@ -1324,7 +1321,7 @@ int orc_magnus_flow(void* HAMp, void* HSp, int flags, int max_iter, double* trac
     int terms = BCH_EXPAND(HS, G, HAM, INT1, INT2, AD, w1, w2, HCC, OCC, flags);
     copy_arrays(ETA, ETA0);
     build_white(ETA, HS);
-    double nrm2 = nrm(ETA);
+    double nrm2 = mat_2_norm(ETA);
     double* t = trace + 7 * rows;
     t[0] = iteration; t[1] = s; t[2] = HS.E0(); t[3] = nrm1; t[4] = nrm2; t[5] = crit; t[6] = terms;
     ++rows;

@@ -25,10 +25,10 @@ import os
 import numpy as np
 
 from . import _native
-from ._native import QD_FULL_NORM, QD_PANDYA, QD_TBME_QUAD, FlowResult, FlowStepInfo, QDError, check, lib
+from ._native import QD_PANDYA, QD_TBME_QUAD, FlowResult, FlowStepInfo, QDError, check, lib
 
 __all__ = [
-    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA", "QD_FULL_NORM",
+    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA",
     "commutator_110", "commutator_220", "commutator_111", "commutator_121", "commutator_221",
     "commutator_122", "commutator_222", "commutator", "calc_cc", "build_white", "add_arrays",
     "copy_arrays", "set_to_zero", "mat_2_norm", "mbpt2", "hf_e2", "bch_expand", "magnus_expand",
@@ -318,15 +318,16 @@ def hf_e2(r) -> float:
     return _scalar(lib().qd_hf_e2, r.h)
 
 
-def _flags(pandya: bool, full_norm: bool) -> int:
-    return (QD_PANDYA if pandya else 0) | (QD_FULL_NORM if full_norm else 0)
+def _flags(pandya: bool) -> int:
+    return QD_PANDYA if pandya else 0
 
 
-def bch_expand(HS, G, H, INT1, INT2, AD, w1, w2, HCC: CCMat, OCC: CCMat, pandya: bool = False,
-               full_norm: bool = False) -> int:
+def bch_expand(HS, G, H, INT1, INT2, AD, w1, w2, HCC: CCMat, OCC: CCMat, pandya: bool = False) -> int:
+    """BCH_EXPAND; INT1 is accepted for the reference's argument list and is
+    not written (its norm is taken from HS in the update pass)."""
     n = C.c_int()
     check(lib().qd_bch_expand(HS.h, G.h, H.h, INT1.h, INT2.h, AD.h, w1.h, w2.h, HCC.h, OCC.h,
-                              _flags(pandya, full_norm), C.byref(n)))
+                              _flags(pandya), C.byref(n)))
     return n.value
 
 
@@ -340,13 +341,12 @@ def euler_step(G, DG, s: float, stp: float) -> float:
     return sv.value
 
 
-def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int = 500, full_norm: bool = False):
+def magnus_flow(HAM: FullHam, HS: FullHam, pandya: bool = False, max_iter: int = 500):
     """s_evolve(build_white): returns (trace[rows,7], FlowResult).  pandya adds
-    the particle-hole channel (absent in run_magnus); full_norm uses the one-
-    plus two-body norm in the BCH truncation and the step rejection."""
+    the particle-hole channel (absent in run_magnus)."""
     trace = np.zeros((max_iter, 7), np.float64)
     res = FlowResult()
-    check(lib().qd_magnus_flow(HAM.h, HS.h, _flags(pandya, full_norm), int(max_iter), _d(trace), C.byref(res)))
+    check(lib().qd_magnus_flow(HAM.h, HS.h, _flags(pandya), int(max_iter), _d(trace), C.byref(res)))
     return trace[: res.rows], res
 
 
@@ -355,10 +355,10 @@ class Flow:
     warm_start(G, s) seeds Omega = G at flow parameter s; step() runs one
     pass of the loop; omega() is the flow's Omega (owned by the flow)."""
 
-    def __init__(self, HAM: FullHam, HS: FullHam, pandya: bool = False, full_norm: bool = False):
+    def __init__(self, HAM: FullHam, HS: FullHam, pandya: bool = False):
         self.layout = HAM.layout
         self.h = C.c_void_p()
-        check(lib().qd_flow_create(HAM.h, HS.h, _flags(pandya, full_norm), C.byref(self.h)))
+        check(lib().qd_flow_create(HAM.h, HS.h, _flags(pandya), C.byref(self.h)))
 
     def warm_start(self, G: FullHam, s: float) -> None:
         check(lib().qd_flow_warm_start(self.h, G.h, float(s)))
@@ -421,8 +421,7 @@ class DeviceView:
         return {"shape": (self.n,), "typestr": "<f8", "data": (self.ptr, False), "version": 3, "strides": None}
 
 
-def magnus_flow_batch(pairs, pandya: bool = False, max_iter: int = 500, full_norm: bool = False,
-                      raise_on_error: bool = True):
+def magnus_flow_batch(pairs, pandya: bool = False, max_iter: int = 500, raise_on_error: bool = True):
     """Run several independent flows concurrently: pairs = [(HAM, HS), ...],
     each pair on its own layout.  Returns ([FlowResult], [status]); with
     raise_on_error, raises QDError for the first failing instance."""
@@ -431,7 +430,7 @@ def magnus_flow_batch(pairs, pandya: bool = False, max_iter: int = 500, full_nor
     hss = (C.c_void_p * n)(*[s.h.value for _, s in pairs])
     res = (FlowResult * n)()
     st = (C.c_int * n)()
-    rc = lib().qd_magnus_flow_batch(n, hams, hss, _flags(pandya, full_norm), int(max_iter), res, st)
+    rc = lib().qd_magnus_flow_batch(n, hams, hss, _flags(pandya), int(max_iter), res, st)
     out = [res[i] for i in range(n)], [int(st[i]) for i in range(n)]
     if raise_on_error:
         check(rc)

@@ -626,7 +626,7 @@ int qd_mat_2_norm(const qd_op* r, double* out) {
   CHECK(r && out, QD_ERR_ARG, "null argument");
   qd_layout* L = r->L;
   TRY(use_device(L));
-  TRY(reduce_norm1b(L, r->d, red_slot(L, 0)));
+  TRY(reduce_norm(L, r->d, red_slot(L, 0)));
   return scalar_out(L, red_slot(L, 0), out);
 }
 
@@ -856,7 +856,7 @@ struct TermGraph {
 using TermGraphs = std::map<TermKey, TermGraph>;
 
 int bch_term(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd_op* w1, qd_op* w2, qd_cc* HCC,
-             qd_cc* OCC, bool pandya, bool full, double cof) {
+             qd_cc* OCC, bool pandya, double cof) {
   if (pandya) {
     TRY(commutator_seq(L, G, AD, INT2, w1, w2, OCC, HCC, true));
   } else {
@@ -864,7 +864,7 @@ int bch_term(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd
   }
   {
     StageTimer tm(L, S_GLUE);
-    TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, full ? 1 : 0, red_slot(L, 1)));
+    TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, red_slot(L, 1)));
   }
   QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
   return QD_OK;
@@ -872,8 +872,8 @@ int bch_term(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd
 }  // namespace
 
 static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd_op* w1, qd_op* w2,
-                          qd_cc* HCC, qd_cc* OCC, bool pandya, bool full, int term, double cof) {
-  if (!L->use_graphs || L->prof.on) return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+                          qd_cc* HCC, qd_cc* OCC, bool pandya, int term, double cof) {
+  if (!L->use_graphs || L->prof.on) return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, cof);
   if (!L->graphs) L->graphs = new TermGraphs();
   TermKey k;
   std::memset(&k, 0, sizeof(k));
@@ -890,7 +890,7 @@ static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, 
   k.mhs = HS->zero_mask;
   k.gh = G->herm;
   k.term = term;
-  k.flags = (pandya ? 1 : 0) | (full ? 2 : 0);
+  k.flags = pandya ? 1 : 0;
   k.split = L->split_slices;
   TermGraph& tg = (*reinterpret_cast<TermGraphs*>(L->graphs))[k];
   if (tg.exec) {
@@ -908,7 +908,7 @@ static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, 
   }
   if (tg.failed || tg.seen == 0) {
     ++tg.seen;
-    return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+    return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, cof);
   }
   // second sight: capture, instantiate, launch
   const long long n0 = L->nlaunch;
@@ -916,7 +916,7 @@ static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, 
   int rc = QD_OK;
   cudaError_t e = cudaStreamBeginCapture(L->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    rc = bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+    rc = bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, cof);
     e = cudaStreamEndCapture(L->stream, &graph);
   }
   if (e == cudaSuccess && rc == QD_OK && graph) e = cudaGraphInstantiate(&tg.exec, graph, 0);
@@ -927,7 +927,7 @@ static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, 
     tg.exec = nullptr;
     tg.failed = true;
     L->nlaunch = n0;
-    return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, full, cof);
+    return bch_term(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, cof);
   }
   tg.launches = L->nlaunch - n0;
   ++L->graphs_captured;
@@ -943,7 +943,7 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   TRY(same_layout(HS, AD));
   TRY(same_layout(HS, w1));
   TRY(same_layout(HS, w2));
-  (void)INT1;  // the norm of INT1 (= HS before the update) is taken from HS itself
+  (void)INT1;  // not written: the norm of INT1 (= HS before the update) is taken from HS itself
   qd_layout* L = HS->L;
   TRY(use_device(L));
   TRY(build_programs(L));
@@ -959,7 +959,7 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
     std::swap(INT2->d, AD->d);  // AD = previous term; INT2 becomes the output buffer
     std::swap(INT2->zero_mask, AD->zero_mask);
     const double cof = kCof[i - 2];
-    TRY(bch_term_graph(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, (flags & QD_FULL_NORM) != 0, i, cof));
+    TRY(bch_term_graph(L, G, AD, INT2, HS, w1, w2, HCC, OCC, pandya, i, cof));
     ++count;
     HS->zero_mask &= INT2->zero_mask;
     QD_CUDA(cudaStreamSynchronize(L->stream));
@@ -1000,11 +1000,7 @@ struct qd_flow {
 namespace {
 const double kConvCriteria = (double)1e-9f;  // real(4) literal in the reference
 
-int flow_eta_norm(qd_flow* f, const qd_op* op, double* out) {
-  if (!(f->flags & QD_FULL_NORM)) return qd_mat_2_norm(op, out);
-  TRY(reduce_norm_full(f->L, op->d, red_slot(f->L, 0)));
-  return scalar_out(f->L, red_slot(f->L, 0), out);
-}
+int flow_eta_norm(qd_flow* f, const qd_op* op, double* out) { return qd_mat_2_norm(op, out); }
 
 int flow_e0(qd_flow* f, double* e0) {
   qd_layout* L = f->L;

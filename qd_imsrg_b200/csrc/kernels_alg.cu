@@ -193,8 +193,12 @@ int reduce_mbpt2(qd_layout* L, const double* h, double* dout) {
 int reduce_hhtrace(qd_layout* L, const double* h, double* dout) {
   return reduce_to(L, RedHHTrace{L->dev, h}, L->dev.pcnt[0], 1.0, 0.0, dout);
 }
-// one- plus two-body norm (every stored entry but E0), sqrt on the device
-int reduce_norm_full(qd_layout* L, const double* a, double* dout) {
+// mat_2_norm (src/ME_general.f90:2112-2138): sqrt of the sum of squares of
+// every stored one- and two-body entry (E0 excluded), sqrt on the device.
+// The entries are summed in vectorize order by the fixed two-stage tree; the
+// reference's order (fph, fpp, fhh, then per block hhhh, pppp, pphh, phph,
+// phhh, ppph) differs only in rounding.
+int reduce_norm(qd_layout* L, const double* a, double* dout) {
   int rc = reduce_to(L, RedDotRange{a, nullptr, L->o_fhh}, L->neq - L->o_fhh, 1.0, 0.0, dout);
   if (rc) return rc;
   k_sqrt<<<1, 1, 0, L->stream>>>(dout);
@@ -206,82 +210,60 @@ int reduce_norm_full(qd_layout* L, const double* a, double* dout) {
 // ---------------------------------------------------------------------------
 // One BCH_EXPAND term update in one pass (magnus_IMSRG.f90:298-316):
 //   c = sa*a + sb*b  (add_arrays, bit-identical: no FMA contraction)
-// together with the norms of both inputs, |a| = |INT1| (HS before the update)
-// and |b| = |INT2|, over the one-body parts (mat_2_norm) or over every stored
-// entry but E0 (full).  Fixed grid and fixed element -> thread assignment:
-// deterministic.  Partial sums: 4 per CTA (a 1-body, a rest, b 1-body, b rest).
+// together with mat_2_norm of both inputs, |a| = |INT1| (HS before the
+// update) and |b| = |INT2|, over every stored entry but E0.  Fixed grid and
+// fixed element -> thread assignment: deterministic.  Partial sums: 2 per
+// CTA (a, b).
 // ---------------------------------------------------------------------------
 constexpr int AXN_BLOCKS = 4 * 148, AXN_THREADS = 256;
 
 __global__ void __launch_bounds__(AXN_THREADS) k_axpy_norms(const double* __restrict__ a, double sa,
                                                             const double* __restrict__ b, double sb,
-                                                            double* __restrict__ c, i64 n, i64 o1, i64 e1,
+                                                            double* __restrict__ c, i64 n, i64 o1,
                                                             double* __restrict__ partial) {
   __shared__ double sh[AXN_THREADS / 32];
-  double a1 = 0.0, a2 = 0.0, b1 = 0.0, b2 = 0.0;
+  double an = 0.0, bn = 0.0;
   const i64 stride = (i64)gridDim.x * blockDim.x;
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const double x = a[i], y = b[i];
     c[i] = __dadd_rn(__dmul_rn(sa, x), __dmul_rn(sb, y));
     if (i >= o1) {
-      if (i < e1) {
-        a1 += x * x;
-        b1 += y * y;
-      } else {
-        a2 += x * x;
-        b2 += y * y;
-      }
+      an += x * x;
+      bn += y * y;
     }
   }
-  a1 = block_sum<AXN_THREADS>(a1, sh);
-  a2 = block_sum<AXN_THREADS>(a2, sh);
-  b1 = block_sum<AXN_THREADS>(b1, sh);
-  b2 = block_sum<AXN_THREADS>(b2, sh);
+  an = block_sum<AXN_THREADS>(an, sh);
+  bn = block_sum<AXN_THREADS>(bn, sh);
   if (threadIdx.x == 0) {
-    partial[blockIdx.x] = a1;
-    partial[gridDim.x + blockIdx.x] = a2;
-    partial[2 * gridDim.x + blockIdx.x] = b1;
-    partial[3 * gridDim.x + blockIdx.x] = b2;
+    partial[blockIdx.x] = an;
+    partial[gridDim.x + blockIdx.x] = bn;
   }
 }
 
-// out[0] = |a|, out[1] = |b| (one-body only, or one- plus two-body)
-__global__ void k_axpy_norms_final(const double* __restrict__ partial, int np, int full, double* __restrict__ out) {
+// out[0] = |a|, out[1] = |b|
+__global__ void k_axpy_norms_final(const double* __restrict__ partial, int np, double* __restrict__ out) {
   __shared__ double sh[RED_THREADS / 32];
-  double v[4];
-  for (int k = 0; k < 4; ++k) {
+  double v[2];
+  for (int k = 0; k < 2; ++k) {
     double s = 0.0;
     for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[k * np + i];
     v[k] = block_sum<RED_THREADS>(s, sh);
   }
   if (threadIdx.x == 0) {
-    out[0] = sqrt(full ? v[0] + v[1] : v[0]);
-    out[1] = sqrt(full ? v[2] + v[3] : v[2]);
+    out[0] = sqrt(v[0]);
+    out[1] = sqrt(v[1]);
   }
 }
 
-int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, int full,
+int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c,
                       double* dout2) {
   if (!L->d_axn) {
-    QD_CUDA(cudaMalloc(&L->d_axn, sizeof(double) * 4 * AXN_BLOCKS));
-    L->ws_bytes += sizeof(double) * 4 * AXN_BLOCKS;
+    QD_CUDA(cudaMalloc(&L->d_axn, sizeof(double) * 2 * AXN_BLOCKS));
+    L->ws_bytes += sizeof(double) * 2 * AXN_BLOCKS;
   }
-  const i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
-  k_axpy_norms<<<AXN_BLOCKS, AXN_THREADS, 0, L->stream>>>(a, sa, b, sb, c, L->neq, L->o_fhh, L->o_fhh + n1,
-                                                          L->d_axn);
-  k_axpy_norms_final<<<1, RED_THREADS, 0, L->stream>>>(L->d_axn, AXN_BLOCKS, full, dout2);
+  k_axpy_norms<<<AXN_BLOCKS, AXN_THREADS, 0, L->stream>>>(a, sa, b, sb, c, L->neq, L->o_fhh, L->d_axn);
+  k_axpy_norms_final<<<1, RED_THREADS, 0, L->stream>>>(L->d_axn, AXN_BLOCKS, dout2);
   L->nlaunch += 2;
-  QD_CUDA(cudaGetLastError());
-  return QD_OK;
-}
-
-// mat_2_norm: one-body parts only, sqrt taken on the device
-int reduce_norm1b(qd_layout* L, const double* a, double* dout) {
-  i64 n1 = (i64)L->n * L->n + (i64)L->mp * L->mp + (i64)L->mp * L->n;
-  int rc = reduce_to(L, RedDotRange{a, nullptr, L->o_fhh}, n1, 1.0, 0.0, dout);
-  if (rc) return rc;
-  k_sqrt<<<1, 1, 0, L->stream>>>(dout);
-  ++L->nlaunch;
   QD_CUDA(cudaGetLastError());
   return QD_OK;
 }

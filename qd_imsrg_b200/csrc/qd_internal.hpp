@@ -202,15 +202,14 @@ i64 part_count(const qd_layout* L, int part);  // total elements of a part over 
 
 // kernels (kernels_*.cu)
 int launch_axpy(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, i64 n);
-int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, int full,
+int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c,
                       double* dout2);
 int reduce_dot_range(qd_layout* L, const double* a, const double* b, i64 o, i64 n, double scale, double add,
                      double* dout);
 int reduce_dot_part(qd_layout* L, const double* a, const double* b, int part, double scale, double add, double* dout);
 int reduce_mbpt2(qd_layout* L, const double* h, double* dout);
 int reduce_hhtrace(qd_layout* L, const double* h, double* dout);
-int reduce_norm1b(qd_layout* L, const double* a, double* dout);
-int reduce_norm_full(qd_layout* L, const double* a, double* dout);
+int reduce_norm(qd_layout* L, const double* a, double* dout);
 double* red_slot(qd_layout* L, int k);
 int launch_white(qd_layout* L, double* gen, const double* h, int herm);
 int launch_keep_parts(qd_layout* L, double* op, unsigned keep);

@@ -135,13 +135,13 @@ class Instance:
 
 
 def trajectory(inst: Instance, nsample: int, rng, max_iter: int = 300):
-    """Run the plain flow (full norm), recording Omega on a fixed subset of
+    """Run the plain flow, recording Omega on a fixed subset of
     entries after every accepted step.  Returns (idx [k], s [steps],
     omega [steps, k], result).  The subset is half uniform, half the entries
     of largest |Omega| at the first step (where the flow does most work)."""
     torch = _torch()
     HS = FullHam(inst.P, 1)
-    f = Flow(inst.H, HS, full_norm=True)
+    f = Flow(inst.H, HS)
     buf = torch.empty(inst.n, dtype=torch.float64, device="cuda")
     snaps, svals, idx = [], [], None
     for _ in range(max_iter + 1):
@@ -218,7 +218,7 @@ def cold_flow(inst: Instance, max_iter: int = 300):
     HS = FullHam(inst.P, 1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    f = Flow(inst.H, HS, full_norm=True)
+    f = Flow(inst.H, HS)
     r = f.run(max_iter)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
@@ -244,7 +244,7 @@ def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300, wi
     t0 = time.perf_counter()
     G = predict_omega(mlp, inst, s_target)
     HS = FullHam(inst.P, 1)
-    f = Flow(inst.H, HS, full_norm=True)
+    f = Flow(inst.H, HS)
     f.warm_start(G, s_target)
     info = f.step()
     crit_warm = float(info.crit)
@@ -264,7 +264,7 @@ def warm_flow(mlp: MLP, inst: Instance, s_target: float, max_iter: int = 300, wi
     else:
         wasted = f.state().commutators
         f.close()
-        f = Flow(inst.H, HS, full_norm=True)
+        f = Flow(inst.H, HS)
         r = f.run(max_iter)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0

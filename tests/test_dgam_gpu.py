@@ -59,6 +59,6 @@ def test_ode_flow_through_dgam():
     # the ODE form flows to the same ground state as the Magnus form
     HS = qd.FullHam(P, 1)
     H.upload(vec)
-    _, res = qd.magnus_flow(H, HS, pandya=True, full_norm=True, max_iter=300)
+    _, res = qd.magnus_flow(H, HS, pandya=True, max_iter=300)
     assert abs(dev.y[0, -1] - res.E0) < 1e-3 * abs(res.E0), (dev.y[0, -1], res.E0)
     assert dev.y[0, -1] < vec[0]  # correlation lowers the HF energy

@@ -25,7 +25,7 @@ def test_flow_graphs_identical(hf6, pandya):
         H, HS = qd.FullHam(P, 1, vec), qd.FullHam(P, 1)
         trs = []
         for _ in range(2):  # the second flow replays the first flow's graphs
-            tr, res = qd.magnus_flow(H, HS, pandya=pandya, full_norm=True, max_iter=200)
+            tr, res = qd.magnus_flow(H, HS, pandya=pandya, max_iter=200)
             trs.append((tr, res.E0, HS.download()))
         out[graphs] = (trs, P.graph_stats())
         for o in (H, HS):

@@ -88,17 +88,19 @@ def test_linearity():
     assert np.abs(C1.get() + C2.get() - C3.get()).max() < 1e-13
 
 
-def test_mat_2_norm_is_one_body_only():
-    # ME_general.f90:2112-2138: the loop over two-body blocks has an empty body
+def test_mat_2_norm_sums_one_and_two_body_parts():
+    # ME_general.f90:2112-2138: fph, fpp, fhh, then per block Vhhhh, Vpppp,
+    # Vpphh, Vphph, Vphhh, Vppph (E0 excluded)
     L, A, B = _ops(6, 4, 15)
     v = B.get()
+    ref = np.sqrt(np.sum(v[1:] ** 2))
+    assert oracle.mat_2_norm(B) == pytest.approx(ref, rel=1e-14)
     n, mp = L.n, L.m - L.n
     nb1 = n * n + mp * mp + mp * n
-    ref = np.sqrt(np.sum(v[1:1 + nb1] ** 2))
-    assert oracle.mat_2_norm(B) == pytest.approx(ref, rel=1e-14)
-    v[1 + nb1:] *= 7.0
+    v[1 + nb1:] *= 7.0   # the two-body parts count
+    v[0] = 123.0         # E0 does not
     B.set(v)
-    assert oracle.mat_2_norm(B) == pytest.approx(ref, rel=1e-14)
+    assert oracle.mat_2_norm(B) == pytest.approx(np.sqrt(np.sum(v[1:] ** 2)), rel=1e-14)
 
 
 def test_bch_with_zero_generator_returns_H():

@@ -103,7 +103,7 @@ def test_config1_flow_split(hf6, slices):
         P = qd.Layout(6, 10, eig=eig)
         P.split = s
         H, HS = qd.FullHam(P, 1, vec), qd.FullHam(P, 1)
-        _, r = qd.magnus_flow(H, HS, pandya=True, full_norm=True, max_iter=200)
+        _, r = qd.magnus_flow(H, HS, pandya=True, max_iter=200)
         res[s] = r.E0
         H.close()
         HS.close()
