@@ -26,9 +26,10 @@ collective (weak scaling); the timed region is bracketed by barriers and the
 max over ranks is reported.
 
 --impl reference: the CPU restatement of the reference (oracle/, OpenMP,
-OpenBLAS dgemm) on the host cores, on a bounded sample of the same workload
-(block-sampled phases of the flow's commutator, scaled to one flow by the
-flow's commutator count; or of the random commutator).
+OpenBLAS dgemm) on the host cores, loading no product library, on a bounded
+sample of the same workload: per step one block-sampled phase of the flow's
+commutator (phases rotate, covering whole commutators), scaled to one flow
+by the FP64 flow's commutator count; or of the random commutator.
 """
 from __future__ import annotations
 
@@ -61,7 +62,6 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-stride", type=int, default=8)
-    ap.add_argument("--cpu-phases", type=int, default=2, help="block-sampled phases timed for the CPU baseline")
     ap.add_argument("--batch-max-iter", type=int, default=300, help="batch: flow step limit per instance")
     ap.add_argument("--ws-train", type=int, default=64, help="warmstart: training draws")
     ap.add_argument("--ws-eval", type=int, default=16, help="warmstart: held-out draws at N=20, R=20")
@@ -308,19 +308,66 @@ def cpu_baseline_full(a: np.ndarray, b: np.ndarray, flops_total: float) -> dict:
 
 
 # --------------------------------------------------------------------------
+class _OracleLayoutView:
+    """The attributes qd_imsrg_b200.flops reads, from an oracle.Layout (the
+    reference arm loads no product library)."""
+
+    def __init__(self, O):
+        self.nbody, self.msp, self.nblock, self.dims, self.emax = O.n, O.m, O.nblock, O.dims, O.emax
+        self.ccn, self.cc_r, self.cc_nb = O.ccn, O.cc_r, O.cc_nb
+
+
+def oracle_operator(O, herm: int, rng, parts=None, sigma: float = 0.1) -> np.ndarray:
+    """Seeded operator in vectorize order for an oracle.Layout, generated with
+    numpy: entries N(0, sigma^2), diagonal-class blocks (fhh, fpp, Vhhhh,
+    Vpppp, Vphph) made (X + herm X^T)/2, one-body entries that change (m_l, m_s)
+    zeroed, E0 = 0.  parts: names of the parts kept non-zero (default all)."""
+    v = rng.normal(0.0, sigma, O.neq)
+    v[0] = 0.0
+    n, m = O.n, O.m
+    mp = m - n
+    g = O.qn[:, 1] * 10 + O.qn[:, 2]
+    keep = set(parts) if parts is not None else None
+
+    def put(name, o, rows, cols, sym, gr=None, gc=None):
+        X = v[o:o + rows * cols].reshape(rows, cols, order="F")
+        if keep is not None and name not in keep:
+            X[:] = 0.0
+        else:
+            if sym:
+                X[:] = (X + herm * X.T) / 2
+            if gr is not None:
+                X[gr[:, None] != gc[None, :]] = 0.0
+        v[o:o + rows * cols] = X.reshape(-1, order="F")
+
+    o = 1
+    put("fhh", o, n, n, True, g[:n], g[:n]); o += n * n
+    put("fpp", o, mp, mp, True, g[n:], g[n:]); o += mp * mp
+    put("fph", o, mp, n, False, g[n:], g[:n])
+    names = ["Vhhhh", "Vpppp", "Vpphh", "Vphph", "Vppph", "Vphhh"]
+    for q in range(O.nblock):
+        nh, nb, npp = (int(x) for x in O.dims[q, :3])
+        shapes = [(nh, nh, True), (npp, npp, True), (npp, nh, False), (nb, nb, True), (npp, nb, False),
+                  (nb, nh, False)]
+        for k, (r, c, sym) in enumerate(shapes):
+            if r * c:
+                put(names[k], int(O.offs[q, k]), r, c, sym)
+    return v
+
+
 def run_reference(args, world, rank):
-    """Reference arm: the CPU restatement on the host cores, block-sampled."""
+    """Reference arm of the commutator workload: the oracle on the host
+    cores, one block-sampled phase of [Omega, H] per step."""
     if rank != 0:
         return 0
     import oracle
-    import qd_imsrg_b200 as qd
     from qd_imsrg_b200.flops import commutator_flops
 
-    P = qd.Layout(args.nbody, args.emax, device=qd.HOST_ONLY)
-    a = qd.random_operator(P, -1, SEED_OMEGA)
-    b = qd.random_operator(P, 1, SEED_H)
-    fl = sample_flops(P, args.ref_stride)
     O = oracle.Layout(args.nbody, args.emax)
+    rng = np.random.default_rng(SEED_H)
+    b = oracle_operator(O, 1, rng)
+    a = oracle_operator(O, -1, rng)
+    fl = sample_flops(_OracleLayoutView(O), args.ref_stride)
     A, B, Cop = oracle.Op(O, -1, a), oracle.Op(O, 1, b), oracle.Op(O, 1)
     S = oracle.Sampler(A)
     stride = args.ref_stride
@@ -337,11 +384,11 @@ def run_reference(args, world, rank):
         t += time.perf_counter() - t0
         done += fl[ph]
     val = done / t / 1e12
-    total = commutator_flops(P)["total"]
+    total = commutator_flops(_OracleLayoutView(O))["total"]
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Philox operators)",
+            "data": "synthetic (seeded numpy operators)",
             "config": {"workload": "FP64 [Omega,H] N=%d R=%d, Pandya on; reference arm: CPU restatement"
                                    % (args.nbody, args.emax), "block_stride": stride,
                        "flops_per_commutator": total},
@@ -418,11 +465,11 @@ def flow_input(args, nbody=None, emax=None, hw=None):
 
 
 def cpu_flow_estimate(vec, eig, args, commutators: int) -> dict:
-    """The oracle on the host cores on a bounded sample of the flow: phases
-    0..p-1 (of `ref_stride`) of the flow's first BCH commutator [Omega, H],
-    Omega = 0.7 eta(H).  Phase 0 carries E0 and the one-body parts plus its
-    blocks; seconds per commutator = t0 + (stride - 1) * mean(t1..),
-    seconds per E_gs = that times the flow's commutator count."""
+    """The oracle on the host cores on one whole commutator of the flow: the
+    flow's first BCH commutator [Omega, H], Omega = 0.7 eta(H_HF), run as the
+    `ref_stride` block-sampled phases back to back (together exactly one
+    commutator); seconds per E_gs = its time times the flow's commutator
+    count (an extrapolation: the whole CPU flow would take about an hour)."""
     import oracle
 
     O = oracle.Layout(args.nbody, args.emax, eig=eig)
@@ -433,19 +480,17 @@ def cpu_flow_estimate(vec, eig, args, commutators: int) -> dict:
     oracle.add_arrays(G, 1.0, eta, float(np.float32(0.7)), G)
     C = oracle.Op(O, 1)
     S = oracle.Sampler(G)
-    stride, phases = args.ref_stride, max(2, min(args.cpu_phases, args.ref_stride))
-    ts = []
-    for ph in range(phases):
-        t0 = time.perf_counter()
+    stride = args.ref_stride
+    t0 = time.perf_counter()
+    for ph in range(stride):
         S.run(G, H, C, stride, ph, pandya=args.pandya)
-        ts.append(time.perf_counter() - t0)
-    per_comm = ts[0] + (stride - 1) * (sum(ts[1:]) / (len(ts) - 1))
+    per_comm = time.perf_counter() - t0
     return {"value": per_comm * commutators, "unit": "s per converged E_gs", "cores": oracle.get_threads(),
             "kind": "port", "seconds_per_commutator": per_comm, "commutators": commutators,
-            "sample": "phases 0..%d of %d block-sampled phases of the flow's first commutator [Omega, H] "
-                      "(Omega = 0.7 eta(H_HF)) timed on the oracle (OpenMP, OpenBLAS); seconds per "
-                      "commutator extrapolated from them, times the flow's %d commutators" %
-                      (phases - 1, stride, commutators)}
+            "sample": "one whole commutator [Omega, H] of the flow (Omega = 0.7 eta(H_HF), its %d block "
+                      "phases back to back) timed on the oracle (OpenMP, OpenBLAS); seconds per E_gs "
+                      "extrapolated: that time x the %d commutators of this run's FP64 GPU flow" %
+                      (stride, commutators)}
 
 
 def flow_desc(args):
@@ -737,36 +782,69 @@ def run_warmstart(args, world, rank, local):
 
 
 def run_reference_flow(args, world, rank):
-    """Reference arm of the flow workload: the oracle on the host cores, per
-    step a bounded sample (block-sampled phases of the flow's commutator),
-    reported as seconds per converged E_gs."""
+    """Reference arm of the flow workload: the oracle (the CPU restatement of
+    the reference) on the host cores, loading no product library.  One step
+    = one block-sampled phase of the flow's commutator [Omega, H]; phases
+    rotate, so the steps cover whole commutators.  Operands: seeded numpy
+    operators with the zero-part pattern of the flow's commutators (Omega:
+    fph and Vpphh only, the White generator's parts; H: every part).  The
+    oracle's work is fixed by the block structure and by which parts are
+    zero, not by the values, so this is the cost of the flow's commutator.
+    Seconds per converged E_gs = seconds per commutator (the sum of the
+    phases' mean times) x the FP64 flow's commutator count at this
+    configuration (an extrapolation, labelled as such)."""
     if rank != 0:
         return 0
-    key = (args.nbody, args.emax, args.hw, bool(args.pandya))
-    vec, eig, hf_it, setup_s = flow_input(args)
-    if key in FLOW_COMMUTATORS:
-        comms, how = FLOW_COMMUTATORS[key], "the FP64 flow's commutator count at this configuration"
-    else:  # small bases: the whole CPU flow runs; count its commutators
-        import oracle
+    import oracle
 
-        O = oracle.Layout(args.nbody, args.emax, eig=eig)
-        tr, _ = oracle.magnus_flow(oracle.Op(O, 1, vec), oracle.Op(O, 1), pandya=args.pandya, max_iter=1000)
-        comms, how = int(np.abs(tr[:, 6]).sum()), "counted by running the CPU flow"
-    vals = []
+    key = (args.nbody, args.emax, args.hw, bool(args.pandya))
+    comms = FLOW_COMMUTATORS.get(key)
+    t_setup = time.perf_counter()
+    O = oracle.Layout(args.nbody, args.emax)
+    rng = np.random.default_rng(SEED_H)
+    h = oracle_operator(O, 1, rng)
+    g = oracle_operator(O, -1, rng, parts=("fph", "Vpphh"))
+    G, H, Cop = oracle.Op(O, -1, g), oracle.Op(O, 1, h), oracle.Op(O, 1)
+    del g, h
+    S = oracle.Sampler(G)
+    stride = args.ref_stride
+    setup_s = time.perf_counter() - t_setup
+    times = {}
     for k in range(args.warmup + args.steps):
-        est = cpu_flow_estimate(vec, eig, args, comms)
+        ph = k % stride
+        t0 = time.perf_counter()
+        S.run(G, H, Cop, stride, ph, pandya=args.pandya)
+        dt = time.perf_counter() - t0
         if k >= args.warmup:
-            vals.append(est)
-    val = statistics.median([e["value"] for e in vals])
-    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "s per converged E_gs", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * val, "higher_is_better": False,
+            times.setdefault(ph, []).append(dt)
+    mean = {p: statistics.mean(v) for p, v in times.items()}
+    covered = len(mean) == stride
+    per_comm = sum(mean.values()) if covered else sum(mean.values()) * stride / max(1, len(mean))
+    timed = sum(len(v) for v in times.values())
+    ms_step = 1e3 * sum(sum(v) for v in times.values()) / max(1, timed)
+    if comms is not None:
+        val, unit = per_comm * comms, "s per converged E_gs"
+        how = ("extrapolation: seconds per commutator x %d, the commutator count of the FP64 flow at this "
+               "configuration (measured on the GPU engine, which matches the oracle flow's count at every "
+               "size where both run)" % comms)
+    else:
+        val, unit, how = per_comm, "s per commutator", "no flow commutator count for this configuration"
+    sample = ("per step one of the %d block-sampled phases of [Omega, H] (phases rotate; all %d timed %s), "
+              "N=%d R=%d, seeded numpy operators with the flow's zero-part pattern; seconds per commutator = "
+              "sum of the phases' mean times = %.3f s" % (stride, stride, "and averaged" if covered else
+                                                          "not all covered: scaled by the phase count",
+                                                          args.nbody, args.emax, per_comm))
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
-            "config": {"workload": flow_desc(args) + "; reference arm: CPU restatement", "commutators": comms,
-                       "commutator_count": how, "hf_setup_s": setup_s},
-            "cpu_baseline": {"value": val, "unit": "s per converged E_gs", "cores": vals[-1]["cores"],
-                             "kind": "port", "sample": vals[-1]["sample"]},
-            "e2e": {"value": val, "unit": "s per converged E_gs", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic: seeded numpy operators with the zero-part pattern of the flow's commutators",
+            "config": {"workload": flow_desc(args) + "; reference arm: CPU restatement (oracle), whole "
+                                                     "commutators in rotating block phases",
+                       "seconds_per_commutator": per_comm, "commutators": comms, "extrapolation": how,
+                       "phases_covered": sorted(mean), "setup_s": setup_s},
+            "cpu_baseline": {"value": val, "unit": unit, "cores": oracle.get_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
