@@ -105,6 +105,12 @@ int qd_layout_profile(qd_layout* L, int enable);
 int qd_layout_profile_read(qd_layout* L, double* ms, int64_t* counts, int nstage);
 /* number of kernels this library has launched for the layout so far        */
 int qd_layout_launches(const qd_layout* L, int64_t* n);
+/* The autotuner's choices so far, as text: the first commutator_122 launch
+ * for each pair of zero-part masks times every launch bucket with 128- and
+ * 256-thread CTAs and keeps the faster (results do not depend on it).
+ * Writes at most len bytes (NUL-terminated) into buf; *needed = full size.
+ * No reference counterpart.                                                 */
+int qd_layout_tuning(const qd_layout* L, char* buf, int64_t len, int64_t* needed);
 
 /* ---- operators: allocate_everything / vectorize / repackage ---------------
  * Replaces src/IMSRG_tools.f90:465-537 (allocate_everything: zero-filled,

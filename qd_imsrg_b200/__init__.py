@@ -126,6 +126,14 @@ class Layout:
         check(lib().qd_layout_launches(self.h, C.byref(n)))
         return n.value
 
+    def tuning(self) -> str:
+        """The autotuner's per-bucket timings and choices (text)."""
+        need = C.c_int64()
+        check(lib().qd_layout_tuning(self.h, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(max(1, need.value))
+        check(lib().qd_layout_tuning(self.h, buf, need.value, C.byref(need)))
+        return buf.value.decode()
+
     def workspace_bytes(self) -> int:
         b = C.c_int64()
         check(lib().qd_layout_workspace_bytes(self.h, C.byref(b)))

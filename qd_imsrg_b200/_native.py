@@ -82,6 +82,7 @@ SIGNATURES = {
     "qd_set_to_zero": (C.c_int, [_vp]),
     "qd_mat_2_norm": (C.c_int, [_vp, _dp]),
     "qd_mat_2_norm_noalloc": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "qd_layout_tuning": (C.c_int, [_vp, C.c_char_p, _i64, _ip64]),
     "qd_commutator_110": (C.c_int, [_vp, _vp, _dp]),
     "qd_commutator_220": (C.c_int, [_vp, _vp, _dp]),
     "qd_commutator_111": (C.c_int, [_vp, _vp, _vp]),

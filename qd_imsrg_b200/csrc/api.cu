@@ -312,6 +312,23 @@ void drop_ws(const qd_layout* L) {
   op_free(w.eomt);
 }
 
+}  // namespace
+
+// A workspace operator of the layout that the full commutator never reads
+// or writes (the reference's w1/w2, which the fused 221 replaces), for the
+// autotuner's timed launches; NULL if none is allocated yet.
+double* qd::scratch_operator(qd_layout* L) {
+  std::lock_guard<std::mutex> lock(g_ws_mutex);
+  auto it = workspaces().find(L);
+  if (it == workspaces().end()) return nullptr;
+  const Workspace& w = it->second;
+  for (qd_op* o : {w.w1, w.w2, w.flow[9], w.flow[10]})
+    if (o) return o->d;
+  return nullptr;
+}
+
+namespace {
+
 const double kCof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666, 0.0083333333333333333,
                          .001388888888888, 1.984126984e-4, 2.48015873e-5, 2.755731922e-6, 2.755731922e-7,
                          2.505210839e-8};
@@ -509,6 +526,18 @@ int qd_layout_profile_read(qd_layout* L, double* ms, int64_t* counts, int nstage
   for (int s = 0; s < nstage && s < S_COUNT; ++s) {
     if (ms) ms[s] = L->prof.ms[s];
     if (counts) counts[s] = L->prof.count[s];
+  }
+  return QD_OK;
+}
+
+int qd_layout_tuning(const qd_layout* L, char* buf, int64_t len, int64_t* needed) {
+  CHECK(L, QD_ERR_ARG, "null layout");
+  const std::string r = tuning_report_122(L);
+  if (needed) *needed = (int64_t)r.size() + 1;
+  if (buf && len > 0) {
+    const size_t n = std::min<size_t>((size_t)len - 1, r.size());
+    std::memcpy(buf, r.data(), n);
+    buf[n] = 0;
   }
   return QD_OK;
 }
@@ -856,7 +885,7 @@ struct TermGraph {
 using TermGraphs = std::map<TermKey, TermGraph>;
 
 int bch_term(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd_op* w1, qd_op* w2, qd_cc* HCC,
-             qd_cc* OCC, bool pandya, double cof) {
+             qd_cc* OCC, bool pandya, double cof, const int* kidx = nullptr) {
   if (pandya) {
     TRY(commutator_seq(L, G, AD, INT2, w1, w2, OCC, HCC, true));
   } else {
@@ -864,9 +893,10 @@ int bch_term(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, qd_op* HS, qd
   }
   {
     StageTimer tm(L, S_GLUE);
-    TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, red_slot(L, 1)));
+    TRY(launch_axpy_norms(L, HS->d, 1.0, INT2->d, cof, HS->d, red_slot(L, 1), kidx));
   }
-  QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+  if (!kidx)  // host decides: copy both norms back
+    QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
   return QD_OK;
 }
 }  // namespace
@@ -935,6 +965,216 @@ static int bch_term_graph(qd_layout* L, const qd_op* G, qd_op* AD, qd_op* INT2, 
   return QD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// ---- a whole BCH_EXPAND as one CUDA graph --------------------------------
+// The exit test runs on the device (k_bch_decide), so the term loop is a
+// graph "while" node and a BCH step needs one host synchronisation (for the
+// term count) instead of one per term.  Layout of the graph:
+//   prologue: HS = H; AD = H; INT2 = [G, AD]; HS += cof(1) INT2; decide
+//   while (go): INT2' = [G, INT2]; HS += cof INT2'; decide (sets go, more)
+//               if (more): INT2 = [G, INT2']; HS += cof INT2; decide (sets go)
+// The two buffers of INT2 and AD alternate between the two halves of the
+// loop body, so no operator is copied.  The term coefficient comes from a
+// device counter (the number of terms so far), which the host reads back.
+// Built like the per-term graphs: a key seen once runs eagerly (which builds
+// every plan and workspace), the second time it is captured; a capture that
+// fails leaves the key eager.
+struct StepKey {
+  const void* p[9];  // G, HS, H, INT2, AD, w1, w2, OCC, HCC data
+  unsigned mg, mh;
+  int gh, hh, flags, split;
+  bool operator<(const StepKey& o) const { return std::memcmp(this, &o, sizeof(StepKey)) < 0; }
+};
+struct StepGraph {
+  int seen = 0;
+  bool failed = false;
+  cudaGraphExec_t exec = nullptr;
+  long long first = 0, per_term = 0;  // launches of the prologue and of one later term
+};
+using StepGraphs = std::map<StepKey, StepGraph>;
+
+int* bch_counter(qd_layout* L) { return reinterpret_cast<int*>(red_slot(L, 16)); }
+
+// A conditional node of `type` on handle h after the current dependencies of
+// a stream capturing into graph g; *body receives its body graph.
+int add_conditional(cudaStream_t st, cudaGraph_t g, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  QD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};  // aggregate: the rest zero
+  cp.conditional.handle = h;
+  cp.conditional.type = type;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  QD_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+  QD_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  *body = cp.conditional.phGraph_out[0];
+  return QD_OK;
+}
+
+// Capture the step graph: P (INT2's buffer) and Q (AD's buffer) alternate.
+int capture_step(qd_layout* L, qd_op* HS, const qd_op* G, const qd_op* H, double* P, double* Q, qd_op* w1,
+                 qd_op* w2, qd_cc* HCC, qd_cc* OCC, bool pandya, cudaGraphExec_t* exec, long long* first,
+                 long long* per_term) {
+  const double conv = (double)1e-5f;
+  int* k = bch_counter(L);
+  cudaStream_t st = L->stream;
+  qd_op ad = *H, out = *H;  // host views of the two buffers (herm +1, as BCH_EXPAND sets)
+  ad.herm = out.herm = 1;
+  cudaGraph_t g = nullptr;
+  QD_CUDA(cudaGraphCreate(&g, 0));
+  int rc = QD_OK;
+  cudaGraph_t body = nullptr, body2 = nullptr, cap = nullptr;
+  cudaGraphConditionalHandle hloop, hmore;
+  const long long n0 = L->nlaunch;
+  do {
+    if (cudaGraphConditionalHandleCreate(&hloop, g, 0, 0) != cudaSuccess) { rc = QD_ERR_CUDA; break; }
+    if (cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      rc = QD_ERR_CUDA;
+      break;
+    }
+    // prologue: HS = H, AD = H (Q), term 1 into P
+    int r2 = QD_OK;
+    if (cudaMemsetAsync(k, 0, sizeof(int), st) != cudaSuccess ||
+        cudaMemcpyAsync(HS->d, H->d, sizeof(double) * L->neq, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(Q, H->d, sizeof(double) * L->neq, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      r2 = QD_ERR_CUDA;
+    ad.d = Q;
+    ad.zero_mask = H->zero_mask;
+    out.d = P;
+    HS->zero_mask = H->zero_mask;
+    if (!r2) r2 = bch_term(L, G, &ad, &out, HS, w1, w2, HCC, OCC, pandya, 0.0, k);
+    if (!r2) r2 = launch_bch_decide(L, red_slot(L, 1), k, conv, hloop, hloop, 0);
+    *first = L->nlaunch - n0;
+    if (!r2) r2 = add_conditional(st, g, hloop, cudaGraphCondTypeWhile, &body);
+    if (cudaStreamEndCapture(st, &cap) != cudaSuccess || r2) {
+      rc = r2 ? r2 : QD_ERR_CUDA;
+      break;
+    }
+    // loop body, first half: AD = P, INT2 = Q; then "more" guards the second half
+    if (cudaGraphConditionalHandleCreate(&hmore, body, 0, 0) != cudaSuccess ||
+        cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      rc = QD_ERR_CUDA;
+      break;
+    }
+    const long long n1 = L->nlaunch;
+    ad.d = P;
+    ad.zero_mask = 0;
+    out.d = Q;
+    r2 = bch_term(L, G, &ad, &out, HS, w1, w2, HCC, OCC, pandya, 0.0, k);
+    if (!r2) r2 = launch_bch_decide(L, red_slot(L, 1), k, conv, hloop, hmore, 1);
+    *per_term = L->nlaunch - n1;
+    if (!r2) r2 = add_conditional(st, body, hmore, cudaGraphCondTypeIf, &body2);
+    if (cudaStreamEndCapture(st, &cap) != cudaSuccess || r2) {
+      rc = r2 ? r2 : QD_ERR_CUDA;
+      break;
+    }
+    // second half: AD = Q, INT2 = P
+    if (cudaStreamBeginCaptureToGraph(st, body2, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess) {
+      rc = QD_ERR_CUDA;
+      break;
+    }
+    ad.d = Q;
+    out.d = P;
+    r2 = bch_term(L, G, &ad, &out, HS, w1, w2, HCC, OCC, pandya, 0.0, k);
+    if (!r2) r2 = launch_bch_decide(L, red_slot(L, 1), k, conv, hloop, hloop, 0);
+    if (cudaStreamEndCapture(st, &cap) != cudaSuccess || r2) {
+      rc = r2 ? r2 : QD_ERR_CUDA;
+      break;
+    }
+    if (cudaGraphInstantiate(exec, g, 0) != cudaSuccess) rc = QD_ERR_CUDA;
+  } while (false);
+  if (rc) {  // leave no capture open and no error pending
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(st, &junk);
+      if (junk) cudaGraphDestroy(junk);
+    }
+    (void)cudaGetLastError();
+    *exec = nullptr;
+  }
+  cudaGraphDestroy(g);
+  L->nlaunch = n0;
+  return rc;
+}
+
+// The eager BCH_EXPAND loop (per-term graphs where enabled).
+int bch_eager(qd_layout* L, qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT2, qd_op* AD, qd_op* w1, qd_op* w2,
+              qd_cc* HCC, qd_cc* OCC, bool pandya, int* nterms);
+
+// Whole step as a graph when possible; *done = false leaves it to the caller.
+int bch_step_graph(qd_layout* L, qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT2, qd_op* AD, qd_op* w1,
+                   qd_op* w2, qd_cc* HCC, qd_cc* OCC, bool pandya, int* nterms, bool* done) {
+  *done = false;
+  if (!L->use_graphs || L->prof.on || L->split_slices > 0) return QD_OK;
+  if (!L->step_graphs) L->step_graphs = new StepGraphs();
+  StepKey key;
+  std::memset(&key, 0, sizeof(key));
+  const void* ptrs[9] = {G->d, HS->d, H->d, INT2->d, AD->d, w1->d, w2->d, OCC ? OCC->d : nullptr,
+                         HCC ? HCC->d : nullptr};
+  for (int i = 0; i < 9; ++i) key.p[i] = ptrs[i];
+  key.mg = G->zero_mask;
+  key.mh = H->zero_mask;
+  key.gh = G->herm;
+  key.hh = H->herm;
+  key.flags = pandya ? 1 : 0;
+  key.split = L->split_slices;
+  StepGraph& sg = (*reinterpret_cast<StepGraphs*>(L->step_graphs))[key];
+  double* P = INT2->d;
+  double* Q = AD->d;
+  if (!sg.exec) {
+    if (sg.failed || sg.seen++ == 0) return QD_OK;  // eager (first sight builds plans for H's masks)
+    // plans and task lists of the later terms ([G, X] with X a full operator)
+    qd_op full = *H;  // H as a full operator: the masks of AD in the later terms
+    full.zero_mask = 0;
+    TRY(prepare_program(L, L->prog_ladder, G->zero_mask, 0u));
+    TRY(prepare_program(L, L->prog_111, G->zero_mask, 0u));
+    TRY(prepare_program(L, L->prog_pandya, 0u, 0u));
+    TRY(prepare_122(L, G, &full));
+    TRY(prepare_program(L, L->prog_ladder, G->zero_mask, H->zero_mask));
+    TRY(prepare_program(L, L->prog_111, G->zero_mask, H->zero_mask));
+    TRY(prepare_122(L, G, H));
+    if (pandya) TRY(ensure_z(L));
+    QD_CUDA(cudaStreamSynchronize(L->stream));
+    if (capture_step(L, HS, G, H, P, Q, w1, w2, HCC, OCC, pandya, &sg.exec, &sg.first, &sg.per_term)) {
+      sg.failed = true;
+      return QD_OK;
+    }
+    ++L->graphs_captured;
+  }
+  QD_CUDA(cudaGraphLaunch(sg.exec, L->stream));
+  int* hk = reinterpret_cast<int*>(L->h_red + 16);
+  QD_CUDA(cudaMemcpyAsync(hk, bch_counter(L), sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+  QD_CUDA(cudaStreamSynchronize(L->stream));
+  const int terms = *hk;
+  L->nlaunch += sg.first + sg.per_term * (terms - 1);
+  ++L->graph_replays;
+  // host-side state the eager loop leaves: HS and the workspaces hold full
+  // operators; the two workspace buffers keep their handles
+  HS->zero_mask = 0;
+  INT2->zero_mask = 0;
+  AD->zero_mask = 0;
+  if (pandya) {
+    OCC->filled = true;
+    OCC->herm = G->herm;
+    HCC->filled = true;
+    HCC->herm = 1;
+  }
+  *nterms = terms;
+  *done = true;
+  return QD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op* INT2, qd_op* AD, qd_op* w1,
                   qd_op* w2, qd_cc* HCC, qd_cc* OCC, unsigned flags, int* nterms) {
   TRY(same_layout(HS, G));
@@ -949,9 +1189,23 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
   TRY(build_programs(L));
   const bool pandya = (flags & QD_PANDYA) != 0;
   CHECK(!pandya || (HCC && OCC), QD_ERR_ARG, "qd_bch_expand: QD_PANDYA needs HCC and OCC");
-  const double conv = (double)1e-5f;  // "conv = 1e-5" is a real(4) literal in the reference
   INT2->herm = 1;
   AD->herm = 1;
+  bool done = false;
+  int count = 0;
+  TRY(bch_step_graph(L, HS, G, H, INT2, AD, w1, w2, HCC, OCC, pandya, &count, &done));
+  if (!done) TRY(bch_eager(L, HS, G, H, INT2, AD, w1, w2, HCC, OCC, pandya, &count));
+  if (nterms) *nterms = count;
+  return QD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int bch_eager(qd_layout* L, qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT2, qd_op* AD, qd_op* w1, qd_op* w2,
+              qd_cc* HCC, qd_cc* OCC, bool pandya, int* nterms) {
+  const double conv = (double)1e-5f;  // "conv = 1e-5" is a real(4) literal in the reference
+  double* const p0 = INT2->d;
   TRY(qd_copy_arrays(H, HS));
   TRY(qd_copy_arrays(HS, INT2));
   int count = 0;
@@ -966,9 +1220,16 @@ int qd_bch_expand(qd_op* HS, const qd_op* G, const qd_op* H, qd_op* INT1, qd_op*
     const double n1 = L->h_red[1], n2 = L->h_red[2];
     if (n2 * cof / n1 < conv) break;
   }
+  if (INT2->d != p0) {  // the workspaces keep their buffers (contents unspecified)
+    std::swap(INT2->d, AD->d);
+    std::swap(INT2->zero_mask, AD->zero_mask);
+  }
   if (nterms) *nterms = count;
   return QD_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int qd_magnus_expand(qd_op* DG, const qd_op* G, const qd_op* ETA) {
   (void)G;
@@ -988,6 +1249,7 @@ struct qd_flow {
   qd_layout* L = nullptr;
   const qd_op* HAM = nullptr;
   qd_op* HS = nullptr;
+  double* hs_home = nullptr;  // the caller's HS buffer (HS and HS0 trade buffers during the flow)
   unsigned flags = 0;
   qd_op *ETA = nullptr, *G = nullptr, *DG = nullptr, *ETA0 = nullptr, *G0 = nullptr, *HS0 = nullptr;
   qd_op *INT1 = nullptr, *INT2 = nullptr, *AD = nullptr, *w1 = nullptr, *w2 = nullptr;
@@ -1001,6 +1263,22 @@ namespace {
 const double kConvCriteria = (double)1e-9f;  // real(4) literal in the reference
 
 int flow_eta_norm(qd_flow* f, const qd_op* op, double* out) { return qd_mat_2_norm(op, out); }
+
+// Operators of one role pair (G/G0, HS/HS0, ETA/ETA0) trade buffers instead
+// of copying: "G0 = G" becomes a swap after which G's buffer is rewritten.
+void swap_ops(qd_op* a, qd_op* b) {
+  std::swap(a->d, b->d);
+  std::swap(a->zero_mask, b->zero_mask);
+}
+
+// Give the caller's HS its own buffer back (copying the current contents).
+int flow_home_hs(qd_flow* f) {
+  if (f->HS->d == f->hs_home) return QD_OK;
+  QD_CUDA(cudaMemcpyAsync(f->hs_home, f->HS->d, sizeof(double) * f->L->neq, cudaMemcpyDeviceToDevice, f->L->stream));
+  swap_ops(f->HS, f->HS0);  // HS0 held hs_home: after the swap HS->d == hs_home again
+  f->HS0->zero_mask = f->HS->zero_mask;
+  return QD_OK;
+}
 
 int flow_e0(qd_flow* f, double* e0) {
   qd_layout* L = f->L;
@@ -1046,9 +1324,12 @@ int qd_flow_create(const qd_op* HAM, qd_op* HS, unsigned flags, qd_flow** out) {
   f->HCC->herm = 1.0;
   f->OCC->herm = -1.0;
   f->HCC->filled = f->OCC->filled = false;  // run_magnus never fills them (the Pandya option does, per commutator)
+  f->hs_home = HS->d;
   int rc = QD_OK;
-  // the generator and the Magnus operator start from zero (allocate_everything)
-  for (qd_op* z : {f->ETA, f->G}) {
+  // the generator and the Magnus operator start from zero (allocate_everything);
+  // ETA0 too, as ETA and ETA0 trade buffers and build_white writes only fph
+  // and Vpphh
+  for (qd_op* z : {f->ETA, f->ETA0, f->G}) {
     if (cudaMemsetAsync(z->d, 0, sizeof(double) * L->neq, L->stream) != cudaSuccess) rc = QD_ERR_CUDA;
     z->zero_mask = ALL_PARTS;
   }
@@ -1102,14 +1383,17 @@ int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
     if (info) *info = inf;
     return QD_OK;
   }
-  TRY(qd_copy_arrays(f->G, f->G0));
-  TRY(qd_magnus_expand(f->DG, f->G, f->ETA));
-  TRY(qd_euler_step(f->G, f->DG, &f->s, f->stp));
-  TRY(qd_copy_arrays(f->HS, f->HS0));
+  // G0 = G; MAGNUS_EXPAND: DG = ETA; euler_step: G = G + stp DG.  G and G0
+  // trade buffers and G = 1 G0 + stp ETA is written in one pass (the same
+  // arithmetic as add_arrays(G, 1, DG, stp, G) with DG = ETA).
+  swap_ops(f->G, f->G0);
+  TRY(qd_add_arrays(f->G0, 1.0, f->ETA, f->stp, f->G));
+  f->s = f->s + f->stp;
+  swap_ops(f->HS, f->HS0);  // HS0 = HS: BCH_EXPAND rewrites every entry of HS
   int terms = 0;
   TRY(qd_bch_expand(f->HS, f->G, f->HAM, f->INT1, f->INT2, f->AD, f->w1, f->w2, f->HCC, f->OCC, f->flags, &terms));
   f->comms += terms;
-  TRY(qd_copy_arrays(f->ETA, f->ETA0));
+  swap_ops(f->ETA, f->ETA0);  // ETA0 = ETA: build_white rewrites fph and Vpphh, the rest stays 0
   TRY(qd_build_white(f->ETA, f->HS));
   double nrm2, E0;
   TRY(flow_eta_norm(f, f->ETA, &nrm2));
@@ -1126,9 +1410,9 @@ int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
   if (f->nrm1 * 1.5 < nrm2) {  // reject: back to the previous state, smaller step
     ++f->rejected;
     f->s = f->s - f->stp;
-    TRY(qd_copy_arrays(f->G0, f->G));
-    TRY(qd_copy_arrays(f->HS0, f->HS));
-    TRY(qd_copy_arrays(f->ETA0, f->ETA));
+    swap_ops(f->G, f->G0);
+    swap_ops(f->HS, f->HS0);
+    swap_ops(f->ETA, f->ETA0);
     f->stp = f->stp / 2.0 + (double)1e-3f;
     inf.accepted = 0;
   } else {
@@ -1164,6 +1448,7 @@ int qd_flow_state(const qd_flow* f, qd_flow_result* r) {
 int qd_flow_destroy(qd_flow* f) {
   if (!f) return QD_OK;
   cudaSetDevice(f->L->device);
+  flow_home_hs(f);
   cudaStreamSynchronize(f->L->stream);
   (void)cudaGetLastError();
   delete f;  // the workspaces stay with the layout
@@ -1232,11 +1517,17 @@ int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, u
 
 namespace qd {
 void graphs_free(qd_layout* L) {
-  auto* m = reinterpret_cast<TermGraphs*>(L->graphs);
-  if (!m) return;
-  for (auto& kv : *m)
-    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-  delete m;
-  L->graphs = nullptr;
+  if (auto* m = reinterpret_cast<TermGraphs*>(L->graphs)) {
+    for (auto& kv : *m)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    delete m;
+    L->graphs = nullptr;
+  }
+  if (auto* m = reinterpret_cast<StepGraphs*>(L->step_graphs)) {
+    for (auto& kv : *m)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    delete m;
+    L->step_graphs = nullptr;
+  }
 }
 }  // namespace qd

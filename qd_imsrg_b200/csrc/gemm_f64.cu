@@ -310,6 +310,174 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __re
 }
 
 // ---------------------------------------------------------------------------
+// K-short problems: every active segment together spans K <= KS_K (in the
+// Magnus flow the generator holds only fph and Vpphh, so the pppp and ppph
+// ladders become rank-n_h updates, n_h <= 16).  Such a tile is one read-
+// modify-write of C: no pipeline, the panels of all segments are staged once
+// (alpha folded in), the two products of a pair tile are formed from four
+// panels, and the shared memory is reused for the transpose stash, so that
+// six CTAs of eight warps fit on an SM.
+// ---------------------------------------------------------------------------
+constexpr int KS_K = 16, KS_THREADS = 256, KS_LDS = 68;
+constexpr int KS_PANEL = KS_K * KS_LDS;                            // doubles per panel
+constexpr size_t KS_SMEM = sizeof(double) * (4 * KS_PANEL > BN * TLD ? 4 * KS_PANEL : BN * TLD);
+
+// panel of op(A) rows [row0, row0+64) (sA[k][m]) and op(B) columns
+// [col0, col0+64) (sB[k][n]) over the concatenated active segments; zeros
+// outside M, N and beyond the total K
+__device__ __forceinline__ void ks_panels(const SegList& sl, int M, int N, int row0, int col0, double* sA,
+                                          double* sB) {
+  for (int i = threadIdx.x; i < KS_PANEL; i += KS_THREADS) {
+    sA[i] = 0.0;
+    sB[i] = 0.0;
+  }
+  __syncthreads();
+  int kb = 0;
+  for (int si = 0; si < sl.nact; ++si) {
+    const GSeg& s = sl.seg[si];
+    const double* A = sl.A[si];
+    const double* B = sl.B[si];
+    const double al = sl.alpha[si];
+    for (int e = threadIdx.x; e < s.K * BM; e += KS_THREADS) {
+      // element (m or n fastest when that index is contiguous in memory)
+      int m, k;
+      if (!s.tA) { m = e % BM; k = e / BM; } else { k = e % s.K; m = e / s.K; }
+      if (row0 + m < M) sA[(kb + k) * KS_LDS + m] = al * (s.tA ? A[k + (i64)(row0 + m) * s.lda] : A[(row0 + m) + (i64)k * s.lda]);
+      int n, k2;
+      if (s.tB) { n = e % BN; k2 = e / BN; } else { k2 = e % s.K; n = e / s.K; }
+      if (col0 + n < N) sB[(kb + k2) * KS_LDS + n] = s.tB ? B[(col0 + n) + (i64)k2 * s.ldb] : B[k2 + (i64)(col0 + n) * s.ldb];
+    }
+    kb += s.K;
+  }
+  __syncthreads();
+}
+
+// acc[4][2][2] (warp tile 32 x 16) = sA^T sB over KS_K
+__device__ __forceinline__ void ks_mma(const double* sA, const double* sB, double acc[4][2][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+  for (int kk = 0; kk < KS_K; kk += 4) {
+    const int kr = kk + (lane & 3);
+    double af[4], bf[2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) af[i] = sA[kr * KS_LDS + wm * 32 + i * 8 + (lane >> 2)];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) bf[j] = sB[kr * KS_LDS + wn * 16 + j * 8 + (lane >> 2)];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+  }
+}
+
+__device__ __forceinline__ void ks_stash(double* T, const double acc[4][2][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int r = wm * 32 + i * 8 + (lane >> 2);
+      const int c = wn * 16 + j * 8 + 2 * (lane & 3);
+      T[c * TLD + r] = acc[i][j][0];
+      T[(c + 1) * TLD + r] = acc[i][j][1];
+    }
+}
+
+__global__ void __launch_bounds__(KS_THREADS, 3) k_gemm_kshort(const GTask* __restrict__ tasks,
+                                                            const GProb* __restrict__ probs,
+                                                            const GSeg* __restrict__ segs, Bufs bufs, double hv0,
+                                                            double hv1, unsigned maskA, unsigned maskB) {
+  extern __shared__ double smem[];
+  __shared__ SegList sl;
+  const GTask t = tasks[blockIdx.x];
+  const GProb P = probs[t.prob];
+  double* out = const_cast<double*>(bufs.p[P.outbuf]) + P.offC;
+  if (threadIdx.x == 0) {
+    int na = 0, tot = 0;
+    for (int k = 0; k < P.nseg && na < 8; ++k) {
+      const GSeg sg = segs[P.seg0 + k];
+      if (!seg_active(sg, maskA, maskB) || sg.K <= 0) continue;
+      sl.seg[na] = sg;
+      sl.A[na] = bufs.p[sg.srcA] + sg.offA;
+      sl.B[na] = bufs.p[sg.srcB] + sg.offB;
+      sl.alpha[na] = sg.c * (sg.pa ? hv0 : 1.0) * (sg.pb ? hv1 : 1.0);
+      tot += sg.K;
+      ++na;
+    }
+    sl.nact = na;
+    sl.total = tot;  // <= KS_K (the host routes only such problems here)
+  }
+  __syncthreads();
+  const bool pair = P.mode == GM_ACC_PAIR || P.mode == GM_SET_PAIR;
+  const bool acc_mode = P.mode == GM_ACC || P.mode == GM_ACC_PAIR;
+  const int r0 = t.ti * BM, c0 = t.tj * BN;
+  double* pA1 = smem;
+  double* pB1 = smem + KS_PANEL;
+  double* T = smem;  // stash, after the products
+  double v1[4][2][2], v2[4][2][2];
+  if (!pair || t.ti == t.tj) {
+    ks_panels(sl, P.M, P.N, r0, c0, pA1, pB1);
+    ks_mma(pA1, pB1, v1);
+    __syncthreads();
+    ks_stash(T, v1);
+    __syncthreads();
+    const double sigma = pair ? P.sc * (P.spa ? hv0 : 1.0) * (P.spb ? hv1 : 1.0) : 0.0;
+    const int mr = min(BM, P.M - r0), nc = min(BN, P.N - c0);
+    for (int idx = threadIdx.x; idx < BM * BN; idx += KS_THREADS) {
+      const int r = idx & (BM - 1), c = idx >> 6;
+      if (r < mr && c < nc) {
+        double* p = out + (r0 + r) + (i64)(c0 + c) * P.ldc;
+        const double v = pair ? T[c * TLD + r] + sigma * T[r * TLD + c] : T[c * TLD + r];
+        *p = acc_mode ? *p + v : v;
+      }
+    }
+    return;
+  }
+  // off-diagonal tile pair: V(I,J) = A_I B_J^T and V(J,I) = A_J B_I^T;
+  // C(I,J) = V(I,J) + sigma V(J,I)^T and C(J,I) = V(J,I) + sigma V(I,J)^T,
+  // each formed in the fragment layout against the other product's stash
+  double* pA2 = smem + 2 * KS_PANEL;
+  double* pB2 = smem + 3 * KS_PANEL;
+  ks_panels(sl, P.M, P.N, r0, c0, pA1, pB1);
+  ks_panels(sl, P.M, P.N, c0, r0, pA2, pB2);
+  ks_mma(pA1, pB1, v1);
+  ks_mma(pA2, pB2, v2);
+  __syncthreads();
+  const double sigma = P.sc * (P.spa ? hv0 : 1.0) * (P.spb ? hv1 : 1.0);
+  const int mI = min(BM, P.M - r0), mJ = min(BM, P.M - c0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    ks_stash(T, side == 0 ? v2 : v1);
+    __syncthreads();
+    const double(*v)[2][2] = side == 0 ? v1 : v2;
+    const int rb = side == 0 ? r0 : c0, cb = side == 0 ? c0 : r0;
+    const int mr = side == 0 ? mI : mJ, nc = side == 0 ? mJ : mI;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = wm * 32 + i * 8 + (lane >> 2), c = wn * 16 + j * 8 + 2 * (lane & 3) + e;
+          if (r < mr && c < nc) {
+            double* p = out + (rb + r) + (i64)(cb + c) * P.ldc;
+            const double x = v[i][j][e] + sigma * T[r * TLD + c];
+            *p = acc_mode ? *p + x : x;
+          }
+        }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side: program construction and launch
 // ---------------------------------------------------------------------------
 namespace {
@@ -512,6 +680,7 @@ int build_programs(qd_layout* L) {
       QD_CUDA(cudaMemcpy(P->d_segs, P->segs.data(), P->segs.size() * sizeof(GSeg), cudaMemcpyHostToDevice));
   }
   QD_CUDA(cudaFuncSetAttribute(k_grouped_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
+  QD_CUDA(cudaFuncSetAttribute(k_gemm_kshort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KS_SMEM));
   L->programs_built = true;
   return QD_OK;
 }
@@ -525,27 +694,37 @@ static bool seg_active_host(const GSeg& s, unsigned mA, unsigned mB) {
   return !dead(s.srcA, s.depA) && !dead(s.srcB, s.depB);
 }
 
-// Task list for (maskA, maskB): every tile (tile pair in the pair modes) of
+// Task lists for (maskA, maskB): every tile (tile pair in the pair modes) of
 // every problem that has an active segment (SET problems always: they must
-// write), longest first.
-static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTask** d_tasks, int* ntasks) {
+// write), longest first; problems whose active segments span K <= KS_K
+// (at most 8 of them) in a separate list for the K-short kernel.
+static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTask** d_tasks, int* ntasks,
+                     GTask** d_short, int* nshort) {
   auto key = std::make_pair(mA, mB);
   auto it = P.tasks.find(key);
   if (it != P.tasks.end()) {
     *d_tasks = it->second.first;
     *ntasks = it->second.second;
+    *d_short = P.tasks_short[key].first;
+    *nshort = P.tasks_short[key].second;
     return QD_OK;
   }
-  std::vector<std::pair<double, GTask>> v;
+  std::vector<std::pair<double, GTask>> v[2];
   for (size_t pi = 0; pi < P.probs.size(); ++pi) {
     const GProb& g = P.probs[pi];
     double kt = 0.0;
+    int ksum = 0, nact = 0;
     for (int k = 0; k < g.nseg; ++k) {
       const GSeg& s = P.segs[g.seg0 + k];
-      if (seg_active_host(s, mA, mB)) kt += (s.K + BK - 1) / BK;
+      if (seg_active_host(s, mA, mB) && s.K > 0) {
+        kt += (s.K + BK - 1) / BK;
+        ksum += s.K;
+        ++nact;
+      }
     }
     bool set = g.mode == GM_SET || g.mode == GM_SET_PAIR;
     if (kt == 0.0 && !set) continue;
+    const int which = (ksum <= KS_K && nact <= 8) ? 1 : 0;
     int tm = (g.M + BM - 1) / BM, tn = (g.N + BN - 1) / BN;
     bool pair = g.mode == GM_ACC_PAIR || g.mode == GM_SET_PAIR;
     for (int i = 0; i < tm; ++i)
@@ -555,21 +734,36 @@ static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTa
         t.ti = (short)i;
         t.tj = (short)j;
         double cost = (kt + 1.0) * ((pair && i != j) ? 2.0 : 1.0);
-        v.push_back({cost, t});
+        v[which].push_back({cost, t});
       }
   }
-  std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-  std::vector<GTask> h(v.size());
-  for (size_t i = 0; i < v.size(); ++i) h[i] = v[i].second;
-  GTask* d = nullptr;
-  if (!h.empty()) {
-    QD_CUDA(cudaMalloc(&d, h.size() * sizeof(GTask)));
-    QD_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(GTask), cudaMemcpyHostToDevice));
+  GTask* d[2] = {nullptr, nullptr};
+  for (int w = 0; w < 2; ++w) {
+    std::stable_sort(v[w].begin(), v[w].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<GTask> h(v[w].size());
+    for (size_t i = 0; i < v[w].size(); ++i) h[i] = v[w][i].second;
+    if (!h.empty()) {
+      QD_CUDA(cudaMalloc(&d[w], h.size() * sizeof(GTask)));
+      QD_CUDA(cudaMemcpy(d[w], h.data(), h.size() * sizeof(GTask), cudaMemcpyHostToDevice));
+    }
   }
-  P.tasks[key] = std::make_pair(d, (int)h.size());
-  *d_tasks = d;
-  *ntasks = (int)h.size();
+  P.tasks[key] = std::make_pair(d[0], (int)v[0].size());
+  P.tasks_short[key] = std::make_pair(d[1], (int)v[1].size());
+  *d_tasks = d[0];
+  *ntasks = (int)v[0].size();
+  *d_short = d[1];
+  *nshort = (int)v[1].size();
   return QD_OK;
+}
+
+// Build (allocate and upload) the task lists of P for a pair of zero-part
+// masks ahead of a stream capture, which must not allocate.
+int prepare_program(qd_layout* L, GemmProgram& P, unsigned maskA, unsigned maskB) {
+  int rc = build_programs(L);
+  if (rc) return rc;
+  GTask *d1, *d2;
+  int n1, n2;
+  return get_tasks(L, P, maskA, maskB, &d1, &n1, &d2, &n2);
 }
 
 int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
@@ -577,14 +771,20 @@ int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double 
   int rc = build_programs(L);
   if (rc) return rc;
   if (L->split_slices > 0) return run_program_split(L, P, bufs, hv0, hv1, maskA, maskB);
-  GTask* d_tasks = nullptr;
-  int nt = 0;
-  if ((rc = get_tasks(L, P, maskA, maskB, &d_tasks, &nt))) return rc;
-  if (nt == 0) return QD_OK;
+  GTask *d_tasks = nullptr, *d_short = nullptr;
+  int nt = 0, ns = 0;
+  if ((rc = get_tasks(L, P, maskA, maskB, &d_tasks, &nt, &d_short, &ns))) return rc;
   Bufs b;
   for (int i = 0; i < NBUF; ++i) b.p[i] = bufs[i];
-  k_grouped_gemm<<<nt, GEMM_THREADS, GEMM_SMEM, L->stream>>>(d_tasks, P.d_probs, P.d_segs, b, hv0, hv1, maskA, maskB);
-  ++L->nlaunch;
+  if (nt > 0) {
+    k_grouped_gemm<<<nt, GEMM_THREADS, GEMM_SMEM, L->stream>>>(d_tasks, P.d_probs, P.d_segs, b, hv0, hv1, maskA,
+                                                                maskB);
+    ++L->nlaunch;
+  }
+  if (ns > 0) {
+    k_gemm_kshort<<<ns, KS_THREADS, KS_SMEM, L->stream>>>(d_short, P.d_probs, P.d_segs, b, hv0, hv1, maskA, maskB);
+    ++L->nlaunch;
+  }
   QD_CUDA(cudaGetLastError());
   return QD_OK;
 }

@@ -1,11 +1,9 @@
-// kernels_122.cu -- commutator_122 (src/commutators.f90:355-676) as two
-// shared-memory-staged passes per (M_L,M_S) block, evaluated group pair by
-// group pair as small dense products.
+// kernels_122.cu -- commutator_122 (src/commutators.f90:355-676) as one pass
+// over independent group-pair tiles.
 //
-// In block q the pairs are ordered [hh | ph | pp] (block-local index P); the
-// full block matrix V(P1,P2) holds the stored classes (class(P1) >=
-// class(P2)) and herm * their transposes above.  For the stored output
-// element <b1 b2|k1 k2> = C(P1,P2):
+// In block q the pairs are ordered [hh | ph | pp]; the full block matrix
+// V(P1,P2) holds the stored classes (class(P1) >= class(P2)) and herm * their
+// transposes above.  For the stored output element <b1 b2|k1 k2> = C(P1,P2):
 //   bra legs: C += sum_{t in G(b1)} [FA(b1,t) VB(t b2|P2) - FB(b1,t) VA(t b2|P2)]
 //                + sum_{t in G(b2)} [FA(b2,t) VB(b1 t|P2) - FB(b2,t) VA(b1 t|P2)]
 //   ket legs: C -= sum_{t in G(k1)} [FA'(k1,t) VB(P1|t k2) - FB'(k1,t) VA(P1|t k2)]
@@ -14,73 +12,88 @@
 // block q.  F/F' are the reference's one-body reads (see dev_common.cuh).
 //
 // Group pairs.  The pairs of block q split into the sets S(g,h) of pairs with
-// one state in (m_l,m_s) group g and one in group h (g <= h).  Indexing S(g,h)
-// as cells (k1,k2) <-> (t1,t2) = (G_g[k1], G_h[k2]) and writing the block's
-// antisymmetric matrix in that orientation, M(k1,k2) = V(t1 t2|.) (= -V of the
-// stored pair when t1 > t2; 0 on the diagonal when g = h), the bra legs of
-// every pair of S(g,h) are
-//   Y = F_g M + M F_h^T,   F_g(k1',k1) = F(G_g[k1'], k1-th member of G_g),
-// and C(pair) = (orientation sign) * Y(cell).  The ket legs are the same with
-// F' and V transposed.  Each product runs along "fibers": a fixed k2 (F_g,
-// length |G_g|) or a fixed k1 (F_h, length |G_h|).  A warp takes one group
-// pair and direction at a time and forms the product on the FP64 tensor pipe
-// (mma.sync m8n8k4): F as A fragments held in registers, the staged cells as
-// B fragments, FA * VB and -FB * VA into one accumulator.
+// one state in (m_l,m_s) group g and one in group h (g <= h).  A bra leg of
+// a pair in S(g,h) replaces a state by another of the same group, so it stays
+// in S(g,h); a ket leg likewise stays in the column pair's set.  Hence the
+// block matrix splits into tiles S_a x S_b, and C on tile (a,b) depends only
+// on A and B on the same tile and on four small one-body matrices:
+//   C[S_a, S_b] = (F_g (x) 1 + 1 (x) F_h) T  -  T (F'_g' (x) 1 + 1 (x) F'_h')^T
+// with T the tile in "cell" coordinates: S(g,h) indexed by cells (k1,k2) <->
+// (G_g[k1], G_h[k2]), T = +-V of the stored pair (the sign orients the pair;
+// when g = h both orientations (k1,k2), (k2,k1) are cells and (k,k) is 0).
 //
-// Pass 1 (bra, SET): a CTA stages TJ columns of V_A and V_B (all ntot rows,
-// upper classes through herm) in shared memory in cell order, runs the k1
-// fibers, then the k2 fibers, and writes those columns of every stored class.
-// Pass 2 (ket, ACC): a CTA stages TJ rows and subtracts the ket legs of those
-// rows.  Each pass reads both operators about once; the products read shared
-// memory and registers only.
+// Kernel: one CTA per tile.  The tile of each operand needed is gathered with
+// cp.async into shared memory (rows of one class of S_a are runs of
+// consecutive stored rows, so the gathers coalesce in runs), the orientation
+// and herm signs are applied in place, then every stored output cell sums its
+// four legs from shared memory and is written once.  C is written exactly
+// once (122 overwrites the two-body part), A and B are read once, apart from
+// the off-diagonal class blocks, which tiles (a,b) and (b,a) both read.
+// When an operand's one-body part has no hh and no pp entries (the Magnus
+// generator Omega), F couples holes to particles only: a leg of a hole sums
+// over the particles of its group and a leg of a particle over its holes
+// (holes are the lowest members of every group).  Tiles whose parts of A are
+// known to be zero skip the A term (and then stage B alone).
 #include <algorithm>
 #include <map>
+#include <cstdio>
 #include <mutex>
+#include <string>
 #include <type_traits>
 
 #include "dev_common.cuh"
 
 namespace qd {
 
-constexpr int T122 = 256;                          // threads per CTA
-constexpr int GMAX122 = 16;                        // largest (m_l,m_s) group (fiber length)
-constexpr size_t SMEM_MAX_ATTR_122 = 227 * 1024;   // opt-in shared memory per CTA on sm_100
-constexpr size_t SMEM_TARGET_122 = 74 * 1024;      // per-CTA staging goal: three CTAs per SM
-constexpr size_t SMEM_STATIC_122 = 1024;           // bound on the pass kernels' static shared memory
-// Per-pass TJ rule (measured on the N=20 R=20 flow, 122 ms per flow): both
-// passes at TJ >= 2 within 74 KB, 592; the ket pass at TJ >= 4 within 112 or
-// 150 KB (whole 32-byte sectors, fewer CTAs), 812-820; TJ = 1 on the largest
-// blocks of either pass, 637-808; 8 staging loads in flight per thread
-// instead of 4 (U122), 611.  Parallelism beats sector efficiency here.
-constexpr size_t KET_SMEM_TARGET_122 = 74 * 1024;   // ket pass: three CTAs per SM
-constexpr int KET_MIN_TJ_122 = 2;
-constexpr int BRA_MIN_TJ_122 = 2;
+#ifndef TRY
+#define TRY(x)           \
+  do {                   \
+    int rc_ = (x);       \
+    if (rc_) return rc_; \
+  } while (0)
+#endif
 
-struct Task122 {
-  int q;
-  short cls;   // column class (bra pass) or row class (ket pass)
-  short pad;
-  int first;   // first column / row within the class
-};
+constexpr size_t SMEM_MAX_122 = 227 * 1024;       // opt-in shared memory per CTA on sm_100
 
 // vectorize slot of the stored part (row class c1 >= column class c2):
 // (0,0) hhhh 0, (2,2) pppp 1, (2,0) pphh 2, (1,1) phph 3, (2,1) ppph 4, (1,0) phhh 5
-__device__ __forceinline__ int slot_of(int c1, int c2) {
+__host__ __device__ __forceinline__ int slot_of(int c1, int c2) {
   if (c1 == 0) return 0;
   if (c1 == 1) return c2 == 0 ? 5 : 3;
   return c2 == 0 ? 2 : (c2 == 1 ? 4 : 1);
 }
-__device__ __forceinline__ int off_of(int c, int4 bd) { return c == 0 ? 0 : (c == 1 ? bd.x : bd.x + bd.y); }
 __device__ __forceinline__ int cnt_of(int c, int4 bd) { return c == 0 ? bd.x : (c == 1 ? bd.y : bd.z); }
-__device__ __forceinline__ int cls_of(int P, int nh, int nb) { return P < nh ? 0 : (P < nh + nb ? 1 : 2); }
+
+// Group-pair descriptor (two int4 per group pair u):
+//   d0 = {q, n1 | n2 << 8 | (g == h) << 16, holes(g) | holes(h) << 8, F offset of g}
+//   d1 = {F offset of h, first pair entry, first cell entry, cnt_hh | cnt_ph << 10 | cnt_pp << 20}
+// Pair entries (int2, sorted by class then index within the class):
+//   {index w within its class, primary cell | (mirror cell + 1) << 8 | (sign < 0) << 16}
+// Cell entries (one byte per cell of the n1 x n2 grid):
+//   valid << 3 | class << 1 | (sign < 0); 0 for the (t,t) cells of g = h.
+struct GpDesc {
+  int q, n1, n2, hg, hh, fg, fh, pstart, cstart, cnt[3];
+};
+__device__ __forceinline__ GpDesc load_gp(const int4* __restrict__ gpd, int u) {
+  const int4 a = __ldg(&gpd[2 * u]), b = __ldg(&gpd[2 * u + 1]);
+  GpDesc d;
+  d.q = a.x;
+  d.n1 = a.y & 0xFF;
+  d.n2 = (a.y >> 8) & 0xFF;
+  d.hg = a.z & 0xFF;
+  d.hh = (a.z >> 8) & 0xFF;
+  d.fg = a.w;
+  d.fh = b.x;
+  d.pstart = b.y;
+  d.cstart = b.z;
+  d.cnt[0] = b.w & 0x3FF;
+  d.cnt[1] = (b.w >> 10) & 0x3FF;
+  d.cnt[2] = (b.w >> 20) & 0x3FF;
+  return d;
+}
 
 // Static tables of a layout (built once, see plan_122):
-//   meta[q]   = {cells of block q, first group pair, end of its group pairs, 0}
-//   sub[u]    = {first cell, |G_g| | |G_h| << 8 | (g = h) << 16, offset of F_g,
-//               offset of F_h} (group pairs of a block in decreasing size)
-//   cell[gp]  = for the pair gp = pbase[q] + P: {primary cell << 1 | (orientation sign < 0),
-//               mirror cell (the same pair seen as (t2,t1) when g = h) or -1}
-//   sbase[s]  = offset of state s's row in the group-major F table
+//   sbase[s] = offset of state s's row in the group-major F table
 // Per call: F table [2][nfent] double2 (FA, FB) bra, then (FA', FB') ket,
 // group-major: F[goff_g + k1' * |G_g| + k].
 __global__ void k_ftab(DevLayout L, const int* __restrict__ sbase, const double* __restrict__ A, double hA,
@@ -105,287 +118,253 @@ __global__ void k_ftab(DevLayout L, const int* __restrict__ sbase, const double*
   F[nfent + pos] = make_double2(fak, fbk);
 }
 
-__device__ __forceinline__ void dmma122(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// One direction of one group pair, by one warp, on the FP64 tensor pipe:
-// Y(r, col) = sum_k F(r,k) (FA * VB - FB * VA)(k, col) as m8n8k4 products.
-// DIR 0: F = F_g (N = |G_g|), columns col = (k2, j), cell (k, col) =
-// base + k n2 + k2 (assigns: it reaches every cell once); DIR 1: F = F_h
-// (N = |G_h|), columns col = (k1, j), cell = base + k1 n2 + k (adds).
-// Fragments (m8n8k4): A row lane/4, k lane%4; B k lane%4, column lane/4;
-// D row lane/4, columns 2 (lane%4) + {0,1}.  Out-of-range rows, k and
-// columns are selected to zero (never multiplied with shared-memory data).
-template <int N, int TJ, int DIR>
-__device__ __forceinline__ void pair_dir(int base, int n1, int n2, int fofs, int lane, const double2* __restrict__ Vc,
-                                         double* __restrict__ Yc, const double2* __restrict__ F) {
-  constexpr int MT = (N + 7) / 8, KS = (N + 3) / 4;
-  double fa[MT][KS], fb[MT][KS];
-#pragma unroll
-  for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-    for (int ks = 0; ks < KS; ++ks) {
-      const int r = 8 * mt + (lane >> 2), k = 4 * ks + (lane & 3);
-      double2 f = make_double2(0.0, 0.0);
-      if (r < N && k < N) f = __ldg(&F[fofs + r * N + k]);
-      fa[mt][ks] = f.x;
-      fb[mt][ks] = -f.y;
-    }
-  const int ncol = (DIR ? n1 : n2) * TJ;
-  auto cell = [&](int k, int col) -> int {  // staged element of (k, col)
-    return DIR ? (base + (col / TJ) * n2 + k) * TJ + (col % TJ) : (base + k * n2) * TJ + col;
-  };
-  for (int c0 = 0; c0 < ncol; c0 += 8) {
-    double d[MT][2];
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt) d[mt][0] = d[mt][1] = 0.0;
-    const int bcol = c0 + (lane >> 2);
-#pragma unroll
-    for (int ks = 0; ks < KS; ++ks) {
-      const int k = 4 * ks + (lane & 3);
-      double2 v = make_double2(0.0, 0.0);
-      if (k < N && bcol < ncol) v = Vc[cell(k, bcol)];
-#pragma unroll
-      for (int mt = 0; mt < MT; ++mt) {
-        dmma122(d[mt][0], d[mt][1], fa[mt][ks], v.y);
-        dmma122(d[mt][0], d[mt][1], fb[mt][ks], v.x);
-      }
-    }
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = 8 * mt + (lane >> 2), c = c0 + 2 * (lane & 3) + e;
-        if (r < N && c < ncol) {
-          double* y = Yc + cell(r, c);
-          if (DIR)
-            *y += d[mt][e];
-          else
-            *y = d[mt][e];
-        }
-      }
+// summation range of a leg: all members of the group, or (one-body part with
+// no hh and pp entries) the members of the other kind
+__device__ __forceinline__ void leg_range(int k, int n, int h, int sparse, int& lo, int& hi) {
+  lo = 0;
+  hi = n;
+  if (sparse) {
+    if (k < h)
+      lo = h;
+    else
+      hi = h;
   }
 }
 
-// all group pairs of the block, one direction; warps take group pairs in turn
-// (no two group pairs share a cell, no two fibers of a direction share a cell)
-template <int TJ, int DIR, int GM>
-__device__ __forceinline__ void run_dir(const int4* __restrict__ sub, int ns, const double2* Vc, double* Yc,
-                                        const double2* __restrict__ F) {
-  const int lane = threadIdx.x & 31;
-  for (int u = threadIdx.x >> 5; u < ns; u += T122 / 32) {
-    const int4 d = __ldg(&sub[u]);
-    const int n1 = d.y & 0xFF, n2 = (d.y >> 8) & 0xFF;
-    const int fofs = DIR ? d.w : d.z;
-    switch (DIR ? n2 : n1) {
-#define QD_DIR_CASE(N)                                                         \
-  case N:                                                                      \
-    if constexpr (N <= GM) pair_dir<N, TJ, DIR>(d.x, n1, n2, fofs, lane, Vc, Yc, F); \
-    break;
-      QD_DIR_CASE(1) QD_DIR_CASE(2) QD_DIR_CASE(3) QD_DIR_CASE(4)
-      QD_DIR_CASE(5) QD_DIR_CASE(6) QD_DIR_CASE(7) QD_DIR_CASE(8)
-      QD_DIR_CASE(9) QD_DIR_CASE(10) QD_DIR_CASE(11) QD_DIR_CASE(12)
-      QD_DIR_CASE(13) QD_DIR_CASE(14) QD_DIR_CASE(15) QD_DIR_CASE(16)
-#undef QD_DIR_CASE
-      default: break;
-    }
-  }
-}
-
-// stage (VA, VB) of a pair into its cell(s), staged column/row j
-template <int TJ>
-__device__ __forceinline__ void stage_cell(double2* Vc, int2 cl, int j, double va, double vb) {
-  const double s = (cl.x & 1) ? -1.0 : 1.0;
-  Vc[(cl.x >> 1) * TJ + j] = make_double2(s * va, s * vb);
-  if (cl.y >= 0) Vc[cl.y * TJ + j] = make_double2(-s * va, -s * vb);
-}
-
-constexpr int U122 = 4;  // staging loads in flight per thread
-
-// Pass kernels.  KET = 0: bra pass over TJ columns of class ct = tk.cls
-// (SET); KET = 1: ket pass over TJ rows of class ct (subtract).  The staged
-// operand values V(P1,P2) are read class segment by class segment of the
-// other index: segment c (cnt_c pairs) of stored part (max(c,ct), min(c,ct))
-// is contiguous along the pair index when its rows are the varying index,
-// else strided; the upper segments carry herm.
-template <int TJ, int KET, int GM>
-__global__ void __launch_bounds__(T122, GM <= 10 ? 3 : 2) k_122_pass(DevLayout L, const Task122* __restrict__ tasks,
-                                                   const int4* __restrict__ meta, const int4* __restrict__ sub,
-                                                   const int2* __restrict__ cell, const double2* __restrict__ Ftab,
-                                                   const double* __restrict__ A, double hA, unsigned zA,
-                                                   const double* __restrict__ B, double hB, unsigned zB,
+// Task: {tile, op}; op bit 0: the B term (FA x TB), bit 1: the A term
+// (-FB x TA), bit 2: accumulate into C instead of setting it.  op & 3 == 0
+// writes zeros.  TW = doubles per staged cell: 1 (one operand), 2 (A and B);
+// T122 = threads per CTA (picked per launch bucket by the autotuner below).
+template <int TW, int T122>
+__global__ void __launch_bounds__(T122) k_122_tile(DevLayout L, const int2* __restrict__ tasks,
+                                                   const int2* __restrict__ tiles, const int4* __restrict__ gpd,
+                                                   const int2* __restrict__ gpp,
+                                                   const unsigned char* __restrict__ cinfo,
+                                                   const double2* __restrict__ F, int nfent,
+                                                   const double* __restrict__ A, double hA, unsigned zA, int spA,
+                                                   const double* __restrict__ B, double hB, unsigned zB, int spB,
                                                    double* __restrict__ C) {
-  extern __shared__ double2 smv[];
-  const Task122 tk = tasks[blockIdx.x];
-  const int q = tk.q, ct = tk.cls;
+  extern __shared__ __align__(16) double sm122[];
+  const int2 task = tasks[blockIdx.x];
+  const int2 tl = __ldg(&tiles[task.x]);
+  const int op = task.y;
+  const bool useB = op & 1, useA = (op >> 1) & 1, acc = (op >> 2) & 1;
+  const GpDesc da = load_gp(gpd, tl.x), db = load_gp(gpd, tl.y);
+  const int q = da.q;
+  const int n1 = da.n1, n2 = da.n2, n3 = db.n1, n4 = db.n2;
+  const int nr = n1 * n2, nc = n3 * n4, ld = nc | 1;
+  const int pa = da.cnt[0] + da.cnt[1] + da.cnt[2], pb = db.cnt[0] + db.cnt[1] + db.cnt[2];
   const int4 bd = __ldg(&L.blk[q]);
-  const int4 mt = __ldg(&meta[q]);
-  double2* Vc = smv;                                        // [cells][TJ] (VA, VB)
-  double* Yc = reinterpret_cast<double*>(smv + mt.x * TJ);  // [cells][TJ]
-  int* pc = reinterpret_cast<int*>(Yc + mt.x * TJ);          // [ntot] primary cell << 1 | sign
-  const int nct = cnt_of(ct, bd);
-  const int nj = min(TJ, nct - tk.first);  // staged columns (bra) / rows (ket)
-  const int pb = __ldg(&L.pbase[q]);
-  const i64* o = L.boff + 6 * q;
-  const int ns = mt.z - mt.y;
-  sub += mt.y;
-  // cells of no pair: the diagonal (t,t) of same-group pairs
-  for (int u = threadIdx.x; u < ns; u += T122) {
-    const int4 d = __ldg(&sub[u]);
-    if (d.y >> 16) {
-      const int n = d.y & 0xFF;
-      for (int k = 0; k < n; ++k)
-#pragma unroll
-        for (int j = 0; j < TJ; ++j) Vc[(d.x + k * (n + 1)) * TJ + j] = make_double2(0.0, 0.0);
-    }
+  const i64* boff = L.boff + 6 * q;
+  // shared memory: T [nr][ld][TW] | F1 F2 F3 F4 (double2) | row, column pairs (int2) | cell bytes
+  double* T = sm122;
+  const int tsz = (nr * ld * TW + 1) & ~1;
+  double2* F1 = reinterpret_cast<double2*>(sm122 + tsz);
+  double2* F2 = F1 + n1 * n1;
+  double2* F3 = F2 + n2 * n2;
+  double2* F4 = F3 + n3 * n3;
+  int2* pr = reinterpret_cast<int2*>(F4 + n4 * n4);
+  int2* pc = pr + pa;
+  unsigned char* cr = reinterpret_cast<unsigned char*>(pc + pb);
+  unsigned char* cc = cr + nr;
+  const int tid = threadIdx.x;
+  const bool work = useA || useB;
+
+  if (work) {
+    for (int i = tid; i < n1 * n1; i += T122) F1[i] = __ldg(&F[da.fg + i]);
+    for (int i = tid; i < n2 * n2; i += T122) F2[i] = __ldg(&F[da.fh + i]);
+    for (int i = tid; i < n3 * n3; i += T122) F3[i] = __ldg(&F[nfent + db.fg + i]);
+    for (int i = tid; i < n4 * n4; i += T122) F4[i] = __ldg(&F[nfent + db.fh + i]);
+    for (int i = tid; i < nr; i += T122) cr[i] = __ldg(&cinfo[da.cstart + i]);
+    for (int i = tid; i < nc; i += T122) cc[i] = __ldg(&cinfo[db.cstart + i]);
   }
-  for (int c = 0; c < 3; ++c) {
-    const int nc = cnt_of(c, bd);
-    if (nc == 0) continue;
-    // element (r, j): the pair r of segment c against staged index j
-    const bool lower = KET ? (ct >= c) : (c >= ct);  // stored without transposition
-    const int sl = KET ? (lower ? slot_of(ct, c) : slot_of(c, ct)) : (lower ? slot_of(c, ct) : slot_of(ct, c));
-    const bool za = (zA >> (P_HHHH + sl)) & 1u, zb = (zB >> (P_HHHH + sl)) & 1u;
-    const double fa = lower ? 1.0 : hA, fb = lower ? 1.0 : hB;
-    // bra: V(row r of c, column first+j); ket: V(row first+j, column r of c).
-    // The stored part's rows are segment c (bra lower, ket upper): address
-    // r + (first+j) * nc; else its rows are class ct: (first+j) + r * nct.
-    const bool crow = KET ? !lower : lower;
-    const i64 rs = crow ? 1 : nct, js = crow ? nc : 1;
-    const i64 b0 = __ldg(o + sl) + (crow ? (i64)tk.first * nc : (i64)tk.first);
-    const int offc = off_of(c, bd);
-    const int total = nc * TJ;
-    for (int e0 = threadIdx.x; e0 < total; e0 += U122 * T122) {
-      double va[U122], vb[U122];
-      int2 cl[U122];
-#pragma unroll
-      for (int u = 0; u < U122; ++u) {
-        const int e = e0 + u * T122;
-        const int r = e / TJ, j = e % TJ;
-        va[u] = vb[u] = 0.0;
-        cl[u] = make_int2(-1, -1);
-        if (e < total && j < nj) {
-          const i64 a = b0 + r * rs + j * js;
-          cl[u] = __ldg(&cell[pb + offc + r]);
-          if (!za) va[u] = fa * __ldg(A + a);
-          if (!zb) vb[u] = fb * __ldg(B + a);
+  for (int i = tid; i < pa; i += T122) pr[i] = __ldg(&gpp[da.pstart + i]);
+  for (int i = tid; i < pb; i += T122) pc[i] = __ldg(&gpp[db.pstart + i]);
+  __syncthreads();
+
+  if (work) {
+    // gather: region (c1 rows of S_a, c2 columns of S_b); the stored element
+    // is (P1,P2) of part (c1,c2) when c1 >= c2, else (P2,P1) of part (c2,c1)
+    for (int x = 0; x < 2; ++x) {
+      if (x == 0 ? !useA : !useB) continue;
+      const double* src = x == 0 ? A : B;
+      const unsigned zm = x == 0 ? zA : zB;
+      const int xo = TW == 2 ? x : 0;
+      int o1 = 0;
+      for (int c1 = 0; c1 < 3; ++c1) {
+        const int r1 = da.cnt[c1];
+        int o2 = 0;
+        for (int c2 = 0; c2 < 3; ++c2) {
+          const int r2 = db.cnt[c2];
+          const bool lower = c1 >= c2;
+          const int part = lower ? slot_of(c1, c2) : slot_of(c2, c1);
+          if (r1 > 0 && r2 > 0 && !((zm >> (P_HHHH + part)) & 1u)) {
+            const i64 base = __ldg(boff + part);
+            const i64 ldv = lower ? cnt_of(c1, bd) : cnt_of(c2, bd);
+            const int total = r1 * r2;
+            for (int e = tid; e < total; e += T122) {
+              int p, u;
+              if (lower) {
+                p = e % r1;
+                u = e / r1;
+              } else {
+                u = e % r2;
+                p = e / r2;
+              }
+              const int2 P = pr[o1 + p], Q = pc[o2 + u];
+              const i64 addr = lower ? base + P.x + (i64)Q.x * ldv : base + Q.x + (i64)P.x * ldv;
+              const double* g = src + addr;
+              const int r = P.y & 0xFF, rm = ((P.y >> 8) & 0xFF) - 1;
+              const int s = Q.y & 0xFF, sm = ((Q.y >> 8) & 0xFF) - 1;
+              cp_async8(&T[(r * ld + s) * TW + xo], g);
+              if (rm >= 0) cp_async8(&T[(rm * ld + s) * TW + xo], g);
+              if (sm >= 0) {
+                cp_async8(&T[(r * ld + sm) * TW + xo], g);
+                if (rm >= 0) cp_async8(&T[(rm * ld + sm) * TW + xo], g);
+              }
+            }
+          }
+          o2 += r2;
         }
-      }
-#pragma unroll
-      for (int u = 0; u < U122; ++u)
-        if (cl[u].x >= 0) {
-          const int e = e0 + u * T122;
-          stage_cell<TJ>(Vc, cl[u], e % TJ, va[u], vb[u]);
-          if (e % TJ == 0) pc[offc + e / TJ] = cl[u].x;
-        }
-    }
-  }
-  __syncthreads();
-  run_dir<TJ, 0, GM>(sub, ns, Vc, Yc, Ftab);
-  __syncthreads();
-  run_dir<TJ, 1, GM>(sub, ns, Vc, Yc, Ftab);
-  __syncthreads();
-  // output: bra -> rows of classes c >= ct of the staged columns (SET);
-  // ket -> columns of classes c <= ct of the staged rows (subtract)
-  for (int c = KET ? 0 : ct; c <= (KET ? ct : 2); ++c) {
-    const int nc = cnt_of(c, bd);
-    if (nc == 0) continue;
-    const int sl = KET ? slot_of(ct, c) : slot_of(c, ct);
-    const i64 rs = KET ? nct : 1, js = KET ? 1 : nc;
-    const i64 b0 = __ldg(o + sl) + (KET ? (i64)tk.first : (i64)tk.first * nc);
-    const int offc = off_of(c, bd);
-    for (int e0 = threadIdx.x; e0 < nc * TJ; e0 += U122 * T122) {
-#pragma unroll
-      for (int u = 0; u < U122; ++u) {
-        const int e = e0 + u * T122;
-        const int r = e / TJ, j = e % TJ;
-        if (e >= nc * TJ || j >= nj) continue;
-        const int cx = pc[offc + r];
-        const double y = Yc[(cx >> 1) * TJ + j];
-        double* out = C + b0 + r * rs + j * js;
-        if (KET)
-          *out -= (cx & 1) ? -y : y;
-        else
-          *out = (cx & 1) ? -y : y;
+        o1 += r1;
       }
     }
+    cp_async_wait_all();
+    __syncthreads();
+    // orientation and herm signs in place; (t,t) cells and known-zero parts -> 0
+    for (int e = tid; e < nr * nc; e += T122) {
+      const int r = e / nc, s = e - r * nc;
+      const int ci = cr[r], cj = cc[s];
+      const int c1 = (ci >> 1) & 3, c2 = (cj >> 1) & 3;
+      const bool valid = (ci & cj & 8) != 0;
+      const int part = c1 >= c2 ? slot_of(c1, c2) : slot_of(c2, c1);
+      const double sg = ((ci ^ cj) & 1) ? -1.0 : 1.0;
+      for (int x = 0; x < 2; ++x) {
+        if (x == 0 ? !useA : !useB) continue;
+        const unsigned zm = x == 0 ? zA : zB;
+        const double f = c1 < c2 ? sg * (x == 0 ? hA : hB) : sg;
+        double* t = &T[(r * ld + s) * TW + (TW == 2 ? x : 0)];
+        *t = (valid && !((zm >> (P_HHHH + part)) & 1u)) ? f * *t : 0.0;
+      }
+    }
+    __syncthreads();
+  }
+
+  // stored output cells: regions with c1 >= c2, rows of S_a fastest
+  const int xa = 0, xb = TW == 2 ? 1 : 0;
+  int o1 = 0;
+  for (int c1 = 0; c1 < 3; ++c1) {
+    const int r1 = da.cnt[c1];
+    int o2 = 0;
+    for (int c2 = 0; c2 <= c1; ++c2) {
+      const int r2 = db.cnt[c2];
+      if (r1 > 0 && r2 > 0) {
+        const i64 base = __ldg(boff + slot_of(c1, c2));
+        const i64 ldc = cnt_of(c1, bd);
+        for (int e = tid; e < r1 * r2; e += T122) {
+          const int p = e % r1, u = e / r1;
+          const int2 P = pr[o1 + p], Q = pc[o2 + u];
+          double y = 0.0;
+          if (work) {
+            const int r = P.y & 0xFF, s = Q.y & 0xFF;
+            const int k1 = r / n2, k2 = r - k1 * n2, l1 = s / n4, l2 = s - l1 * n4;
+            int lo, hi;
+            if (useB) {  // FA x TB
+              leg_range(k1, n1, da.hg, spA, lo, hi);
+              for (int t = lo; t < hi; ++t) y += F1[k1 * n1 + t].x * T[((t * n2 + k2) * ld + s) * TW + xb];
+              leg_range(k2, n2, da.hh, spA, lo, hi);
+              for (int t = lo; t < hi; ++t) y += F2[k2 * n2 + t].x * T[((k1 * n2 + t) * ld + s) * TW + xb];
+              leg_range(l1, n3, db.hg, spA, lo, hi);
+              for (int t = lo; t < hi; ++t) y -= F3[l1 * n3 + t].x * T[(r * ld + t * n4 + l2) * TW + xb];
+              leg_range(l2, n4, db.hh, spA, lo, hi);
+              for (int t = lo; t < hi; ++t) y -= F4[l2 * n4 + t].x * T[(r * ld + l1 * n4 + t) * TW + xb];
+            }
+            if (useA) {  // -FB x TA
+              leg_range(k1, n1, da.hg, spB, lo, hi);
+              for (int t = lo; t < hi; ++t) y -= F1[k1 * n1 + t].y * T[((t * n2 + k2) * ld + s) * TW + xa];
+              leg_range(k2, n2, da.hh, spB, lo, hi);
+              for (int t = lo; t < hi; ++t) y -= F2[k2 * n2 + t].y * T[((k1 * n2 + t) * ld + s) * TW + xa];
+              leg_range(l1, n3, db.hg, spB, lo, hi);
+              for (int t = lo; t < hi; ++t) y += F3[l1 * n3 + t].y * T[(r * ld + t * n4 + l2) * TW + xa];
+              leg_range(l2, n4, db.hh, spB, lo, hi);
+              for (int t = lo; t < hi; ++t) y += F4[l2 * n4 + t].y * T[(r * ld + l1 * n4 + t) * TW + xa];
+            }
+            if ((P.y ^ Q.y) & (1 << 16)) y = -y;
+          }
+          double* out = C + base + P.x + (i64)Q.x * ldc;
+          if (acc)
+            *out += y;
+          else
+            *out = y;
+        }
+      }
+      o2 += r2;
+    }
+    o1 += r1;
   }
 }
 
 // ---- host side --------------------------------------------------------------
 namespace {
-// Tasks are grouped in buckets by TJ; each bucket is one launch per pass
-// whose dynamic shared memory fits its largest block.
+struct TileInfo {
+  int a, b;          // group pairs
+  int cells;         // nr * nc
+  int nf, npair;     // F entries (double2) and pair entries of the two group pairs
+  int nr, nc;
+  unsigned parts;    // two-body parts the tile touches (bit = vectorize slot)
+};
 struct Bucket122 {
-  int tj;       // 1, 2, 4, 8 or 16
+  int tw;       // doubles per staged cell
   int first;    // range in the task array
   int count;
   size_t smem;
+  int threads = 256;    // CTA size (autotuned)
+  float ms[2] = {0, 0};  // measured time of the 128- and 256-thread variants
+};
+struct TaskSet {
+  int2* d_task = nullptr;
+  std::vector<Bucket122> buckets;
+  bool tuned = false;
 };
 struct Plan122 {
-  Task122* d_task = nullptr;
-  int4* d_meta = nullptr;
-  int4* d_sub = nullptr;
-  int2* d_cell = nullptr;
+  int4* d_gpd = nullptr;
+  int2* d_gpp = nullptr;
+  unsigned char* d_cinfo = nullptr;
+  int2* d_tiles = nullptr;
   int* d_sbase = nullptr;
   double2* d_ftab = nullptr;
-  int ntask = 0, gmax = 0, nfent = 0;
-  std::vector<Bucket122> buckets[2];  // bra pass, ket pass
+  int gmax = 0, nfent = 0;
+  std::vector<TileInfo> tiles;
+  std::map<std::pair<unsigned, unsigned>, TaskSet> sets;  // per (zero mask A, zero mask B)
 };
 std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
   return m;
 }
 // plans of different layouts are built and dropped from concurrent host
-// threads (batched flows); map nodes stay put, so a found plan needs no lock
+// threads (batched flows)
 std::mutex g_plan_mutex;
 
-size_t smem_122(int cells, int npair, int tj) {
-  return (sizeof(double2) + sizeof(double)) * (size_t)cells * tj + sizeof(int) * (size_t)((npair + 3) & ~3);
+size_t tile_smem(const TileInfo& t, int tw) {
+  const size_t ld = (size_t)(t.nc | 1);
+  const size_t tsz = ((size_t)t.nr * ld * tw + 1) & ~(size_t)1;
+  return 8 * tsz + 16 * (size_t)t.nf + 8 * (size_t)t.npair + (size_t)t.nr + (size_t)t.nc;
 }
-}  // namespace
 
-// the attribute is process-wide: set it to the device limit, so that plans
-// built concurrently for other layouts can never lower it below a need
-template <int GM>
-static int set_attr_122() {
-  const void* fns[10] = {(const void*)k_122_pass<16, 0, GM>, (const void*)k_122_pass<16, 1, GM>,
-                         (const void*)k_122_pass<8, 0, GM>,  (const void*)k_122_pass<8, 1, GM>,
-                         (const void*)k_122_pass<4, 0, GM>,  (const void*)k_122_pass<4, 1, GM>,
-                         (const void*)k_122_pass<2, 0, GM>,  (const void*)k_122_pass<2, 1, GM>,
-                         (const void*)k_122_pass<1, 0, GM>,  (const void*)k_122_pass<1, 1, GM>};
-  for (const void* fn : fns) {
-    cudaFuncAttributes fa;
-    QD_CUDA(cudaFuncGetAttributes(&fa, fn));  // static + dynamic shared memory <= the limit
-    QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)SMEM_MAX_ATTR_122 - (int)fa.sharedSizeBytes));
-  }
+template <class T>
+int upload_vec(qd_layout* L, const std::vector<T>& vec, T** dptr) {
+  QD_CUDA(cudaMalloc(dptr, std::max<size_t>(1, vec.size()) * sizeof(T)));
+  if (!vec.empty()) QD_CUDA(cudaMemcpy(*dptr, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
+  L->ws_bytes += (i64)(vec.size() * sizeof(T));
   return QD_OK;
 }
-
-template <int GM, int KET>
-static void pass_122(const Plan122* p, qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
-  const double2* ft = p->d_ftab + (KET ? p->nfent : 0);
-  for (const Bucket122& b : p->buckets[KET]) {
-#define QD_122_LAUNCH(TJ)                                                                                          \
-  k_122_pass<TJ, KET, GM><<<b.count, T122, b.smem, L->stream>>>(L->dev, p->d_task + b.first, p->d_meta, p->d_sub, \
-                                                                p->d_cell, ft, A->d, (double)A->herm,             \
-                                                                A->zero_mask, B->d, (double)B->herm,              \
-                                                                B->zero_mask, C)
-    switch (b.tj) {
-      case 16: QD_122_LAUNCH(16); break;
-      case 8: QD_122_LAUNCH(8); break;
-      case 4: QD_122_LAUNCH(4); break;
-      case 2: QD_122_LAUNCH(2); break;
-      default: QD_122_LAUNCH(1); break;
-    }
-#undef QD_122_LAUNCH
-    ++L->nlaunch;
-  }
-}
+}  // namespace
 
 static int plan_122(qd_layout* L, Plan122** out) {
   std::lock_guard<std::mutex> lock(g_plan_mutex);
@@ -397,135 +376,205 @@ static int plan_122(qd_layout* L, Plan122** out) {
   Plan122 p;
   const int m = L->m;
   const int ngroup = (int)L->gstart.size() - 1;
-  std::vector<int> gsz(ngroup), goff(ngroup + 1, 0), kpos(m, 0), sbase(m, 0);
+  std::vector<int> gsz(ngroup), goff(ngroup + 1, 0), kpos(m, 0), sbase(m, 0), holes(ngroup, 0);
   for (int g = 0; g < ngroup; ++g) {
     gsz[g] = L->gstart[g + 1] - L->gstart[g];
     p.gmax = std::max(p.gmax, gsz[g]);
     goff[g + 1] = goff[g] + gsz[g] * gsz[g];
-    for (int k = 0; k < gsz[g]; ++k) kpos[L->gmem[L->gstart[g] + k]] = k;
+    for (int k = 0; k < gsz[g]; ++k) {
+      const int s = L->gmem[L->gstart[g] + k];
+      kpos[s] = k;
+      if (s < L->n) {
+        if (k != holes[g]) {  // holes must be the lowest members of every group
+          set_error("commutator_122: holes are not the lowest states of their (ml,ms) group");
+          return QD_ERR_LAYOUT;
+        }
+        ++holes[g];
+      }
+    }
   }
-  if (p.gmax > GMAX122) {
-    set_error("commutator_122: (ml,ms) group of %d states exceeds %d", p.gmax, GMAX122);
+  if (p.gmax > 16) {  // cells of a group pair fit the 8-bit cell fields
+    set_error("commutator_122: (ml,ms) group of %d states exceeds 16", p.gmax);
     return QD_ERR_ARG;
   }
   p.nfent = goff[ngroup];
   for (int s = 0; s < m; ++s) sbase[s] = goff[L->gid[s]] + kpos[s] * gsz[L->gid[s]];
 
-  // group pairs and cells of every block
-  std::vector<int4> meta(L->nblock), sub;
-  std::vector<int2> cell(L->pairs.size(), int2{-1, -1});
+  std::vector<int4> gpd;
+  std::vector<int2> gpp;
+  std::vector<unsigned char> cinfo;
+  struct GpHost {
+    int n1, n2, cnt[3], nf, npair;
+  };
   for (int q = 0; q < L->nblock; ++q) {
     const int nh = L->blk[q].x, nb = L->blk[q].y, ntot = L->blk[q].w, pb = L->pbase[q];
-    std::map<std::pair<int, int>, int> subs;  // (g <= h) -> first cell
+    // group pairs in order of first appearance; per group pair its pairs in
+    // class order (pairs are enumerated [hh | ph | pp], each class by index)
+    std::map<std::pair<int, int>, int> idx;
     std::vector<std::pair<int, int>> order;
-    int ncell = 0;
+    std::vector<std::vector<int2>> plist;  // {w, packed cells}
+    std::vector<std::vector<unsigned char>> cl;
+    std::vector<GpHost> gh;
     for (int P = 0; P < ntot; ++P) {
-      const int2 pr = L->pairs[pb + P];
-      const int g = std::min(L->gid[pr.x], L->gid[pr.y]), h = std::max(L->gid[pr.x], L->gid[pr.y]);
-      if (subs.emplace(std::make_pair(g, h), ncell).second) {
+      const int2 pr = L->pairs[pb + P];  // 0-based states, pr.x < pr.y
+      const int c = P < nh ? 0 : (P < nh + nb ? 1 : 2);
+      const int w = P - (c == 0 ? 0 : (c == 1 ? nh : nh + nb));
+      const int gi = L->gid[pr.x], gj = L->gid[pr.y];
+      const int g = std::min(gi, gj), h = std::max(gi, gj);
+      auto ins = idx.emplace(std::make_pair(g, h), (int)order.size());
+      if (ins.second) {
         order.push_back({g, h});
-        ncell += gsz[g] * gsz[h];
+        plist.emplace_back();
+        cl.emplace_back((size_t)gsz[g] * gsz[h], (unsigned char)0);
+        gh.push_back(GpHost{gsz[g], gsz[h], {0, 0, 0}, 0, 0});
       }
-    }
-    std::vector<int4> sv;
-    for (const auto& gh : order) {
-      const int g = gh.first, h = gh.second, base = subs[gh], n1 = gsz[g], n2 = gsz[h];
-      for (int k1 = 0; k1 < n1; ++k1)
-        for (int k2 = 0; k2 < n2; ++k2) {
-          if (g == h && k1 == k2) continue;  // (t,t): no pair, M = 0
-          const int t1 = L->gmem[L->gstart[g] + k1], t2 = L->gmem[L->gstart[h] + k2];
-          const int e = L->ptab[(size_t)t1 * m + t2];
-          if (e < 0 || pt_blk(e) != q) {
-            set_error("commutator_122: group pair outside its block (layout inconsistency)");
-            return QD_ERR_LAYOUT;
-          }
-          const int c = pt_cls(e);
-          const int P = pt_idx(e) + (c == 0 ? 0 : (c == 1 ? nh : nh + nb));
-          const int cidx = base + k1 * n2 + k2;
-          if (g != h || k1 < k2)
-            cell[pb + P].x = cidx << 1 | pt_swap(e);
-          else
-            cell[pb + P].y = cidx;
-        }
-      sv.push_back(int4{base, n1 | n2 << 8 | (g == h) << 16, goff[g], goff[h]});
-    }
-    for (int P = 0; P < ntot; ++P)
-      if (cell[pb + P].x < 0) {
-        set_error("commutator_122: pair without a group-pair cell (layout inconsistency)");
-        return QD_ERR_LAYOUT;
+      const int u = ins.first->second;
+      int t1, t2;
+      if (g != h) {
+        t1 = gi == g ? pr.x : pr.y;
+        t2 = gi == g ? pr.y : pr.x;
+      } else {
+        t1 = pr.x;
+        t2 = pr.y;
       }
-    // largest group pairs first: the warps take them in turn
-    std::stable_sort(sv.begin(), sv.end(), [](const int4& a, const int4& b) {
-      return (a.y & 0xFF) * ((a.y >> 8) & 0xFF) > (b.y & 0xFF) * ((b.y >> 8) & 0xFF);
-    });
-    meta[q] = int4{ncell, (int)sub.size(), (int)(sub.size() + sv.size()), 0};
-    sub.insert(sub.end(), sv.begin(), sv.end());
+      const int n2c = gsz[h];
+      const int r = kpos[t1] * n2c + kpos[t2];
+      const int neg = t1 > t2 ? 1 : 0;
+      const int rm = g == h ? kpos[t2] * n2c + kpos[t1] : -1;
+      if (gsz[g] * gsz[h] > 256 || r >= 255 || rm >= 255) {
+        set_error("commutator_122: group pair of %d cells exceeds the cell fields", gsz[g] * gsz[h]);
+        return QD_ERR_ARG;
+      }
+      plist[u].push_back(int2{w, r | ((rm + 1) << 8) | (neg << 16)});
+      cl[u][r] = (unsigned char)(8 | (c << 1) | neg);
+      if (rm >= 0) cl[u][rm] = (unsigned char)(8 | (c << 1) | (1 - neg));
+      gh[u].cnt[c] += 1;
+    }
+    const int u0 = (int)gpd.size() / 2;
+    for (size_t u = 0; u < order.size(); ++u) {
+      const int g = order[u].first, h = order[u].second;
+      GpHost& d = gh[u];
+      if (d.cnt[0] > 1023 || d.cnt[1] > 1023 || d.cnt[2] > 1023) {
+        set_error("commutator_122: group pair class count exceeds 1023");
+        return QD_ERR_ARG;
+      }
+      d.nf = d.n1 * d.n1 + d.n2 * d.n2;
+      d.npair = d.cnt[0] + d.cnt[1] + d.cnt[2];
+      gpd.push_back(int4{q, d.n1 | (d.n2 << 8) | ((g == h ? 1 : 0) << 16), holes[g] | (holes[h] << 8), goff[g]});
+      gpd.push_back(int4{goff[h], (int)gpp.size(), (int)cinfo.size(), d.cnt[0] | (d.cnt[1] << 10) | (d.cnt[2] << 20)});
+      gpp.insert(gpp.end(), plist[u].begin(), plist[u].end());
+      cinfo.insert(cinfo.end(), cl[u].begin(), cl[u].end());
+    }
+    // tiles: every ordered pair of group pairs with at least one stored
+    // output cell (a row class >= a column class)
+    for (size_t a = 0; a < order.size(); ++a)
+      for (size_t b = 0; b < order.size(); ++b) {
+        const GpHost &A = gh[a], &B = gh[b];
+        bool out = false;
+        unsigned parts = 0;
+        for (int c1 = 0; c1 < 3; ++c1)
+          for (int c2 = 0; c2 < 3; ++c2)
+            if (A.cnt[c1] > 0 && B.cnt[c2] > 0) {
+              parts |= 1u << (c1 >= c2 ? slot_of(c1, c2) : slot_of(c2, c1));
+              if (c1 >= c2) out = true;
+            }
+        if (!out) continue;
+        TileInfo t;
+        t.a = u0 + (int)a;
+        t.b = u0 + (int)b;
+        t.nr = A.n1 * A.n2;
+        t.nc = B.n1 * B.n2;
+        t.cells = t.nr * t.nc;
+        t.nf = A.nf + B.nf;
+        t.npair = A.npair + B.npair;
+        t.parts = parts;
+        p.tiles.push_back(t);
+      }
   }
-
-  // tasks per pass: TJ = the largest power of two (min_tj..16) whose staging
-  // fits the pass's per-CTA goal; larger blocks first within a bucket.  The
-  // ket pass stages rows of column-major parts in TJ-long runs, so its TJ
-  // starts at KET_MIN_TJ_122 (whole 32-byte sectors).
-  std::vector<Task122> ht;
-  for (int pass = 0; pass < 2; ++pass) {
-    const size_t target = pass ? KET_SMEM_TARGET_122 : SMEM_TARGET_122;
-    const int min_tj = pass ? KET_MIN_TJ_122 : BRA_MIN_TJ_122;
-    const int tjs[5] = {16, 8, 4, 2, 1};
-    for (int bkt = 0; bkt < 5; ++bkt) {
-      const int tj = tjs[bkt];
-      if (tj < min_tj) continue;
-      std::vector<std::pair<int, Task122>> v;
-      int cmax = 0;
-      for (int q = 0; q < L->nblock; ++q) {
-        const int nc = meta[q].x;
-        if (L->blk[q].w == 0) continue;
-        int want = min_tj;
-        for (int t : tjs)
-          if (t >= min_tj && smem_122(nc, L->blk[q].w, t) <= target) {
-            want = t;
-            break;
-          }
-        if (want != tj) continue;
-        if (smem_122(nc, L->blk[q].w, tj) > SMEM_MAX_ATTR_122 - SMEM_STATIC_122) {
-          set_error("commutator_122: block of %d cells exceeds shared memory", nc);
-          return QD_ERR_ARG;
-        }
-        cmax = std::max(cmax, (int)smem_122(nc, L->blk[q].w, tj));
-        const int cnt[3] = {L->blk[q].x, L->blk[q].y, L->blk[q].z};
-        for (int c = 0; c < 3; ++c)
-          for (int f = 0; f < cnt[c]; f += tj) v.push_back({nc, Task122{q, (short)c, 0, f}});
-      }
-      if (v.empty()) continue;
-      std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-      Bucket122 bk;
-      bk.tj = tj;
-      bk.first = (int)ht.size();
-      bk.count = (int)v.size();
-      bk.smem = (size_t)cmax;
-      for (auto& x : v) ht.push_back(x.second);
-      p.buckets[pass].push_back(bk);
+  for (const TileInfo& t : p.tiles)
+    if (tile_smem(t, 1) > SMEM_MAX_122) {
+      set_error("commutator_122: tile of %d cells exceeds shared memory", t.cells);
+      return QD_ERR_ARG;
     }
-  }
-  p.ntask = (int)ht.size();
-  auto up = [&](auto& vec, auto** dptr) -> int {
-    using T = typename std::decay<decltype(vec[0])>::type;
-    QD_CUDA(cudaMalloc(dptr, std::max<size_t>(1, vec.size()) * sizeof(T)));
-    if (!vec.empty()) QD_CUDA(cudaMemcpy(*dptr, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
-    L->ws_bytes += (i64)(vec.size() * sizeof(T));
-    return QD_OK;
-  };
+  std::vector<int2> th(p.tiles.size());
+  for (size_t i = 0; i < p.tiles.size(); ++i) th[i] = int2{p.tiles[i].a, p.tiles[i].b};
   int rc;
-  if ((rc = up(ht, &p.d_task)) || (rc = up(meta, &p.d_meta)) || (rc = up(sub, &p.d_sub)) ||
-      (rc = up(cell, &p.d_cell)) || (rc = up(sbase, &p.d_sbase)))
+  if ((rc = upload_vec(L, gpd, &p.d_gpd)) || (rc = upload_vec(L, gpp, &p.d_gpp)) ||
+      (rc = upload_vec(L, cinfo, &p.d_cinfo)) || (rc = upload_vec(L, th, &p.d_tiles)) ||
+      (rc = upload_vec(L, sbase, &p.d_sbase)))
     return rc;
   QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)std::max(1, p.nfent)));
   L->ws_bytes += (i64)sizeof(double2) * 2 * p.nfent;
-  if (!p.buckets[0].empty() || !p.buckets[1].empty()) {
-    int rc2 = p.gmax <= 10 ? set_attr_122<10>() : set_attr_122<16>();
-    if (rc2) return rc2;
+  for (const void* fn : {(const void*)k_122_tile<1, 128>, (const void*)k_122_tile<2, 128>,
+                         (const void*)k_122_tile<1, 256>, (const void*)k_122_tile<2, 256>}) {
+    cudaFuncAttributes fa;
+    QD_CUDA(cudaFuncGetAttributes(&fa, fn));
+    QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMEM_MAX_122 - (int)fa.sharedSizeBytes));
   }
   plans()[L] = p;
   *out = &plans()[L];
+  return QD_OK;
+}
+
+// Tasks for one pair of zero-part masks: per tile the terms it needs, in
+// buckets of similar shared memory (largest first).  A tile that needs both
+// terms but does not fit with both operands staged runs as a B task that
+// sets C and an A task (in a later launch) that accumulates.
+static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet** out) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  auto key = std::make_pair(zA, zB);
+  auto it = p->sets.find(key);
+  if (it != p->sets.end()) {
+    *out = &it->second;
+    return QD_OK;
+  }
+  const unsigned one = (1u << P_FHH) | (1u << P_FPP) | (1u << P_FPH);
+  const bool fa0 = (zA & one) == one, fb0 = (zB & one) == one;  // a one-body part entirely zero
+  const unsigned za2 = (zA >> P_HHHH) & 63u, zb2 = (zB >> P_HHHH) & 63u;
+  // lists: 0 one operand (set), 1 both operands (set), 2 one operand (accumulate)
+  std::vector<std::pair<size_t, int2>> lst[3];
+  for (size_t i = 0; i < p->tiles.size(); ++i) {
+    const TileInfo& t = p->tiles[i];
+    const bool nb = !fa0 && (t.parts & ~zb2), na = !fb0 && (t.parts & ~za2);
+    const int op = (nb ? 1 : 0) | (na ? 2 : 0);
+    if (op == 3) {
+      if (tile_smem(t, 2) <= SMEM_MAX_122) {
+        lst[1].push_back({tile_smem(t, 2), int2{(int)i, 3}});
+      } else {
+        lst[0].push_back({tile_smem(t, 1), int2{(int)i, 1}});
+        lst[2].push_back({tile_smem(t, 1), int2{(int)i, 2 | 4}});
+      }
+    } else {
+      lst[0].push_back({tile_smem(t, 1), int2{(int)i, op}});  // op 0: zeros (the carve-out is kept)
+    }
+  }
+  TaskSet ts;
+  std::vector<int2> all;
+  const size_t bounds[4] = {24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122};
+  for (int l = 0; l < 3; ++l) {
+    auto& v = lst[l];
+    std::stable_sort(v.begin(), v.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    size_t i = 0;
+    while (i < v.size()) {
+      // bucket: tasks down to the next size bound below the first one
+      const size_t top = v[i].first;
+      size_t lower = 0;
+      for (size_t bnd : bounds)
+        if (bnd < top) lower = bnd;
+      Bucket122 b;
+      b.tw = l == 1 ? 2 : 1;
+      b.first = (int)all.size();
+      b.smem = top;
+      while (i < v.size() && v[i].first > lower) all.push_back(v[i++].second);
+      b.count = (int)all.size() - b.first;
+      ts.buckets.push_back(b);
+    }
+  }
+  int rc = upload_vec(L, all, &ts.d_task);
+  if (rc) return rc;
+  p->sets[key] = ts;
+  *out = &p->sets[key];
   return QD_OK;
 }
 
@@ -533,29 +582,132 @@ void drop_122_plan(const qd_layout* L) {
   std::lock_guard<std::mutex> lock(g_plan_mutex);
   auto it = plans().find(L);
   if (it == plans().end()) return;
-  const Plan122& p = it->second;
-  for (void* ptr : {(void*)p.d_task, (void*)p.d_meta, (void*)p.d_sub, (void*)p.d_cell, (void*)p.d_sbase,
+  Plan122& p = it->second;
+  for (void* ptr : {(void*)p.d_gpd, (void*)p.d_gpp, (void*)p.d_cinfo, (void*)p.d_tiles, (void*)p.d_sbase,
                     (void*)p.d_ftab})
     if (ptr) cudaFree(ptr);
+  for (auto& kv : p.sets)
+    if (kv.second.d_task) cudaFree(kv.second.d_task);
   plans().erase(it);
+}
+
+static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, const Bucket122& b, int threads,
+                         const qd_op* A, const qd_op* B, int spA, int spB, double* C) {
+#define QD_122_LAUNCH(TW, NT)                                                                                   \
+  k_122_tile<TW, NT><<<b.count, NT, b.smem, L->stream>>>(L->dev, ts->d_task + b.first, p->d_tiles, p->d_gpd,   \
+                                                         p->d_gpp, p->d_cinfo, p->d_ftab, p->nfent, A->d,       \
+                                                         (double)A->herm, A->zero_mask, spA, B->d,              \
+                                                         (double)B->herm, B->zero_mask, spB, C)
+  if (b.tw == 2) {
+    if (threads == 128) QD_122_LAUNCH(2, 128); else QD_122_LAUNCH(2, 256);
+  } else {
+    if (threads == 128) QD_122_LAUNCH(1, 128); else QD_122_LAUNCH(1, 256);
+  }
+#undef QD_122_LAUNCH
+  ++L->nlaunch;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// Autotuner: the first launch of a task set times every bucket with 128- and
+// 256-thread CTAs (CUDA events, best of two runs each) on the real operands,
+// writing into a scratch operator of the layout, and keeps the faster size
+// per bucket.  Every output cell is summed by one thread in a fixed order
+// whatever the CTA size, so the choice never changes a result.
+static int tune_122(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, const qd_op* B, int spA, int spB) {
+  double* scratch = scratch_operator(L);
+  if (!scratch) return QD_OK;  // no scratch: keep the defaults
+  cudaEvent_t e0, e1;
+  QD_CUDA(cudaEventCreate(&e0));
+  QD_CUDA(cudaEventCreate(&e1));
+  const long long n0 = L->nlaunch;
+  for (Bucket122& b : ts->buckets) {
+    for (int v = 0; v < 2; ++v) {
+      const int threads = v ? 256 : 128;
+      float best = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        QD_CUDA(cudaEventRecord(e0, L->stream));
+        TRY(launch_bucket(L, p, ts, b, threads, A, B, spA, spB, scratch));
+        QD_CUDA(cudaEventRecord(e1, L->stream));
+        QD_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        QD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, ms);
+      }
+      b.ms[v] = best;
+    }
+    b.threads = b.ms[0] < b.ms[1] ? 128 : 256;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  L->nlaunch = n0;  // tuning launches are not the caller's work
+  ts->tuned = true;
+  return QD_OK;
+}
+
+// Text summary of the autotuned buckets of every task set of the layout.
+std::string tuning_report_122(const qd_layout* L) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  auto it = plans().find(L);
+  if (it == plans().end()) return "";
+  std::string out;
+  char line[256];
+  for (const auto& kv : it->second.sets) {
+    snprintf(line, sizeof(line), "commutator_122 masks A=0x%03x B=0x%03x:\n", kv.first.first, kv.first.second);
+    out += line;
+    for (const Bucket122& b : kv.second.buckets) {
+      snprintf(line, sizeof(line), "  tiles %6d staged %d smem %6zu B: 128 thr %.4f ms, 256 thr %.4f ms -> %d\n",
+               b.count, b.tw, b.smem, b.ms[0], b.ms[1], b.threads);
+      out += line;
+    }
+  }
+  return out;
+}
+
+static bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+static int spars(const qd_op* X) {
+  const unsigned hp = (1u << P_FHH) | (1u << P_FPP);
+  return (X->zero_mask & hp) == hp;
+}
+
+// Build (and autotune on A, B) the plan and the task set of a pair of
+// zero-part masks ahead of a stream capture, which must neither allocate
+// nor synchronise.  A and B may be views with the masks zA, zB.
+int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B) {
+  Plan122* p;
+  int rc = plan_122(L, &p);
+  if (rc) return rc;
+  TaskSet* ts;
+  if ((rc = task_set(L, p, A->zero_mask, B->zero_mask, &ts))) return rc;
+  if (!ts->tuned && !L->prof.on && !capturing(L->stream)) {
+    // the F tables of these operands first: the timed launches read them
+    const int nf = L->m * p->gmax;
+    k_ftab<<<(nf + 127) / 128, 128, 0, L->stream>>>(L->dev, p->d_sbase, A->d, (double)A->herm, B->d,
+                                                    (double)B->herm, p->d_ftab, p->gmax, p->nfent);
+    QD_CUDA(cudaGetLastError());
+    TRY(tune_122(L, p, ts, A, B, spars(A), spars(B)));
+  }
+  return QD_OK;
 }
 
 int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   Plan122* p;
   int rc = plan_122(L, &p);
   if (rc) return rc;
-  if (p->ntask == 0) return QD_OK;
+  if (p->tiles.empty()) return QD_OK;
+  TaskSet* ts;
+  if ((rc = task_set(L, p, A->zero_mask, B->zero_mask, &ts))) return rc;
+  const int spA = spars(A), spB = spars(B);
   const int nf = L->m * p->gmax;
   k_ftab<<<(nf + 127) / 128, 128, 0, L->stream>>>(L->dev, p->d_sbase, A->d, (double)A->herm, B->d,
                                                   (double)B->herm, p->d_ftab, p->gmax, p->nfent);
   ++L->nlaunch;
-  if (p->gmax <= 10) {
-    pass_122<10, 0>(p, L, A, B, C);
-    pass_122<10, 1>(p, L, A, B, C);
-  } else {
-    pass_122<16, 0>(p, L, A, B, C);
-    pass_122<16, 1>(p, L, A, B, C);
-  }
+  if (!ts->tuned && !L->prof.on && !capturing(L->stream)) TRY(tune_122(L, p, ts, A, B, spA, spB));
+  for (const Bucket122& b : ts->buckets) TRY(launch_bucket(L, p, ts, b, b.threads, A, B, spA, spB, C));
   QD_CUDA(cudaGetLastError());
   return QD_OK;
 }

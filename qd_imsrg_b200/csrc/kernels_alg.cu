@@ -6,6 +6,13 @@
 
 namespace qd {
 
+// BCH_EXPAND's truncated coefficients cof(1..11) (magnus_IMSRG.f90:265-267),
+// for terms whose coefficient is picked on the device (whole BCH step in one
+// graph): term k (0-based) adds cof[k] * INT2.
+__constant__ double c_bch_cof[11] = {1.0, 0.5, 0.166666666666666666, 0.04166666666666666,
+                                     0.0083333333333333333, .001388888888888, 1.984126984e-4, 2.48015873e-5,
+                                     2.755731922e-6, 2.755731922e-7, 2.505210839e-8};
+
 // ---------------------------------------------------------------------------
 // add_arrays (src/ME_general.f90:592-618): c = sa*a + sb*b over the whole
 // vectorize array (E0 included).  double2-vectorised when all three pointers
@@ -193,6 +200,30 @@ int reduce_mbpt2(qd_layout* L, const double* h, double* dout) {
 int reduce_hhtrace(qd_layout* L, const double* h, double* dout) {
   return reduce_to(L, RedHHTrace{L->dev, h}, L->dev.pcnt[0], 1.0, 0.0, dout);
 }
+// BCH_EXPAND's exit test on the device (magnus_IMSRG.f90:316): after the
+// term whose coefficient index is *kidx, continue while
+// |INT2| cof / |INT1| >= conv and fewer than 11 terms ran; the answer sets the
+// graph's loop condition (and, for the first term of a two-term loop body,
+// the condition of the second).  *kidx advances by one.
+__global__ void k_bch_decide(const double* __restrict__ norms, int* __restrict__ kidx, double conv,
+                             cudaGraphConditionalHandle hloop, cudaGraphConditionalHandle hnext, int set_next) {
+  const int k = *kidx;
+  const double cof = c_bch_cof[k];
+  const bool stop = norms[1] * cof / norms[0] < conv;  // NaN continues, as the host test does
+  const unsigned go = (!stop && k + 1 < 11) ? 1u : 0u;
+  *kidx = k + 1;
+  cudaGraphSetConditional(hloop, go);
+  if (set_next) cudaGraphSetConditional(hnext, go);
+}
+
+int launch_bch_decide(qd_layout* L, const double* norms, int* kidx, double conv, cudaGraphConditionalHandle hloop,
+                      cudaGraphConditionalHandle hnext, int set_next) {
+  k_bch_decide<<<1, 1, 0, L->stream>>>(norms, kidx, conv, hloop, hnext, set_next);
+  ++L->nlaunch;
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
 // mat_2_norm (src/ME_general.f90:2112-2138): sqrt of the sum of squares of
 // every stored one- and two-body entry (E0 excluded), sqrt on the device.
 // The entries are summed in vectorize order by the fixed two-stage tree; the
@@ -217,17 +248,40 @@ int reduce_norm(qd_layout* L, const double* a, double* dout) {
 // ---------------------------------------------------------------------------
 constexpr int AXN_BLOCKS = 4 * 148, AXN_THREADS = 256;
 
+
+// 16-byte accesses: the arrays are 16-byte aligned (cudaMalloc) and walked
+// as pairs of entries; entry 0 (E0) is left out of the norms, an odd last
+// entry is handled by thread 0.
 __global__ void __launch_bounds__(AXN_THREADS) k_axpy_norms(const double* __restrict__ a, double sa,
                                                             const double* __restrict__ b, double sb,
                                                             double* __restrict__ c, i64 n, i64 o1,
-                                                            double* __restrict__ partial) {
+                                                            double* __restrict__ partial,
+                                                            const int* __restrict__ kidx) {
   __shared__ double sh[AXN_THREADS / 32];
+  if (kidx) sb = c_bch_cof[*kidx];  // coefficient of the term the device counter names
   double an = 0.0, bn = 0.0;
   const i64 stride = (i64)gridDim.x * blockDim.x;
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const double x = a[i], y = b[i];
-    c[i] = __dadd_rn(__dmul_rn(sa, x), __dmul_rn(sb, y));
-    if (i >= o1) {
+  const i64 n2 = n >> 1;
+  const double2* a2 = reinterpret_cast<const double2*>(a);
+  const double2* b2 = reinterpret_cast<const double2*>(b);
+  double2* c2 = reinterpret_cast<double2*>(c);
+  for (i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += stride) {
+    const double2 x = a2[j], y = b2[j];
+    c2[j] = make_double2(__dadd_rn(__dmul_rn(sa, x.x), __dmul_rn(sb, y.x)),
+                         __dadd_rn(__dmul_rn(sa, x.y), __dmul_rn(sb, y.y)));
+    if (2 * j >= o1) {
+      an += x.x * x.x;
+      bn += y.x * y.x;
+    }
+    if (2 * j + 1 >= o1) {
+      an += x.y * x.y;
+      bn += y.y * y.y;
+    }
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const double x = a[n - 1], y = b[n - 1];
+    c[n - 1] = __dadd_rn(__dmul_rn(sa, x), __dmul_rn(sb, y));
+    if (n - 1 >= o1) {
       an += x * x;
       bn += y * y;
     }
@@ -256,12 +310,16 @@ __global__ void k_axpy_norms_final(const double* __restrict__ partial, int np, d
 }
 
 int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c,
-                      double* dout2) {
+                      double* dout2, const int* kidx) {
   if (!L->d_axn) {
     QD_CUDA(cudaMalloc(&L->d_axn, sizeof(double) * 2 * AXN_BLOCKS));
     L->ws_bytes += sizeof(double) * 2 * AXN_BLOCKS;
   }
-  k_axpy_norms<<<AXN_BLOCKS, AXN_THREADS, 0, L->stream>>>(a, sa, b, sb, c, L->neq, L->o_fhh, L->d_axn);
+  if ((((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15) != 0) {
+    set_error("launch_axpy_norms: operator arrays must be 16-byte aligned");
+    return QD_ERR_ARG;
+  }
+  k_axpy_norms<<<AXN_BLOCKS, AXN_THREADS, 0, L->stream>>>(a, sa, b, sb, c, L->neq, L->o_fhh, L->d_axn, kidx);
   k_axpy_norms_final<<<1, RED_THREADS, 0, L->stream>>>(L->d_axn, AXN_BLOCKS, dout2);
   L->nlaunch += 2;
   QD_CUDA(cudaGetLastError());

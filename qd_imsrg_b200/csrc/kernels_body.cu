@@ -52,10 +52,18 @@ __device__ __forceinline__ unsigned part_bit_of(int c1, int c2) {
   return 1u << part;
 }
 
-__global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, const double* __restrict__ B, double hB,
-                      unsigned zA, unsigned zB, const int* __restrict__ flag, double* __restrict__ C) {
+// One warp per target: the lanes split the (hole, particle) column sums of
+// the target's cross-coupled blocks and a fixed shuffle tree adds them (only
+// the targets of flagged blocks do work, about 2,900 of 176,400 at N=20,
+// R=20 for (m_l, m_s)-conserving operators, so one thread per target would
+// leave most SMs idle).
+constexpr int T121 = 256;
+__global__ void __launch_bounds__(T121) k_121(DevLayout L, const double* __restrict__ A, double hA,
+                                              const double* __restrict__ B, double hB, unsigned zA, unsigned zB,
+                                              const int* __restrict__ flag, double* __restrict__ C) {
   const i64 n1 = (i64)L.n * L.n + (i64)L.mp * L.mp + (i64)L.mp * L.n;
-  i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const i64 t = ((i64)blockIdx.x * T121 + threadIdx.x) >> 5;  // warp-uniform
+  const int lane = threadIdx.x & 31;
   if (t >= n1) return;
   int x, y;
   decode1b(L.n, L.mp, t, x, y);
@@ -70,29 +78,30 @@ __global__ void k_121(DevLayout L, const double* __restrict__ A, double hA, cons
   const unsigned part2 = part_bit_of(px ? 1 : 0, py ? 2 : 1);  // <i x|a y>
   const bool b1 = !(zB & part1), a1 = !(zA & part1), b2 = !(zB & part2), a2 = !(zA & part2);
   double s = 0.0;
-  if (on1) {
-    int base = __ldg(&L.cchp_base[q1]), nb = __ldg(&L.ccdim[q1]).y;
-    for (int k = 0; k < nb; ++k) {
-      int2 ia = __ldg(&L.cchp[base + k]);
+  if (on1 && (a1 || b1)) {
+    const int base = __ldg(&L.cchp_base[q1]), nb = __ldg(&L.ccdim[q1]).y;
+    for (int k = lane; k < nb; k += 32) {
+      const int2 ia = __ldg(&L.cchp[base + k]);
       const int i = ia.x, a = ia.y;
-      double fa = A[L.o_fph + (a - n) + (i64)i * mp], fb = B[L.o_fph + (a - n) + (i64)i * mp];
+      const double fa = A[L.o_fph + (a - n) + (i64)i * mp], fb = B[L.o_fph + (a - n) + (i64)i * mp];
       const double tb = b1 ? fa * hA * dv_elem(L, B, hB, a, x, i, y) : 0.0;
       const double ta = a1 ? fb * hB * dv_elem(L, A, hA, a, x, i, y) : 0.0;
       s += tb - ta;
     }
   }
-  if (on2) {
-    int base = __ldg(&L.cchp_base[q2]), nb = __ldg(&L.ccdim[q2]).y;
-    for (int k = 0; k < nb; ++k) {
-      int2 ia = __ldg(&L.cchp[base + k]);
+  if (on2 && (a2 || b2)) {
+    const int base = __ldg(&L.cchp_base[q2]), nb = __ldg(&L.ccdim[q2]).y;
+    for (int k = lane; k < nb; k += 32) {
+      const int2 ia = __ldg(&L.cchp[base + k]);
       const int i = ia.x, a = ia.y;
-      double fa = A[L.o_fph + (a - n) + (i64)i * mp], fb = B[L.o_fph + (a - n) + (i64)i * mp];
+      const double fa = A[L.o_fph + (a - n) + (i64)i * mp], fb = B[L.o_fph + (a - n) + (i64)i * mp];
       const double tb = b2 ? -fa * dv_elem(L, B, hB, i, x, a, y) : 0.0;
       const double ta = a2 ? fb * dv_elem(L, A, hA, i, x, a, y) : 0.0;
       s += tb + ta;
     }
   }
-  C[L.o_fhh + t] += s;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) C[L.o_fhh + t] += s;
 }
 
 int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
@@ -110,9 +119,9 @@ int launch_121(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
     k_ccflag<<<(nhp + 255) / 256, 256, 0, L->stream>>>(L->dev, A->d, B->d, L->d_ccflag);
     ++L->nlaunch;
   }
-  k_121<<<(unsigned)((n1 + 127) / 128), 128, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d, (double)B->herm,
-                                                             A->zero_mask, B->zero_mask,
-                                                             L->d_ccflag, C);
+  k_121<<<(unsigned)((n1 * 32 + T121 - 1) / T121), T121, 0, L->stream>>>(L->dev, A->d, (double)A->herm, B->d,
+                                                                         (double)B->herm, A->zero_mask, B->zero_mask,
+                                                                         L->d_ccflag, C);
   ++L->nlaunch;
   QD_CUDA(cudaGetLastError());
   return QD_OK;
@@ -275,32 +284,152 @@ __device__ __forceinline__ double w221(const DevLayout& L, int which, const doub
   return sgn * w221_stored(L, which, q, sl, i1, i2, A, B, zA, zB);
 }
 
+// Term descriptor of one w221 read: the stored element (which, q, slot, r, c)
+// of intermediate `which`, or none; the dot product that forms it is
+// resolved by w221_dot.
+struct W221Term {
+  int q, sl, r, c;  // sl < 0: the read is an exact zero
+  int which;
+};
+
+__device__ __forceinline__ W221Term w221_term(const DevLayout& L, int which, unsigned zA, unsigned zB, int a, int b,
+                                              int c, int d, double& sgn) {
+  W221Term t{0, -1, 0, 0, which};
+  sgn = 0.0;
+  if (a == b || c == d) return t;
+  const int e1 = __ldg(&L.ptab[a * L.m + b]);
+  const int e2 = __ldg(&L.ptab[c * L.m + d]);
+  const int q = pt_blk(e1);
+  if (q != pt_blk(e2)) return t;
+  sgn = (pt_swap(e1) ^ pt_swap(e2)) ? -1.0 : 1.0;
+  int c1 = pt_cls(e1), c2 = pt_cls(e2), i1 = pt_idx(e1), i2 = pt_idx(e2);
+  if (c1 < c2) {  // upper class: herm (+1) times the transposed stored element
+    int x = c1; c1 = c2; c2 = x;
+    x = i1; i1 = i2; i2 = x;
+  }
+  int sl;
+  if (c1 == 0) sl = 0;
+  else if (c1 == 1) sl = c2 == 0 ? 5 : 3;
+  else sl = c2 == 0 ? 2 : (c2 == 1 ? 4 : 1);
+  // parts of the operands the product reads (as in w221_stored)
+  const unsigned pphh = 1u << P_PPHH, ppph = 1u << P_PPPH, phhh = 1u << P_PHHH;
+  unsigned za = 0, zb = 0;
+  bool live = true;
+  if (which == 1) {
+    switch (sl) {
+      case 0: case 1: za = pphh; zb = pphh; break;
+      case 3: za = ppph; zb = ppph; break;
+      case 5: za = pphh; zb = ppph; break;
+      case 4: za = pphh; zb = phhh; break;
+      default: live = false; break;
+    }
+  } else {
+    switch (sl) {
+      case 3: za = phhh; zb = phhh; break;
+      case 5: za = ppph; zb = pphh; break;
+      case 4: za = phhh; zb = pphh; break;
+      default: live = false; break;
+    }
+  }
+  if (!live || ((zA & za) | (zB & zb))) return t;
+  t.q = q;
+  t.sl = sl;
+  t.r = i1;
+  t.c = i2;
+  return t;
+}
+
+// The dot product of w221_stored for term t: u[k * su] v[k * sv], k < K.
+__device__ __forceinline__ void w221_dot(const DevLayout& L, const W221Term& t, const double* __restrict__ A,
+                                         const double* __restrict__ B, const double*& u, const double*& v, int& K,
+                                         int& su, int& sv) {
+  const int4 bd = __ldg(&L.blk[t.q]);
+  const int nh = bd.x, nb = bd.y, np = bd.z;
+  const i64* o = L.boff + 6 * t.q;
+  const int r = t.r, c = t.c;
+  if (t.which == 1) {
+    switch (t.sl) {
+      case 0: u = B + __ldg(o + 2) + (i64)r * np; v = A + __ldg(o + 2) + (i64)c * np; K = np; su = sv = 1; break;
+      case 1: u = A + __ldg(o + 2) + r; v = B + __ldg(o + 2) + c; K = nh; su = sv = np; break;
+      case 3: u = B + __ldg(o + 4) + (i64)r * np; v = A + __ldg(o + 4) + (i64)c * np; K = np; su = sv = 1; break;
+      case 5: u = B + __ldg(o + 4) + (i64)r * np; v = A + __ldg(o + 2) + (i64)c * np; K = np; su = sv = 1; break;
+      default: u = A + __ldg(o + 2) + r; v = B + __ldg(o + 5) + c; K = nh; su = np; sv = nb; break;  // 4
+    }
+  } else {
+    switch (t.sl) {
+      case 3: u = A + __ldg(o + 5) + r; v = B + __ldg(o + 5) + c; K = nh; su = sv = nb; break;
+      case 5: u = A + __ldg(o + 4) + (i64)r * np; v = B + __ldg(o + 2) + (i64)c * np; K = np; su = sv = 1; break;
+      default: u = B + __ldg(o + 2) + r; v = A + __ldg(o + 5) + c; K = nh; su = np; sv = nb; break;  // 4
+    }
+  }
+}
+
+// One CTA per target whose two states share (m_l, m_s).  Phase 1: thread u
+// resolves the two w221 reads of leg state u into term descriptors and
+// coefficients (shared memory).  Phase 2: the CTA walks the live terms in
+// order; thread k takes the elements k, k + T221, ... of every term's dot
+// product (long ones run over up to n_p = 1,264 entries); one block sum at
+// the end.  Fixed assignment and order: deterministic.
 constexpr int T221 = 128;
 
 __global__ void __launch_bounds__(T221) k_221_fused(DevLayout L, const int* __restrict__ targets, double hA,
                                                     double hB, const double* __restrict__ A,
                                                     const double* __restrict__ B, unsigned zA, unsigned zB,
                                                     double* __restrict__ C) {
-  __shared__ double sh[T221 / 32];
+  extern __shared__ double sh221[];
+  double* coef = sh221;                                      // [2m]
+  int4* term = reinterpret_cast<int4*>(sh221 + 2 * L.m);     // [2m]: {q | which << 16, sl, r, c}
+  __shared__ double red[T221 / 32];
   const int n = L.n, mp = L.mp, m = L.m;
   const i64 nhh = (i64)n * n, npp = (i64)mp * mp;
   const i64 t = __ldg(targets + blockIdx.x);
   int x, y;
   decode1b(n, mp, t, x, y);
-  double s = 0.0;
   for (int u = threadIdx.x; u < m; u += T221) {
+    // the two reads of leg state u and their coefficients (commutators.f90:280-348)
+    int w0, w1;
+    int a0, b0, c0, d0, a1, b1, c1, d1;
+    double f0, f1;
     if (t < nhh) {  // fhh(h,h2): x = h, y = h2
-      if (u < n) s += hA * w221(L, 1, A, B, zA, zB, u, y, u, x) - hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
-      else s += -hA * w221(L, 2, A, B, zA, zB, u, y, u, x) + hB * w221(L, 2, A, B, zA, zB, u, x, u, y);
+      w0 = w1 = u < n ? 1 : 2;
+      a0 = u; b0 = y; c0 = u; d0 = x; a1 = u; b1 = x; c1 = u; d1 = y;
+      f0 = u < n ? hA : -hA;
+      f1 = u < n ? -hB : hB;
     } else if (t < nhh + npp) {  // fpp(p,p2)
-      if (u < n) s += hA * w221(L, 1, A, B, zA, zB, u, y, u, x) - hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
-      else s += -hA * w221(L, 1, A, B, zA, zB, u, y, u, x) + hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
+      w0 = w1 = 1;
+      a0 = u; b0 = y; c0 = u; d0 = x; a1 = u; b1 = x; c1 = u; d1 = y;
+      f0 = u < n ? hA : -hA;
+      f1 = u < n ? -hB : hB;
     } else {  // fph(p,h)
-      if (u < n) s += hA * w221(L, 2, A, B, zA, zB, u, x, u, y) - hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
-      else s += -hA * w221(L, 2, A, B, zA, zB, u, x, u, y) + hB * w221(L, 1, A, B, zA, zB, u, x, u, y);
+      w0 = 2;
+      w1 = 1;
+      a0 = u; b0 = x; c0 = u; d0 = y; a1 = u; b1 = x; c1 = u; d1 = y;
+      f0 = u < n ? hA : -hA;
+      f1 = u < n ? -hB : hB;
     }
+    double s0, s1;
+    const W221Term t0 = w221_term(L, w0, zA, zB, a0, b0, c0, d0, s0);
+    const W221Term t1 = w221_term(L, w1, zA, zB, a1, b1, c1, d1, s1);
+    term[2 * u] = make_int4(t0.q | (t0.which << 16), t0.sl, t0.r, t0.c);
+    term[2 * u + 1] = make_int4(t1.q | (t1.which << 16), t1.sl, t1.r, t1.c);
+    coef[2 * u] = f0 * s0;
+    coef[2 * u + 1] = f1 * s1;
   }
-  s = block_sum<T221>(s, sh);
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < 2 * m; ++k) {
+    const int4 d = term[k];
+    if (d.y < 0) continue;  // uniform: every thread reads the same descriptor
+    W221Term tt{d.x & 0xFFFF, d.y, d.z, d.w, d.x >> 16};
+    const double* u;
+    const double* v;
+    int K, su, sv;
+    w221_dot(L, tt, A, B, u, v, K, su, sv);
+    double p = 0.0;
+    for (int j = threadIdx.x; j < K; j += T221) p += u[(i64)j * su] * v[(i64)j * sv];
+    s += coef[k] * p;
+  }
+  s = block_sum<T221>(s, red);
   if (threadIdx.x == 0) C[L.o_fhh + t] += s;
 }
 
@@ -321,8 +450,10 @@ int launch_221_fused(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
     L->ntgt221 = (int)tg.size();
   }
   if (L->ntgt221 > 0) {
-    k_221_fused<<<L->ntgt221, T221, 0, L->stream>>>(L->dev, L->d_tgt221, (double)A->herm, (double)B->herm, A->d,
-                                                   B->d, A->zero_mask, B->zero_mask, C);
+    const size_t smem = (sizeof(double) + sizeof(int4)) * 2 * (size_t)L->m;
+    if (smem > 48 * 1024) QD_CUDA(cudaFuncSetAttribute(k_221_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_221_fused<<<L->ntgt221, T221, smem, L->stream>>>(L->dev, L->d_tgt221, (double)A->herm, (double)B->herm,
+                                                      A->d, B->d, A->zero_mask, B->zero_mask, C);
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());

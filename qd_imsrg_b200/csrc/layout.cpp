@@ -284,11 +284,13 @@ int layout_upload(qd_layout* L) {
 void GemmProgram::clear_device() {
   if (d_probs) cudaFree(d_probs);
   if (d_segs) cudaFree(d_segs);
-  for (auto& kv : tasks)
-    if (kv.second.first) cudaFree(kv.second.first);
+  for (auto* m : {&tasks, &tasks_short})
+    for (auto& kv : *m)
+      if (kv.second.first) cudaFree(kv.second.first);
   d_probs = nullptr;
   d_segs = nullptr;
   tasks.clear();
+  tasks_short.clear();
 }
 
 void layout_free_device(qd_layout* L) {

@@ -99,8 +99,9 @@ struct GemmProgram {
   std::vector<GSeg> segs;
   GProb* d_probs = nullptr;
   GSeg* d_segs = nullptr;
-  // task lists cached per (maskA, maskB)
-  std::map<std::pair<unsigned, unsigned>, std::pair<GTask*, int>> tasks;
+  // task lists cached per (maskA, maskB): problems with a long K, and
+  // K-short problems (every active segment together K <= 16)
+  std::map<std::pair<unsigned, unsigned>, std::pair<GTask*, int>> tasks, tasks_short;
   void clear_device();
 };
 
@@ -161,7 +162,8 @@ struct qd_layout {
   void* split = nullptr;  // plans and workspaces (split_gemm.cu)
   // BCH terms replayed as CUDA graphs (api.cu)
   bool use_graphs = true;
-  void* graphs = nullptr;
+  void* graphs = nullptr;       // per-term graphs
+  void* step_graphs = nullptr;  // whole BCH steps with the truncation decided on the device
   long long graphs_captured = 0, graph_replays = 0;
 };
 
@@ -203,7 +205,13 @@ i64 part_count(const qd_layout* L, int part);  // total elements of a part over 
 // kernels (kernels_*.cu)
 int launch_axpy(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c, i64 n);
 int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b, double sb, double* c,
-                      double* dout2);
+                      double* dout2, const int* kidx = nullptr);
+int launch_bch_decide(qd_layout* L, const double* norms, int* kidx, double conv, cudaGraphConditionalHandle hloop,
+                      cudaGraphConditionalHandle hnext, int set_next);
+int prepare_program(qd_layout* L, GemmProgram& P, unsigned maskA, unsigned maskB);
+int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B);
+std::string tuning_report_122(const qd_layout* L);
+double* scratch_operator(qd_layout* L);
 int reduce_dot_range(qd_layout* L, const double* a, const double* b, i64 o, i64 n, double scale, double add,
                      double* dout);
 int reduce_dot_part(qd_layout* L, const double* a, const double* b, int part, double scale, double add, double* dout);
