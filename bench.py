@@ -645,6 +645,15 @@ def run_batch(args, world, rank, local):
     t_sep = time.perf_counter() - t0
     good = [d for d in inst if d["ok"]]
     pairs = [(d["H"], d["HS"]) for d in good]
+    # the thread-per-instance stream mode, for comparison (outside the timed region)
+    for _ in range(max(1, args.warmup - 1)):
+        qd.magnus_flow_batch(pairs, raise_on_error=False, streams=True, **kw)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    res_s, st_s = qd.magnus_flow_batch(pairs, raise_on_error=False, streams=True, **kw)
+    torch.cuda.synchronize(device)
+    t_streams = time.perf_counter() - t0
+    # lockstep: one launch per kernel over all instances' tiles (timed)
     for _ in range(max(0, args.warmup - 1)):
         qd.magnus_flow_batch(pairs, raise_on_error=False, **kw)
     clocks = ClockSampler(local)
@@ -658,10 +667,11 @@ def run_batch(args, world, rank, local):
     t_batch = (time.perf_counter() - t0) / args.steps
     clk = clocks.stop()
     t_batch = max_over_ranks(t_batch, world, device)
-    worst = 0.0
-    for d, r, s_ in zip(good, res, st):
+    worst = worst_s = 0.0
+    for d, r, s_, rs in zip(good, res, st, res_s):
         d["E_batch"], d["status"] = float(r.E0), s_
         worst = max(worst, abs(d["E_batch"] - d["E_sep"]))
+        worst_s = max(worst_s, abs(float(rs.E0) - d["E_sep"]))
     if rank == 0:
         per = [{k: d[k] for k in ("N", "hw", "R", "E_HF", "E_sep", "E_batch", "steps") if k in d} for d in good]
         fails = [{"N": d["N"], "hw": d["hw"], "R": d["R"], "why": d["why"]} for d in inst if not d["ok"]]
@@ -670,10 +680,13 @@ def run_batch(args, world, rank, local):
                 "ms_per_step": 1e3 * t_batch, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
                 "config": {"workload": "batched Magnus IM-SRG(2) flows, N in {6,12,20,30} x hbar-omega in "
-                                       "{0.1,0.28,0.5,1.0}, R=16 for N<=12 else 20, %s" %
-                                       ("particle-hole channel on" if args.pandya else "ladders only"),
+                                       "{0.1,0.28,0.5,1.0}, R=16 for N<=12 else 20, %s; lockstep, each BCH "
+                                       "term's 122 tiles and ladder tasks of all instances in one launch per "
+                                       "kernel" % ("particle-hole channel on" if args.pandya else "ladders only"),
                            "separate_s": t_sep, "speedup_vs_separate": t_sep / t_batch,
-                           "max_abs_dE_batch_vs_separate": worst, "instances": per, "flow_failed": fails,
+                           "streams_s": t_streams, "speedup_vs_streams": t_streams / t_batch,
+                           "max_abs_dE_batch_vs_separate": worst, "max_abs_dE_streams_vs_separate": worst_s,
+                           "instances": per, "flow_failed": fails,
                            "hf_failed": skipped, "setup_s": setup_s},
                 "clocks": clk}
         print(json.dumps(line), flush=True)

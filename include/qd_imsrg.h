@@ -307,10 +307,17 @@ int qd_flow_omega(const qd_flow* flow, qd_op** G);
 int qd_flow_state(const qd_flow* flow, qd_flow_result* result);
 int qd_flow_destroy(qd_flow* flow);
 /* Several independent flows (e.g. a grid of (N, hbar-omega, emax)), one per
- * layout, run concurrently: one host thread per instance, each on its own
- * layout's stream.  No reference counterpart (the reference runs one flow per
- * process).  status[i] is instance i's qd_magnus_flow code; the call returns
- * the first failing one (and names the instance in qd_last_error).          */
+ * layout.  Default: the instances advance in lockstep on one stream, and each
+ * BCH term's commutator_122 tiles and ladder GEMM tasks of every instance
+ * whose series is still running go into one launch per kernel (uneven blocks
+ * of all instances in one task list, longest first); the small stages run
+ * per instance.  flags | QD_BATCH_STREAMS instead runs one host thread per
+ * instance on its own layout's stream (each flow as qd_magnus_flow, BCH steps
+ * as graphs).  Results equal the separate flows'.  No reference counterpart
+ * (the reference runs one flow per process).  status[i] is instance i's
+ * code; the call returns the first failing one (and names the instance in
+ * qd_last_error).                                                           */
+#define QD_BATCH_STREAMS 4u
 int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, unsigned flags, int max_iter,
                          qd_flow_result* results, int* status);
 

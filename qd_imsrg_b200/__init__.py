@@ -25,10 +25,10 @@ import os
 import numpy as np
 
 from . import _native
-from ._native import QD_PANDYA, QD_TBME_QUAD, FlowResult, FlowStepInfo, QDError, check, lib
+from ._native import QD_BATCH_STREAMS, QD_PANDYA, QD_TBME_QUAD, FlowResult, FlowStepInfo, QDError, check, lib
 
 __all__ = [
-    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA",
+    "Layout", "FullHam", "CCMat", "QDError", "QD_PANDYA", "QD_BATCH_STREAMS",
     "commutator_110", "commutator_220", "commutator_111", "commutator_121", "commutator_221",
     "commutator_122", "commutator_222", "commutator", "calc_cc", "build_white", "add_arrays",
     "copy_arrays", "set_to_zero", "mat_2_norm", "mbpt2", "hf_e2", "bch_expand", "magnus_expand",
@@ -429,16 +429,20 @@ class DeviceView:
         return {"shape": (self.n,), "typestr": "<f8", "data": (self.ptr, False), "version": 3, "strides": None}
 
 
-def magnus_flow_batch(pairs, pandya: bool = False, max_iter: int = 500, raise_on_error: bool = True):
-    """Run several independent flows concurrently: pairs = [(HAM, HS), ...],
-    each pair on its own layout.  Returns ([FlowResult], [status]); with
+def magnus_flow_batch(pairs, pandya: bool = False, max_iter: int = 500, raise_on_error: bool = True,
+                      streams: bool = False):
+    """Run several independent flows: pairs = [(HAM, HS), ...], each pair on
+    its own layout.  Default: lockstep, each BCH term's 122 tiles and ladder
+    tasks of all instances in one launch per kernel; streams=True: one host
+    thread and stream per instance.  Returns ([FlowResult], [status]); with
     raise_on_error, raises QDError for the first failing instance."""
     n = len(pairs)
     hams = (C.c_void_p * n)(*[h.h.value for h, _ in pairs])
     hss = (C.c_void_p * n)(*[s.h.value for _, s in pairs])
     res = (FlowResult * n)()
     st = (C.c_int * n)()
-    rc = lib().qd_magnus_flow_batch(n, hams, hss, _flags(pandya), int(max_iter), res, st)
+    flags = _flags(pandya) | (QD_BATCH_STREAMS if streams else 0)
+    rc = lib().qd_magnus_flow_batch(n, hams, hss, flags, int(max_iter), res, st)
     out = [res[i] for i in range(n)], [int(st[i]) for i in range(n)]
     if raise_on_error:
         check(rc)

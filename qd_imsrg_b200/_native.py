@@ -22,6 +22,7 @@ _vpp = C.POINTER(C.c_void_p)
 
 QD_OK = 0
 QD_PANDYA = 1
+QD_BATCH_STREAMS = 4
 QD_TBME_QUAD = 1
 QD_NSTAGE = 10
 STAGES = ["E0", "c111", "c121", "c221", "c122", "calc_cc", "ladder_gemm", "pandya_gemm", "pandya_gather", "glue"]

@@ -82,6 +82,8 @@ int op_new(qd_layout* L, int herm, qd_op** out) {
 
 // Tear down a layout's device state and the layout itself.
 void layout_finish(qd_layout* L) {
+  drop_merged_gemm(L);
+  drop_merged_122(L);
   drop_122_plan(L);
   layout_free_device(L);
   delete L;
@@ -1368,19 +1370,21 @@ int qd_flow_warm_start(qd_flow* f, const qd_op* G, double s) {
   return QD_OK;
 }
 
-int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
-  CHECK(f, QD_ERR_ARG, "qd_flow_step: null flow");
-  qd_layout* L = f->L;
-  TRY(use_device(L));
-  qd_flow_step_info inf;
-  std::memset(&inf, 0, sizeof(inf));
-  if (f->crit <= kConvCriteria) {  // converged: nothing to do
-    inf.s = f->s;
-    inf.E0 = f->E0;
-    inf.nrm1 = f->nrm1;
-    inf.crit = f->crit;
-    inf.converged = 1;
-    if (info) *info = inf;
+}  // extern "C"
+
+namespace {
+// s_evolve's loop body in two halves around BCH_EXPAND (the batched flows run
+// the BCH of several instances between them).  flow_begin returns
+// *converged = true (and fills info) when there is nothing to do.
+int flow_begin(qd_flow* f, qd_flow_step_info* inf, bool* converged) {
+  std::memset(inf, 0, sizeof(*inf));
+  *converged = f->crit <= kConvCriteria;
+  if (*converged) {
+    inf->s = f->s;
+    inf->E0 = f->E0;
+    inf->nrm1 = f->nrm1;
+    inf->crit = f->crit;
+    inf->converged = 1;
     return QD_OK;
   }
   // G0 = G; MAGNUS_EXPAND: DG = ETA; euler_step: G = G + stp DG.  G and G0
@@ -1390,8 +1394,10 @@ int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
   TRY(qd_add_arrays(f->G0, 1.0, f->ETA, f->stp, f->G));
   f->s = f->s + f->stp;
   swap_ops(f->HS, f->HS0);  // HS0 = HS: BCH_EXPAND rewrites every entry of HS
-  int terms = 0;
-  TRY(qd_bch_expand(f->HS, f->G, f->HAM, f->INT1, f->INT2, f->AD, f->w1, f->w2, f->HCC, f->OCC, f->flags, &terms));
+  return QD_OK;
+}
+
+int flow_end(qd_flow* f, int terms, qd_flow_step_info* inf) {
   f->comms += terms;
   swap_ops(f->ETA, f->ETA0);  // ETA0 = ETA: build_white rewrites fph and Vpphh, the rest stays 0
   TRY(qd_build_white(f->ETA, f->HS));
@@ -1400,12 +1406,12 @@ int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
   TRY(flow_e0(f, &E0));
   CHECK(std::isfinite(E0) && std::isfinite(nrm2), QD_ERR_NAN,
         "qd_flow_step: non-finite energy or generator norm at s = %g", f->s);
-  inf.s = f->s;
-  inf.E0 = E0;
-  inf.nrm1 = f->nrm1;
-  inf.nrm2 = nrm2;
-  inf.crit = f->crit;  // the criterion before this step, as the reference's trace
-  inf.terms = terms;
+  inf->s = f->s;
+  inf->E0 = E0;
+  inf->nrm1 = f->nrm1;
+  inf->nrm2 = nrm2;
+  inf->crit = f->crit;  // the criterion before this step, as the reference's trace
+  inf->terms = terms;
   ++f->rows;
   if (f->nrm1 * 1.5 < nrm2) {  // reject: back to the previous state, smaller step
     ++f->rejected;
@@ -1414,16 +1420,34 @@ int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
     swap_ops(f->HS, f->HS0);
     swap_ops(f->ETA, f->ETA0);
     f->stp = f->stp / 2.0 + (double)1e-3f;
-    inf.accepted = 0;
+    inf->accepted = 0;
   } else {
     double mb;
     TRY(qd_mbpt2(f->HS, &mb));
     f->crit = std::fabs(mb);
     f->E0 = E0;
     f->iteration += 1;
-    inf.accepted = 1;
+    inf->accepted = 1;
   }
-  inf.converged = f->crit <= kConvCriteria ? 1 : 0;
+  inf->converged = f->crit <= kConvCriteria ? 1 : 0;
+  return QD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int qd_flow_step(qd_flow* f, qd_flow_step_info* info) {
+  CHECK(f, QD_ERR_ARG, "qd_flow_step: null flow");
+  TRY(use_device(f->L));
+  qd_flow_step_info inf;
+  bool conv = false;
+  TRY(flow_begin(f, &inf, &conv));
+  if (!conv) {
+    int terms = 0;
+    TRY(qd_bch_expand(f->HS, f->G, f->HAM, f->INT1, f->INT2, f->AD, f->w1, f->w2, f->HCC, f->OCC, f->flags,
+                      &terms));
+    TRY(flow_end(f, terms, &inf));
+  }
   if (info) *info = inf;
   return QD_OK;
 }
@@ -1482,6 +1506,226 @@ int qd_magnus_flow(const qd_op* HAM, qd_op* HS, unsigned flags, int max_iter, do
   return rc;
 }
 
+}  // extern "C"
+
+namespace {
+// ---- batched flows: several instances in lockstep, one launch per stage ---
+// One commutator C = [A, B] per item, every item's layout on the same stream:
+// the small stages (E0, 111, 121, 221, Pandya re-coupling) per item, the
+// 122 tiles and the ladder GEMM tasks of all items in one launch each.
+struct CommItem {
+  qd_layout* L;
+  const qd_op *A, *B;
+  qd_op* C;
+  qd_cc *ACC, *BCC;
+};
+
+// Streams of a lockstep batch: each instance's small stages run on its own
+// layout's stream; the merged launches run on `st` after a join (events) and
+// the instances' streams wait for them before going on.
+struct BatchCtx {
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_st = nullptr;
+  std::map<const qd_layout*, cudaEvent_t> ev;
+};
+
+int join_to(cudaStream_t st, const std::vector<qd_layout*>& Ls, BatchCtx& bc) {
+  for (qd_layout* L : Ls) {
+    cudaEvent_t e = bc.ev[L];
+    QD_CUDA(cudaEventRecord(e, L->stream));
+    QD_CUDA(cudaStreamWaitEvent(st, e, 0));
+  }
+  return QD_OK;
+}
+
+int fork_from(cudaStream_t st, const std::vector<qd_layout*>& Ls, BatchCtx& bc) {
+  QD_CUDA(cudaEventRecord(bc.ev_st, st));
+  for (qd_layout* L : Ls) QD_CUDA(cudaStreamWaitEvent(L->stream, bc.ev_st, 0));
+  return QD_OK;
+}
+
+int commutator_batch(BatchCtx& bc, std::vector<CommItem>& items, bool pandya) {
+  std::vector<Item122> i122;
+  std::vector<GemmItem> gl;
+  std::vector<qd_layout*> Ls;
+  for (CommItem& it : items) {
+    qd_layout* L = it.L;
+    Ls.push_back(L);
+    TRY(build_programs(L));
+    TRY(stage_e0(L, it.A, it.B, it.C->d, 0.0));
+    TRY(stage_111(L, it.A, it.B, it.C));
+    TRY(launch_121(L, it.A, it.B, it.C->d));
+    TRY(launch_221_fused(L, it.A, it.B, it.C->d));
+    if (pandya) {
+      TRY(launch_calc_cc(L, it.A, it.ACC->d));
+      it.ACC->filled = true;
+      it.ACC->herm = it.A->herm;
+      TRY(launch_calc_cc(L, it.B, it.BCC->d));
+      it.BCC->filled = true;
+      it.BCC->herm = it.B->herm;
+    }
+    i122.push_back(Item122{L, it.A, it.B, it.C->d});
+    GemmItem g;
+    g.L = L;
+    g.P = &L->prog_ladder;
+    const double* bufs[NBUF] = {it.A->d, it.B->d, nullptr, nullptr, it.C->d, nullptr, nullptr};
+    for (int k = 0; k < NBUF; ++k) g.bufs[k] = bufs[k];
+    g.hv0 = (double)it.A->herm;
+    g.hv1 = (double)it.B->herm;
+    g.maskA = it.A->zero_mask;
+    g.maskB = it.B->zero_mask;
+    gl.push_back(g);
+  }
+  TRY(join_to(bc.st, Ls, bc));
+  TRY(launch_122_batched(bc.st, i122));
+  TRY(run_programs_batched(bc.st, gl));
+  TRY(fork_from(bc.st, Ls, bc));
+  for (CommItem& it : items) {
+    qd_layout* L = it.L;
+    if (pandya && L->zsize > 0) {  // the particle-hole channel, as stage_222 after its ladders
+      TRY(ensure_z(L));
+      const double* zb[7] = {nullptr, nullptr, it.ACC->d, it.BCC->d, nullptr, nullptr, L->d_z};
+      TRY(run_program(L, L->prog_pandya, zb, it.ACC->herm, it.BCC->herm, 0u, 0u));
+      TRY(launch_pandya_gather(L, L->d_z, it.C->d));
+    }
+    it.C->zero_mask = 0;
+  }
+  return QD_OK;
+}
+
+// BCH_EXPAND of several flows in lockstep: every term is one batched
+// commutator over the instances whose series is still running; the host
+// reads all norms once per term and applies each instance's exit test.
+int bch_batch(BatchCtx& bc, const std::vector<qd_flow*>& fl, std::vector<int>& terms) {
+  const double conv = (double)1e-5f;
+  const bool pandya = fl.empty() ? false : (fl[0]->flags & QD_PANDYA) != 0;
+  std::vector<double*> p0(fl.size());
+  std::vector<int> live;
+  for (size_t j = 0; j < fl.size(); ++j) {
+    qd_flow* f = fl[j];
+    f->INT2->herm = 1;
+    f->AD->herm = 1;
+    TRY(qd_copy_arrays(f->HAM, f->HS));
+    TRY(qd_copy_arrays(f->HS, f->INT2));
+    p0[j] = f->INT2->d;
+    terms[j] = 0;
+    live.push_back((int)j);
+  }
+  for (int i = 2; i <= 12 && !live.empty(); ++i) {
+    const double cof = kCof[i - 2];
+    std::vector<CommItem> items;
+    for (int j : live) {
+      qd_flow* f = fl[j];
+      std::swap(f->INT2->d, f->AD->d);
+      std::swap(f->INT2->zero_mask, f->AD->zero_mask);
+      items.push_back(CommItem{f->L, f->G, f->AD, f->INT2, f->OCC, f->HCC});
+    }
+    TRY(commutator_batch(bc, items, pandya));
+    for (int j : live) {
+      qd_flow* f = fl[j];
+      qd_layout* L = f->L;
+      TRY(launch_axpy_norms(L, f->HS->d, 1.0, f->INT2->d, cof, f->HS->d, red_slot(L, 1)));
+      QD_CUDA(cudaMemcpyAsync(L->h_red + 1, red_slot(L, 1), 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                              L->stream));
+      f->HS->zero_mask &= f->INT2->zero_mask;
+      ++terms[j];
+    }
+    for (int j : live) QD_CUDA(cudaStreamSynchronize(fl[j]->L->stream));
+    std::vector<int> next;
+    for (int j : live) {
+      const double n1 = fl[j]->L->h_red[1], n2 = fl[j]->L->h_red[2];
+      if (!(n2 * cof / n1 < conv)) next.push_back(j);
+    }
+    live.swap(next);
+  }
+  for (size_t j = 0; j < fl.size(); ++j)  // the workspaces keep their buffers
+    if (fl[j]->INT2->d != p0[j]) {
+      std::swap(fl[j]->INT2->d, fl[j]->AD->d);
+      std::swap(fl[j]->INT2->zero_mask, fl[j]->AD->zero_mask);
+    }
+  return QD_OK;
+}
+
+// The lockstep batch: every layout on one stream (restored afterwards); per
+// flow step the instances not yet converged run their step halves and one
+// batched BCH_EXPAND.  An instance that fails or exceeds max_iter leaves the
+// batch with its own status.
+int flow_batch_lockstep(int count, const qd_op* const* HAM, qd_op* const* HS, unsigned flags, int max_iter,
+                        qd_flow_result* results, int* status, std::vector<std::string>& msg) {
+  std::vector<qd_layout*> Ls(count);
+  for (int i = 0; i < count; ++i) {
+    Ls[i] = HAM[i]->L;
+    TRY(use_device(Ls[i]));
+  }
+  BatchCtx bc;
+  QD_CUDA(cudaStreamCreateWithFlags(&bc.st, cudaStreamNonBlocking));
+  QD_CUDA(cudaEventCreateWithFlags(&bc.ev_st, cudaEventDisableTiming));
+  for (qd_layout* L : Ls) {
+    cudaEvent_t e;
+    QD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    bc.ev[L] = e;
+  }
+  std::vector<qd_flow*> fl(count, nullptr);
+  std::vector<int> loops(count, 0);
+  int rc = QD_OK;
+  for (int i = 0; i < count; ++i) {
+    std::memset(&results[i], 0, sizeof(qd_flow_result));
+    status[i] = qd_flow_create(HAM[i], HS[i], flags, &fl[i]);
+    if (status[i] != QD_OK) msg[i] = qd::last_error();
+  }
+  while (rc == QD_OK) {
+    std::vector<qd_flow*> act;
+    std::vector<int> idx;
+    std::vector<qd_flow_step_info> inf(count);
+    for (int i = 0; i < count; ++i) {
+      if (status[i] != QD_OK || !fl[i] || fl[i]->crit <= kConvCriteria) continue;
+      if (loops[i]++ >= max_iter) {
+        status[i] = QD_ERR_NOCONV;
+        char b[128];
+        snprintf(b, sizeof(b), "not converged after %d steps (crit %.3e)", max_iter, fl[i]->crit);
+        msg[i] = b;
+        continue;
+      }
+      bool conv = false;
+      status[i] = flow_begin(fl[i], &inf[i], &conv);
+      if (status[i] != QD_OK) {
+        msg[i] = qd::last_error();
+        continue;
+      }
+      act.push_back(fl[i]);
+      idx.push_back(i);
+    }
+    if (act.empty()) break;
+    std::vector<int> terms(act.size(), 0);
+    rc = bch_batch(bc, act, terms);
+    if (rc) break;
+    for (size_t k = 0; k < act.size(); ++k) {
+      const int i = idx[k];
+      status[i] = flow_end(act[k], terms[k], &inf[i]);
+      if (status[i] != QD_OK) msg[i] = qd::last_error();
+    }
+  }
+  const std::string batch_err = rc ? qd::last_error() : std::string();
+  for (int i = 0; i < count; ++i) {
+    if (fl[i]) {
+      qd_flow_state(fl[i], &results[i]);
+      qd_flow_destroy(fl[i]);
+    }
+    if (rc) {
+      status[i] = rc;
+      msg[i] = batch_err;
+    }
+  }
+  cudaStreamSynchronize(bc.st);
+  for (auto& kv : bc.ev) cudaEventDestroy(kv.second);
+  cudaEventDestroy(bc.ev_st);
+  cudaStreamDestroy(bc.st);
+  return QD_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, unsigned flags, int max_iter,
                          qd_flow_result* results, int* status) {
   CHECK(count >= 0, QD_ERR_ARG, "qd_magnus_flow_batch: negative count");
@@ -1493,9 +1737,22 @@ int qd_magnus_flow_batch(int count, const qd_op* const* HAM, qd_op* const* HS, u
       CHECK(HAM[i]->L != HAM[j]->L, QD_ERR_ARG,
             "qd_magnus_flow_batch: instances %d and %d share a layout (one stream per instance)", j, i);
   }
+  std::vector<std::string> msg(count);
+  bool lockstep = !(flags & QD_BATCH_STREAMS);
+  for (int i = 0; i < count && lockstep; ++i)
+    lockstep = HAM[i]->L->device == HAM[0]->L->device && HAM[i]->L->split_slices == 0 && !HAM[i]->L->prof.on;
+  if (lockstep) {
+    TRY(flow_batch_lockstep(count, HAM, HS, flags & ~QD_BATCH_STREAMS, max_iter, results, status, msg));
+    for (int i = 0; i < count; ++i)
+      if (status[i] != QD_OK) {
+        qd::set_error("qd_magnus_flow_batch: instance %d: %s", i, msg[i].c_str());
+        return status[i];
+      }
+    return QD_OK;
+  }
   // one host thread per instance; each flow runs on its own layout's stream,
   // so the instances' kernels run concurrently on the device
-  std::vector<std::string> msg(count);
+  flags &= ~QD_BATCH_STREAMS;
   std::vector<std::thread> th;
   th.reserve(count);
   for (int i = 0; i < count; ++i)

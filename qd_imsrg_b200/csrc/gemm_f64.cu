@@ -21,6 +21,15 @@
 // tcgen05 has no f64 kind, so mma.sync DMMA is the FP64 tensor path here.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#define TRY_GEMM(x)      \
+  do {                   \
+    int rc_ = (x);       \
+    if (rc_) return rc_; \
+  } while (0)
 
 #include "dev_common.cuh"
 
@@ -31,11 +40,6 @@ constexpr int GEMM_THREADS = 128;
 constexpr int SMEM_PIPE = 2 * NSTAGE * BK * LDS;  // doubles
 constexpr int SMEM_TILE = BN * TLD;               // doubles
 constexpr size_t GEMM_SMEM = sizeof(double) * (SMEM_PIPE + SMEM_TILE);
-constexpr int NBUF = 7;
-
-struct Bufs {
-  const double* p[NBUF];
-};
 
 __device__ __forceinline__ void cp_async8(double* s, const double* g, bool pred) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(s);
@@ -221,8 +225,20 @@ __device__ __forceinline__ void stash(double* T, const double acc[4][4][2]) {
 __global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __restrict__ tasks,
                                                                const GProb* __restrict__ probs,
                                                                const GSeg* __restrict__ segs, Bufs bufs, double hv0,
-                                                               double hv1, unsigned maskA, unsigned maskB) {
+                                                               double hv1, unsigned maskA, unsigned maskB,
+                                                               const int* __restrict__ tinst,
+                                                               const GInst* __restrict__ insts) {
   extern __shared__ double smem[];
+  if (tinst) {  // a task of several instances' programs: this instance's operands
+    const GInst& I = insts[tinst[blockIdx.x]];
+    probs = I.probs;
+    segs = I.segs;
+    bufs = I.bufs;
+    hv0 = I.hv0;
+    hv1 = I.hv1;
+    maskA = I.maskA;
+    maskB = I.maskB;
+  }
   const GTask t = tasks[blockIdx.x];
   const GProb P = probs[t.prob];
   double* out = const_cast<double*>(bufs.p[P.outbuf]) + P.offC;
@@ -315,12 +331,15 @@ __global__ void __launch_bounds__(GEMM_THREADS) k_grouped_gemm(const GTask* __re
 // ladders become rank-n_h updates, n_h <= 16).  Such a tile is one read-
 // modify-write of C: no pipeline, the panels of all segments are staged once
 // (alpha folded in), the two products of a pair tile are formed from four
-// panels, and the shared memory is reused for the transpose stash, so that
-// six CTAs of eight warps fit on an SM.
+// panels, and the shared memory is reused for the two transpose stashes
+// (66.5 KB per CTA: three CTAs of eight warps on an SM).
 // ---------------------------------------------------------------------------
 constexpr int KS_K = 16, KS_THREADS = 256, KS_LDS = 68;
 constexpr int KS_PANEL = KS_K * KS_LDS;                            // doubles per panel
-constexpr size_t KS_SMEM = sizeof(double) * (4 * KS_PANEL > BN * TLD ? 4 * KS_PANEL : BN * TLD);
+// shared memory: stash 1 [BN*TLD] | panels A1 B1 A2 B2 (stash 2 overlaps the panels once the products are done)
+constexpr int KS_PANEL0 = BN * TLD;
+constexpr size_t KS_SMEM = sizeof(double) * (KS_PANEL0 + 4 * KS_PANEL > 2 * BN * TLD ? KS_PANEL0 + 4 * KS_PANEL
+                                                                                      : 2 * BN * TLD);
 
 // panel of op(A) rows [row0, row0+64) (sA[k][m]) and op(B) columns
 // [col0, col0+64) (sB[k][n]) over the concatenated active segments; zeros
@@ -392,9 +411,21 @@ __device__ __forceinline__ void ks_stash(double* T, const double acc[4][2][2]) {
 __global__ void __launch_bounds__(KS_THREADS, 3) k_gemm_kshort(const GTask* __restrict__ tasks,
                                                             const GProb* __restrict__ probs,
                                                             const GSeg* __restrict__ segs, Bufs bufs, double hv0,
-                                                            double hv1, unsigned maskA, unsigned maskB) {
+                                                            double hv1, unsigned maskA, unsigned maskB,
+                                                            const int* __restrict__ tinst,
+                                                            const GInst* __restrict__ insts) {
   extern __shared__ double smem[];
   __shared__ SegList sl;
+  if (tinst) {  // a task of several instances' programs: this instance's operands
+    const GInst& I = insts[tinst[blockIdx.x]];
+    probs = I.probs;
+    segs = I.segs;
+    bufs = I.bufs;
+    hv0 = I.hv0;
+    hv1 = I.hv1;
+    maskA = I.maskA;
+    maskB = I.maskB;
+  }
   const GTask t = tasks[blockIdx.x];
   const GProb P = probs[t.prob];
   double* out = const_cast<double*>(bufs.p[P.outbuf]) + P.offC;
@@ -417,10 +448,10 @@ __global__ void __launch_bounds__(KS_THREADS, 3) k_gemm_kshort(const GTask* __re
   const bool pair = P.mode == GM_ACC_PAIR || P.mode == GM_SET_PAIR;
   const bool acc_mode = P.mode == GM_ACC || P.mode == GM_ACC_PAIR;
   const int r0 = t.ti * BM, c0 = t.tj * BN;
-  double* pA1 = smem;
-  double* pB1 = smem + KS_PANEL;
-  double* T = smem;  // stash, after the products
-  double v1[4][2][2], v2[4][2][2];
+  double* pA1 = smem + KS_PANEL0;
+  double* pB1 = pA1 + KS_PANEL;
+  double* T = smem;  // stash 1: below the panels
+  double v1[4][2][2];
   if (!pair || t.ti == t.tj) {
     ks_panels(sl, P.M, P.N, r0, c0, pA1, pB1);
     ks_mma(pA1, pB1, v1);
@@ -429,51 +460,70 @@ __global__ void __launch_bounds__(KS_THREADS, 3) k_gemm_kshort(const GTask* __re
     __syncthreads();
     const double sigma = pair ? P.sc * (P.spa ? hv0 : 1.0) * (P.spb ? hv1 : 1.0) : 0.0;
     const int mr = min(BM, P.M - r0), nc = min(BN, P.N - c0);
-    for (int idx = threadIdx.x; idx < BM * BN; idx += KS_THREADS) {
-      const int r = idx & (BM - 1), c = idx >> 6;
-      if (r < mr && c < nc) {
-        double* p = out + (r0 + r) + (i64)(c0 + c) * P.ldc;
-        const double v = pair ? T[c * TLD + r] + sigma * T[r * TLD + c] : T[c * TLD + r];
-        *p = acc_mode ? *p + v : v;
+    // read-modify-write of C: a thread's loads of a chunk first, then the stores
+    constexpr int PER = BM * BN / KS_THREADS, CH = 8;
+#pragma unroll
+    for (int k0 = 0; k0 < PER; k0 += CH) {
+      double cv[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const int idx = threadIdx.x + (k0 + k) * KS_THREADS, r = idx & (BM - 1), c = idx >> 6;
+        cv[k] = (acc_mode && r < mr && c < nc) ? out[(r0 + r) + (i64)(c0 + c) * P.ldc] : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const int idx = threadIdx.x + (k0 + k) * KS_THREADS, r = idx & (BM - 1), c = idx >> 6;
+        if (r < mr && c < nc) {
+          const double v = pair ? T[c * TLD + r] + sigma * T[r * TLD + c] : T[c * TLD + r];
+          out[(r0 + r) + (i64)(c0 + c) * P.ldc] = acc_mode ? cv[k] + v : v;
+        }
       }
     }
     return;
   }
-  // off-diagonal tile pair: V(I,J) = A_I B_J^T and V(J,I) = A_J B_I^T;
-  // C(I,J) = V(I,J) + sigma V(J,I)^T and C(J,I) = V(J,I) + sigma V(I,J)^T,
-  // each formed in the fragment layout against the other product's stash
-  double* pA2 = smem + 2 * KS_PANEL;
-  double* pB2 = smem + 3 * KS_PANEL;
+  // off-diagonal tile pair: V(I,J) = A_I B_J^T and V(J,I) = A_J B_I^T, each
+  // stashed right after its product (one accumulator live at a time), then
+  // C(I,J) = V(I,J) + sigma V(J,I)^T and C(J,I) = V(J,I) + sigma V(I,J)^T
+  // written column by column
+  double* pA2 = pB1 + KS_PANEL;
+  double* pB2 = pA2 + KS_PANEL;
+  double* T1 = smem;
+  double* T2 = smem + BN * TLD;  // overlaps the panels: written after every product is done
   ks_panels(sl, P.M, P.N, r0, c0, pA1, pB1);
   ks_panels(sl, P.M, P.N, c0, r0, pA2, pB2);
   ks_mma(pA1, pB1, v1);
-  ks_mma(pA2, pB2, v2);
+  ks_stash(T1, v1);
+  ks_mma(pA2, pB2, v1);
+  __syncthreads();
+  ks_stash(T2, v1);
   __syncthreads();
   const double sigma = P.sc * (P.spa ? hv0 : 1.0) * (P.spb ? hv1 : 1.0);
   const int mI = min(BM, P.M - r0), mJ = min(BM, P.M - c0);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm = warp & 1, wn = warp >> 1;
+  constexpr int PER = BM * BN / KS_THREADS;
 #pragma unroll
   for (int side = 0; side < 2; ++side) {
-    ks_stash(T, side == 0 ? v2 : v1);
-    __syncthreads();
-    const double(*v)[2][2] = side == 0 ? v1 : v2;
+    const double* Ta = side == 0 ? T1 : T2;
+    const double* Tb = side == 0 ? T2 : T1;
     const int rb = side == 0 ? r0 : c0, cb = side == 0 ? c0 : r0;
     const int mr = side == 0 ? mI : mJ, nc = side == 0 ? mJ : mI;
+    constexpr int CH = 8;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int k0 = 0; k0 < PER; k0 += CH) {
+      double cv[CH];  // read-modify-write of C: a chunk's loads first, then its stores
 #pragma unroll
-      for (int j = 0; j < 2; ++j)
+      for (int k = 0; k < CH; ++k) {
+        const int idx = threadIdx.x + (k0 + k) * KS_THREADS, r = idx & (BM - 1), c = idx >> 6;
+        cv[k] = (acc_mode && r < mr && c < nc) ? out[(rb + r) + (i64)(cb + c) * P.ldc] : 0.0;
+      }
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int r = wm * 32 + i * 8 + (lane >> 2), c = wn * 16 + j * 8 + 2 * (lane & 3) + e;
-          if (r < mr && c < nc) {
-            double* p = out + (rb + r) + (i64)(cb + c) * P.ldc;
-            const double x = v[i][j][e] + sigma * T[r * TLD + c];
-            *p = acc_mode ? *p + x : x;
-          }
+      for (int k = 0; k < CH; ++k) {
+        const int idx = threadIdx.x + (k0 + k) * KS_THREADS, r = idx & (BM - 1), c = idx >> 6;
+        if (r < mr && c < nc) {
+          const double x = Ta[c * TLD + r] + sigma * Tb[r * TLD + c];
+          out[(rb + r) + (i64)(cb + c) * P.ldc] = acc_mode ? cv[k] + x : x;
         }
-    __syncthreads();
+      }
+    }
   }
 }
 
@@ -694,22 +744,12 @@ static bool seg_active_host(const GSeg& s, unsigned mA, unsigned mB) {
   return !dead(s.srcA, s.depA) && !dead(s.srcB, s.depB);
 }
 
-// Task lists for (maskA, maskB): every tile (tile pair in the pair modes) of
-// every problem that has an active segment (SET problems always: they must
-// write), longest first; problems whose active segments span K <= KS_K
-// (at most 8 of them) in a separate list for the K-short kernel.
-static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTask** d_tasks, int* ntasks,
-                     GTask** d_short, int* nshort) {
-  auto key = std::make_pair(mA, mB);
-  auto it = P.tasks.find(key);
-  if (it != P.tasks.end()) {
-    *d_tasks = it->second.first;
-    *ntasks = it->second.second;
-    *d_short = P.tasks_short[key].first;
-    *nshort = P.tasks_short[key].second;
-    return QD_OK;
-  }
-  std::vector<std::pair<double, GTask>> v[2];
+// Host task lists of P for (mA, mB): [0] long-K problems, [1] K-short ones,
+// each as (cost, task), longest first.  Every tile (tile pair in the pair
+// modes) of every problem that has an active segment (SET problems always:
+// they must write); problems whose active segments span K <= KS_K (at most
+// 8 of them) go to the K-short kernel.
+static void task_vectors(const GemmProgram& P, unsigned mA, unsigned mB, std::vector<std::pair<double, GTask>> v[2]) {
   for (size_t pi = 0; pi < P.probs.size(); ++pi) {
     const GProb& g = P.probs[pi];
     double kt = 0.0;
@@ -737,9 +777,26 @@ static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTa
         v[which].push_back({cost, t});
       }
   }
+  for (int w = 0; w < 2; ++w)
+    std::stable_sort(v[w].begin(), v[w].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+}
+
+static int get_tasks(qd_layout* L, GemmProgram& P, unsigned mA, unsigned mB, GTask** d_tasks, int* ntasks,
+                     GTask** d_short, int* nshort) {
+  (void)L;
+  auto key = std::make_pair(mA, mB);
+  auto it = P.tasks.find(key);
+  if (it != P.tasks.end()) {
+    *d_tasks = it->second.first;
+    *ntasks = it->second.second;
+    *d_short = P.tasks_short[key].first;
+    *nshort = P.tasks_short[key].second;
+    return QD_OK;
+  }
+  std::vector<std::pair<double, GTask>> v[2];
+  task_vectors(P, mA, mB, v);
   GTask* d[2] = {nullptr, nullptr};
   for (int w = 0; w < 2; ++w) {
-    std::stable_sort(v[w].begin(), v[w].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     std::vector<GTask> h(v[w].size());
     for (size_t i = 0; i < v[w].size(); ++i) h[i] = v[w][i].second;
     if (!h.empty()) {
@@ -778,15 +835,134 @@ int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double 
   for (int i = 0; i < NBUF; ++i) b.p[i] = bufs[i];
   if (nt > 0) {
     k_grouped_gemm<<<nt, GEMM_THREADS, GEMM_SMEM, L->stream>>>(d_tasks, P.d_probs, P.d_segs, b, hv0, hv1, maskA,
-                                                                maskB);
+                                                                maskB, nullptr, nullptr);
     ++L->nlaunch;
   }
   if (ns > 0) {
-    k_gemm_kshort<<<ns, KS_THREADS, KS_SMEM, L->stream>>>(d_short, P.d_probs, P.d_segs, b, hv0, hv1, maskA, maskB);
+    k_gemm_kshort<<<ns, KS_THREADS, KS_SMEM, L->stream>>>(d_short, P.d_probs, P.d_segs, b, hv0, hv1, maskA, maskB,
+                                                          nullptr, nullptr);
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());
   return QD_OK;
+}
+
+// ---- one launch over several instances' programs (batched flows) ---------
+namespace {
+struct MergedGemm {
+  GTask* d_task[2] = {nullptr, nullptr};  // long-K, K-short
+  int* d_tinst[2] = {nullptr, nullptr};
+  int n[2] = {0, 0};
+  GInst* d_inst = nullptr;
+  GInst* h_inst = nullptr;  // pinned staging of the per-call instance table
+  std::vector<const qd_layout*> layouts;
+};
+std::map<std::vector<uintptr_t>, MergedGemm>& merged_gemm() {
+  static std::map<std::vector<uintptr_t>, MergedGemm> m;
+  return m;
+}
+std::mutex g_merged_gemm_mutex;
+
+void free_merged(MergedGemm& m) {
+  for (int w = 0; w < 2; ++w) {
+    if (m.d_task[w]) cudaFree(m.d_task[w]);
+    if (m.d_tinst[w]) cudaFree(m.d_tinst[w]);
+  }
+  if (m.d_inst) cudaFree(m.d_inst);
+  if (m.h_inst) cudaFreeHost(m.h_inst);
+}
+}  // namespace
+
+// Every item's program P on its operands, as one launch per kernel (long-K
+// and K-short tasks of all items interleaved, longest first); the items'
+// layouts share `st`.  The task lists are cached per (layout, program,
+// masks) tuple; the instance table is uploaded per call from pinned memory,
+// which the caller rewrites only after synchronising the stream.
+int run_programs_batched(cudaStream_t st, const std::vector<GemmItem>& items) {
+  if (items.empty()) return QD_OK;
+  std::vector<uintptr_t> key;
+  for (const GemmItem& it : items) {
+    TRY_GEMM(build_programs(it.L));
+    key.push_back((uintptr_t)it.L);
+    key.push_back((uintptr_t)it.P);
+    key.push_back(((uintptr_t)it.maskA << 16) | it.maskB);
+  }
+  MergedGemm* m;
+  {
+    std::lock_guard<std::mutex> lock(g_merged_gemm_mutex);
+    auto f = merged_gemm().find(key);
+    if (f == merged_gemm().end()) {
+      MergedGemm mg;
+      std::vector<std::pair<double, std::pair<GTask, int>>> all[2];
+      for (size_t i = 0; i < items.size(); ++i) {
+        std::vector<std::pair<double, GTask>> v[2];
+        task_vectors(*items[i].P, items[i].maskA, items[i].maskB, v);
+        for (int w = 0; w < 2; ++w)
+          for (auto& x : v[w]) all[w].push_back({x.first, {x.second, (int)i}});
+        mg.layouts.push_back(items[i].L);
+      }
+      for (int w = 0; w < 2; ++w) {
+        std::stable_sort(all[w].begin(), all[w].end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        std::vector<GTask> ht(all[w].size());
+        std::vector<int> hi(all[w].size());
+        for (size_t k = 0; k < all[w].size(); ++k) {
+          ht[k] = all[w][k].second.first;
+          hi[k] = all[w][k].second.second;
+        }
+        mg.n[w] = (int)ht.size();
+        if (!ht.empty()) {
+          QD_CUDA(cudaMalloc(&mg.d_task[w], ht.size() * sizeof(GTask)));
+          QD_CUDA(cudaMemcpy(mg.d_task[w], ht.data(), ht.size() * sizeof(GTask), cudaMemcpyHostToDevice));
+          QD_CUDA(cudaMalloc(&mg.d_tinst[w], hi.size() * sizeof(int)));
+          QD_CUDA(cudaMemcpy(mg.d_tinst[w], hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+      }
+      QD_CUDA(cudaMalloc(&mg.d_inst, items.size() * sizeof(GInst)));
+      QD_CUDA(cudaMallocHost(&mg.h_inst, items.size() * sizeof(GInst)));
+      f = merged_gemm().emplace(key, mg).first;
+    }
+    m = &f->second;
+  }
+  for (size_t i = 0; i < items.size(); ++i) {
+    const GemmItem& it = items[i];
+    GInst& g = m->h_inst[i];
+    g.probs = it.P->d_probs;
+    g.segs = it.P->d_segs;
+    for (int b = 0; b < NBUF; ++b) g.bufs.p[b] = it.bufs[b];
+    g.hv0 = it.hv0;
+    g.hv1 = it.hv1;
+    g.maskA = it.maskA;
+    g.maskB = it.maskB;
+  }
+  QD_CUDA(cudaMemcpyAsync(m->d_inst, m->h_inst, items.size() * sizeof(GInst), cudaMemcpyHostToDevice, st));
+  Bufs none;
+  for (int b = 0; b < NBUF; ++b) none.p[b] = nullptr;
+  if (m->n[0] > 0) {
+    k_grouped_gemm<<<m->n[0], GEMM_THREADS, GEMM_SMEM, st>>>(m->d_task[0], nullptr, nullptr, none, 0.0, 0.0, 0u, 0u,
+                                                             m->d_tinst[0], m->d_inst);
+    ++items[0].L->nlaunch;
+  }
+  if (m->n[1] > 0) {
+    k_gemm_kshort<<<m->n[1], KS_THREADS, KS_SMEM, st>>>(m->d_task[1], nullptr, nullptr, none, 0.0, 0.0, 0u, 0u,
+                                                        m->d_tinst[1], m->d_inst);
+    ++items[0].L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// Drop every merged task list that involves layout L (called when L goes).
+void drop_merged_gemm(const qd_layout* L) {
+  std::lock_guard<std::mutex> lock(g_merged_gemm_mutex);
+  auto& mm = merged_gemm();
+  for (auto it = mm.begin(); it != mm.end();) {
+    if (std::find(it->second.layouts.begin(), it->second.layouts.end(), L) != it->second.layouts.end()) {
+      free_merged(it->second);
+      it = mm.erase(it);
+    } else {
+      ++it;
+    }
+  }
 }
 
 }  // namespace qd

@@ -68,7 +68,8 @@ __device__ __forceinline__ int cnt_of(int c, int4 bd) { return c == 0 ? bd.x : (
 //   d0 = {q, n1 | n2 << 8 | (g == h) << 16, holes(g) | holes(h) << 8, F offset of g}
 //   d1 = {F offset of h, first pair entry, first cell entry, cnt_hh | cnt_ph << 10 | cnt_pp << 20}
 // Pair entries (int2, sorted by class then index within the class):
-//   {index w within its class, primary cell | (mirror cell + 1) << 8 | (sign < 0) << 16}
+//   {index w within its class, primary cell | (mirror cell + 1) << 8 | (sign < 0) << 16 |
+//    k1 << 17 | k2 << 21}, the primary cell being (k1, k2) = k1 * n2 + k2
 // Cell entries (one byte per cell of the n1 x n2 grid):
 //   valid << 3 | class << 1 | (sign < 0); 0 for the (t,t) cells of g = h.
 struct GpDesc {
@@ -124,33 +125,91 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// summation range of a leg: all members of the group, or (one-body part with
-// no hh and pp entries) the members of the other kind
-__device__ __forceinline__ void leg_range(int k, int n, int h, int sparse, int& lo, int& hi) {
-  lo = 0;
-  hi = n;
-  if (sparse) {
-    if (k < h)
-      lo = h;
-    else
-      hi = h;
-  }
+// class of a pair from the kinds of its two states: 0 hh, 1 ph, 2 pp
+__device__ __forceinline__ int pair_class(bool hole1, bool hole2) { return (hole1 ? 0 : 1) + (hole2 ? 0 : 1); }
+
+// Whether a leg's sum over the holes (t_hole) or the particles of its group
+// can add anything: the one-body factor F(k, t) of a sparse operand (no hh
+// and pp entries) couples a hole k only to particles t and a particle only to
+// holes; the staged operand must be able to be non-zero on the cells reached,
+// whose class pair is (class of (t, other), fixed class) -- nz holds one bit
+// per class pair (c1 * 3 + c2, symmetric) of the operand's non-zero parts.
+__device__ __forceinline__ bool leg_ok(int sparse, bool k_hole, bool t_hole, bool other_hole, int cfix,
+                                       unsigned nz) {
+  if (sparse && k_hole == t_hole) return false;
+  return (nz >> (pair_class(t_hole, other_hole) * 3 + cfix)) & 1u;
 }
+
+// sum over t of F(k, t) T[base + t * stride], holes [0, h) then particles
+// [h, n), each range only where allowed
+__device__ __forceinline__ double leg_sum(const double2* __restrict__ Frow, bool fx, const double* __restrict__ T,
+                                          int base, int stride, int n, int h, bool hole_ok, bool part_ok) {
+  double y = 0.0;
+  if (hole_ok)
+    for (int t = 0; t < h; ++t) y += (fx ? Frow[t].x : Frow[t].y) * T[base + t * stride];
+  if (part_ok)
+    for (int t = h; t < n; ++t) y += (fx ? Frow[t].x : Frow[t].y) * T[base + t * stride];
+  return y;
+}
+
+// One instance of a launch that covers several layouts (batched flows): its
+// layout view, plan tables, F table and operands.
+struct Inst122 {
+  DevLayout L;
+  const int2* tiles;
+  const int4* gpd;
+  const int2* gpp;
+  const unsigned char* cinfo;
+  const double2* F;
+  int nfent;
+  const double* A;
+  double hA;
+  unsigned zA;
+  int spA;
+  const double* B;
+  double hB;
+  unsigned zB;
+  int spB;
+  double* C;
+  unsigned nzA, nzB;
+};
 
 // Task: {tile, op}; op bit 0: the B term (FA x TB), bit 1: the A term
 // (-FB x TA), bit 2: accumulate into C instead of setting it.  op & 3 == 0
 // writes zeros.  TW = doubles per staged cell: 1 (one operand), 2 (A and B);
 // T122 = threads per CTA (picked per launch bucket by the autotuner below).
 template <int TW, int T122>
-__global__ void __launch_bounds__(T122) k_122_tile(DevLayout L, const int2* __restrict__ tasks,
+__global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, const int2* __restrict__ tasks,
                                                    const int2* __restrict__ tiles, const int4* __restrict__ gpd,
                                                    const int2* __restrict__ gpp,
                                                    const unsigned char* __restrict__ cinfo,
                                                    const double2* __restrict__ F, int nfent,
                                                    const double* __restrict__ A, double hA, unsigned zA, int spA,
                                                    const double* __restrict__ B, double hB, unsigned zB, int spB,
-                                                   double* __restrict__ C) {
+                                                   double* __restrict__ C, unsigned nzA, unsigned nzB,
+                                                   const int* __restrict__ tinst, const Inst122* __restrict__ insts) {
   extern __shared__ __align__(16) double sm122[];
+  if (tinst) {  // a task of several layouts' task lists: this instance's tables and operands
+    const Inst122& I = insts[tinst[blockIdx.x]];
+    L = I.L;
+    tiles = I.tiles;
+    gpd = I.gpd;
+    gpp = I.gpp;
+    cinfo = I.cinfo;
+    F = I.F;
+    nfent = I.nfent;
+    A = I.A;
+    hA = I.hA;
+    zA = I.zA;
+    spA = I.spA;
+    B = I.B;
+    hB = I.hB;
+    zB = I.zB;
+    spB = I.spB;
+    C = I.C;
+    nzA = I.nzA;
+    nzB = I.nzB;
+  }
   const int2 task = tasks[blockIdx.x];
   const int2 tl = __ldg(&tiles[task.x]);
   const int op = task.y;
@@ -197,9 +256,11 @@ __global__ void __launch_bounds__(T122) k_122_tile(DevLayout L, const int2* __re
       const unsigned zm = x == 0 ? zA : zB;
       const int xo = TW == 2 ? x : 0;
       int o1 = 0;
+#pragma unroll
       for (int c1 = 0; c1 < 3; ++c1) {
         const int r1 = da.cnt[c1];
         int o2 = 0;
+#pragma unroll
         for (int c2 = 0; c2 < 3; ++c2) {
           const int r2 = db.cnt[c2];
           const bool lower = c1 >= c2;
@@ -208,14 +269,18 @@ __global__ void __launch_bounds__(T122) k_122_tile(DevLayout L, const int2* __re
             const i64 base = __ldg(boff + part);
             const i64 ldv = lower ? cnt_of(c1, bd) : cnt_of(c2, bd);
             const int total = r1 * r2;
+            // e = fast + nf * slow, walked without dividing: the memory-contiguous
+            // index (rows for stored parts, columns for transposed ones) is fast
+            const int nf = lower ? r1 : r2;
+            int fa = tid % nf, sl = tid / nf;
+            const int dfa = T122 % nf, dsl = T122 / nf;
             for (int e = tid; e < total; e += T122) {
-              int p, u;
-              if (lower) {
-                p = e % r1;
-                u = e / r1;
-              } else {
-                u = e % r2;
-                p = e / r2;
+              const int p = lower ? fa : sl, u = lower ? sl : fa;
+              fa += dfa;
+              sl += dsl;
+              if (fa >= nf) {
+                fa -= nf;
+                ++sl;
               }
               const int2 P = pr[o1 + p], Q = pc[o2 + u];
               const i64 addr = lower ? base + P.x + (i64)Q.x * ldv : base + Q.x + (i64)P.x * ldv;
@@ -238,8 +303,16 @@ __global__ void __launch_bounds__(T122) k_122_tile(DevLayout L, const int2* __re
     cp_async_wait_all();
     __syncthreads();
     // orientation and herm signs in place; (t,t) cells and known-zero parts -> 0
+    int fs = tid % nc, fr = tid / nc;
+    const int dfs = T122 % nc, dfr = T122 / nc;
     for (int e = tid; e < nr * nc; e += T122) {
-      const int r = e / nc, s = e - r * nc;
+      const int r = fr, s = fs;
+      fs += dfs;
+      fr += dfr;
+      if (fs >= nc) {
+        fs -= nc;
+        ++fr;
+      }
       const int ci = cr[r], cj = cc[s];
       const int c1 = (ci >> 1) & 3, c2 = (cj >> 1) & 3;
       const bool valid = (ci & cj & 8) != 0;
@@ -259,41 +332,59 @@ __global__ void __launch_bounds__(T122) k_122_tile(DevLayout L, const int2* __re
   // stored output cells: regions with c1 >= c2, rows of S_a fastest
   const int xa = 0, xb = TW == 2 ? 1 : 0;
   int o1 = 0;
+#pragma unroll
   for (int c1 = 0; c1 < 3; ++c1) {
     const int r1 = da.cnt[c1];
     int o2 = 0;
+#pragma unroll
     for (int c2 = 0; c2 <= c1; ++c2) {
       const int r2 = db.cnt[c2];
       if (r1 > 0 && r2 > 0) {
         const i64 base = __ldg(boff + slot_of(c1, c2));
         const i64 ldc = cnt_of(c1, bd);
+        int p = tid % r1, u = tid / r1;
+        const int dp = T122 % r1, du = T122 / r1;
         for (int e = tid; e < r1 * r2; e += T122) {
-          const int p = e % r1, u = e / r1;
           const int2 P = pr[o1 + p], Q = pc[o2 + u];
+          p += dp;
+          u += du;
+          if (p >= r1) {
+            p -= r1;
+            ++u;
+          }
           double y = 0.0;
           if (work) {
             const int r = P.y & 0xFF, s = Q.y & 0xFF;
-            const int k1 = r / n2, k2 = r - k1 * n2, l1 = s / n4, l2 = s - l1 * n4;
-            int lo, hi;
+            const int k1 = (P.y >> 17) & 15, k2 = (P.y >> 21) & 15;
+            const int l1 = (Q.y >> 17) & 15, l2 = (Q.y >> 21) & 15;
+            const bool h1 = k1 < da.hg, h2 = k2 < da.hh, h3 = l1 < db.hg, h4 = l2 < db.hh;
+            // leg t-ranges: holes [0, h) and particles [h, n) of the leg's group,
+            // each kept only if the one-body factor allows it (sparse: hole <->
+            // particle only) and the staged operand can be non-zero on the cells
+            // it reaches (class pairs of the operand's non-zero parts)
+            const int bL1 = (k2 * ld + s) * TW, sL1 = n2 * ld * TW;        // T((t,k2), s)
+            const int bL2 = (k1 * n2 * ld + s) * TW, sL2 = ld * TW;        // T((k1,t), s)
+            const int bL3 = (r * ld + l2) * TW, sL3 = n4 * TW;             // T(r, (t,l2))
+            const int bL4 = (r * ld + l1 * n4) * TW, sL4 = TW;             // T(r, (l1,t))
             if (useB) {  // FA x TB
-              leg_range(k1, n1, da.hg, spA, lo, hi);
-              for (int t = lo; t < hi; ++t) y += F1[k1 * n1 + t].x * T[((t * n2 + k2) * ld + s) * TW + xb];
-              leg_range(k2, n2, da.hh, spA, lo, hi);
-              for (int t = lo; t < hi; ++t) y += F2[k2 * n2 + t].x * T[((k1 * n2 + t) * ld + s) * TW + xb];
-              leg_range(l1, n3, db.hg, spA, lo, hi);
-              for (int t = lo; t < hi; ++t) y -= F3[l1 * n3 + t].x * T[(r * ld + t * n4 + l2) * TW + xb];
-              leg_range(l2, n4, db.hh, spA, lo, hi);
-              for (int t = lo; t < hi; ++t) y -= F4[l2 * n4 + t].x * T[(r * ld + l1 * n4 + t) * TW + xb];
+              y += leg_sum(F1 + k1 * n1, true, T + xb, bL1, sL1, n1, da.hg,
+                           leg_ok(spA, h1, true, h2, c2, nzB), leg_ok(spA, h1, false, h2, c2, nzB));
+              y += leg_sum(F2 + k2 * n2, true, T + xb, bL2, sL2, n2, da.hh,
+                           leg_ok(spA, h2, true, h1, c2, nzB), leg_ok(spA, h2, false, h1, c2, nzB));
+              y -= leg_sum(F3 + l1 * n3, true, T + xb, bL3, sL3, n3, db.hg,
+                           leg_ok(spA, h3, true, h4, c1, nzB), leg_ok(spA, h3, false, h4, c1, nzB));
+              y -= leg_sum(F4 + l2 * n4, true, T + xb, bL4, sL4, n4, db.hh,
+                           leg_ok(spA, h4, true, h3, c1, nzB), leg_ok(spA, h4, false, h3, c1, nzB));
             }
             if (useA) {  // -FB x TA
-              leg_range(k1, n1, da.hg, spB, lo, hi);
-              for (int t = lo; t < hi; ++t) y -= F1[k1 * n1 + t].y * T[((t * n2 + k2) * ld + s) * TW + xa];
-              leg_range(k2, n2, da.hh, spB, lo, hi);
-              for (int t = lo; t < hi; ++t) y -= F2[k2 * n2 + t].y * T[((k1 * n2 + t) * ld + s) * TW + xa];
-              leg_range(l1, n3, db.hg, spB, lo, hi);
-              for (int t = lo; t < hi; ++t) y += F3[l1 * n3 + t].y * T[(r * ld + t * n4 + l2) * TW + xa];
-              leg_range(l2, n4, db.hh, spB, lo, hi);
-              for (int t = lo; t < hi; ++t) y += F4[l2 * n4 + t].y * T[(r * ld + l1 * n4 + t) * TW + xa];
+              y -= leg_sum(F1 + k1 * n1, false, T + xa, bL1, sL1, n1, da.hg,
+                           leg_ok(spB, h1, true, h2, c2, nzA), leg_ok(spB, h1, false, h2, c2, nzA));
+              y -= leg_sum(F2 + k2 * n2, false, T + xa, bL2, sL2, n2, da.hh,
+                           leg_ok(spB, h2, true, h1, c2, nzA), leg_ok(spB, h2, false, h1, c2, nzA));
+              y += leg_sum(F3 + l1 * n3, false, T + xa, bL3, sL3, n3, db.hg,
+                           leg_ok(spB, h3, true, h4, c1, nzA), leg_ok(spB, h3, false, h4, c1, nzA));
+              y += leg_sum(F4 + l2 * n4, false, T + xa, bL4, sL4, n4, db.hh,
+                           leg_ok(spB, h4, true, h3, c1, nzA), leg_ok(spB, h4, false, h3, c1, nzA));
             }
             if ((P.y ^ Q.y) & (1 << 16)) y = -y;
           }
@@ -324,11 +415,13 @@ struct Bucket122 {
   int first;    // range in the task array
   int count;
   size_t smem;
+  int list = 0;          // 0 one operand (sets C), 1 both operands, 2 one operand (accumulates)
   int threads = 256;    // CTA size (autotuned)
   float ms[2] = {0, 0};  // measured time of the 128- and 256-thread variants
 };
 struct TaskSet {
   int2* d_task = nullptr;
+  std::vector<int2> h_task;  // host copy (merged launches of several layouts)
   std::vector<Bucket122> buckets;
   bool tuned = false;
 };
@@ -445,7 +538,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
         set_error("commutator_122: group pair of %d cells exceeds the cell fields", gsz[g] * gsz[h]);
         return QD_ERR_ARG;
       }
-      plist[u].push_back(int2{w, r | ((rm + 1) << 8) | (neg << 16)});
+      plist[u].push_back(int2{w, r | ((rm + 1) << 8) | (neg << 16) | (kpos[t1] << 17) | (kpos[t2] << 21)});
       cl[u][r] = (unsigned char)(8 | (c << 1) | neg);
       if (rm >= 0) cl[u][rm] = (unsigned char)(8 | (c << 1) | (1 - neg));
       gh[u].cnt[c] += 1;
@@ -564,6 +657,7 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
         if (bnd < top) lower = bnd;
       Bucket122 b;
       b.tw = l == 1 ? 2 : 1;
+      b.list = l;
       b.first = (int)all.size();
       b.smem = top;
       while (i < v.size() && v[i].first > lower) all.push_back(v[i++].second);
@@ -571,8 +665,17 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
       ts.buckets.push_back(b);
     }
   }
+  // within a bucket, tiles sharing a column strip (block q, column group pair
+  // b) run together: their gathers read the same columns, whose memory atoms
+  // also hold neighbouring group pairs' rows, so concurrent CTAs hit in L2
+  for (const Bucket122& bk : ts.buckets)
+    std::stable_sort(all.begin() + bk.first, all.begin() + bk.first + bk.count, [&](const int2& x, const int2& y) {
+      const TileInfo &tx = p->tiles[x.x], &ty = p->tiles[y.x];
+      return tx.b != ty.b ? tx.b < ty.b : tx.a < ty.a;
+    });
   int rc = upload_vec(L, all, &ts.d_task);
   if (rc) return rc;
+  ts.h_task = all;
   p->sets[key] = ts;
   *out = &p->sets[key];
   return QD_OK;
@@ -591,13 +694,26 @@ void drop_122_plan(const qd_layout* L) {
   plans().erase(it);
 }
 
+// class pairs (c1 * 3 + c2, both orders) on which an operand can be non-zero
+static unsigned nz_mask(unsigned zmask) {
+  unsigned nz = 0;
+  for (int c1 = 0; c1 < 3; ++c1)
+    for (int c2 = 0; c2 < 3; ++c2) {
+      const int part = c1 >= c2 ? slot_of(c1, c2) : slot_of(c2, c1);
+      if (!((zmask >> (P_HHHH + part)) & 1u)) nz |= 1u << (c1 * 3 + c2);
+    }
+  return nz;
+}
+
 static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, const Bucket122& b, int threads,
                          const qd_op* A, const qd_op* B, int spA, int spB, double* C) {
 #define QD_122_LAUNCH(TW, NT)                                                                                   \
   k_122_tile<TW, NT><<<b.count, NT, b.smem, L->stream>>>(L->dev, ts->d_task + b.first, p->d_tiles, p->d_gpd,   \
                                                          p->d_gpp, p->d_cinfo, p->d_ftab, p->nfent, A->d,       \
                                                          (double)A->herm, A->zero_mask, spA, B->d,              \
-                                                         (double)B->herm, B->zero_mask, spB, C)
+                                                         (double)B->herm, B->zero_mask, spB, C,                \
+                                                         nz_mask(A->zero_mask), nz_mask(B->zero_mask), nullptr, \
+                                                         nullptr)
   if (b.tw == 2) {
     if (threads == 128) QD_122_LAUNCH(2, 128); else QD_122_LAUNCH(2, 256);
   } else {
@@ -710,6 +826,174 @@ int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   for (const Bucket122& b : ts->buckets) TRY(launch_bucket(L, p, ts, b, b.threads, A, B, spA, spB, C));
   QD_CUDA(cudaGetLastError());
   return QD_OK;
+}
+
+// ---- one launch over several layouts' tiles (batched flows) ---------------
+namespace {
+struct Merged122 {
+  int2* d_task = nullptr;
+  int* d_tinst = nullptr;
+  std::vector<Bucket122> buckets;
+  Inst122* d_inst = nullptr;
+  Inst122* h_inst = nullptr;  // pinned staging of the per-call instance table
+  std::vector<const qd_layout*> layouts;
+};
+std::map<std::vector<uintptr_t>, Merged122>& merged122() {
+  static std::map<std::vector<uintptr_t>, Merged122> m;
+  return m;
+}
+std::mutex g_m122_mutex;
+}  // namespace
+
+// commutator_122 of every item in one set of launches: the items' tiles are
+// merged per list (set with one operand, set with both, accumulate) and per
+// shared-memory bucket, largest first, each task carrying its instance; the
+// items' layouts share `st`.  Merged lists are cached per (layout, masks)
+// tuple; the instance table is uploaded per call from pinned memory, which
+// the caller rewrites only after synchronising the stream.
+int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
+  if (items.empty()) return QD_OK;
+  const size_t n = items.size();
+  std::vector<Plan122*> pl(n);
+  std::vector<TaskSet*> tsv(n);
+  std::vector<uintptr_t> key;
+  for (size_t i = 0; i < n; ++i) {
+    qd_layout* L = items[i].L;
+    TRY(plan_122(L, &pl[i]));
+    TRY(task_set(L, pl[i], items[i].A->zero_mask, items[i].B->zero_mask, &tsv[i]));
+    key.push_back((uintptr_t)L);
+    key.push_back(((uintptr_t)items[i].A->zero_mask << 16) | items[i].B->zero_mask);
+  }
+  Merged122* m;
+  {
+    std::lock_guard<std::mutex> lock(g_m122_mutex);
+    auto f = merged122().find(key);
+    if (f == merged122().end()) {
+      Merged122 mg;
+      std::vector<std::pair<size_t, std::pair<int2, int>>> lists[3];
+      for (size_t i = 0; i < n; ++i) {
+        mg.layouts.push_back(items[i].L);
+        for (const Bucket122& b : tsv[i]->buckets)
+          for (int k = b.first; k < b.first + b.count; ++k) {
+            const int2 t = tsv[i]->h_task[k];
+            lists[b.list].push_back({tile_smem(pl[i]->tiles[t.x], b.tw), {t, (int)i}});
+          }
+      }
+      std::vector<int2> ht;
+      std::vector<int> hi;
+      const size_t bounds[4] = {24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122};
+      for (int l = 0; l < 3; ++l) {
+        auto& v = lists[l];
+        std::stable_sort(v.begin(), v.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        size_t k = 0;
+        while (k < v.size()) {
+          const size_t top = v[k].first;
+          size_t lower = 0;
+          for (size_t bnd : bounds)
+            if (bnd < top) lower = bnd;
+          Bucket122 b;
+          b.tw = l == 1 ? 2 : 1;
+          b.list = l;
+          b.first = (int)ht.size();
+          b.smem = top;
+          while (k < v.size() && v[k].first > lower) {
+            ht.push_back(v[k].second.first);
+            hi.push_back(v[k].second.second);
+            ++k;
+          }
+          b.count = (int)ht.size() - b.first;
+          mg.buckets.push_back(b);
+          {  // column strips together within the bucket (see task_set)
+            std::vector<size_t> ord(b.count);
+            for (int x = 0; x < b.count; ++x) ord[x] = b.first + x;
+            std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+              const TileInfo &tx = pl[hi[x]]->tiles[ht[x].x], &ty = pl[hi[y]]->tiles[ht[y].x];
+              if (hi[x] != hi[y]) return hi[x] < hi[y];
+              return tx.b != ty.b ? tx.b < ty.b : tx.a < ty.a;
+            });
+            std::vector<int2> t2(b.count);
+            std::vector<int> i2(b.count);
+            for (int x = 0; x < b.count; ++x) {
+              t2[x] = ht[ord[x]];
+              i2[x] = hi[ord[x]];
+            }
+            std::copy(t2.begin(), t2.end(), ht.begin() + b.first);
+            std::copy(i2.begin(), i2.end(), hi.begin() + b.first);
+          }
+        }
+      }
+      QD_CUDA(cudaMalloc(&mg.d_task, std::max<size_t>(1, ht.size()) * sizeof(int2)));
+      QD_CUDA(cudaMalloc(&mg.d_tinst, std::max<size_t>(1, hi.size()) * sizeof(int)));
+      if (!ht.empty()) {
+        QD_CUDA(cudaMemcpy(mg.d_task, ht.data(), ht.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        QD_CUDA(cudaMemcpy(mg.d_tinst, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice));
+      }
+      QD_CUDA(cudaMalloc(&mg.d_inst, n * sizeof(Inst122)));
+      QD_CUDA(cudaMallocHost(&mg.h_inst, n * sizeof(Inst122)));
+      f = merged122().emplace(key, mg).first;
+    }
+    m = &f->second;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    const Item122& it = items[i];
+    const Plan122* p = pl[i];
+    const int nf = it.L->m * p->gmax;
+    k_ftab<<<(nf + 127) / 128, 128, 0, st>>>(it.L->dev, p->d_sbase, it.A->d, (double)it.A->herm, it.B->d,
+                                             (double)it.B->herm, p->d_ftab, p->gmax, p->nfent);
+    ++it.L->nlaunch;
+    Inst122& I = m->h_inst[i];
+    I.L = it.L->dev;
+    I.tiles = p->d_tiles;
+    I.gpd = p->d_gpd;
+    I.gpp = p->d_gpp;
+    I.cinfo = p->d_cinfo;
+    I.F = p->d_ftab;
+    I.nfent = p->nfent;
+    I.A = it.A->d;
+    I.hA = (double)it.A->herm;
+    I.zA = it.A->zero_mask;
+    I.spA = spars(it.A);
+    I.B = it.B->d;
+    I.hB = (double)it.B->herm;
+    I.zB = it.B->zero_mask;
+    I.spB = spars(it.B);
+    I.C = it.C;
+    I.nzA = nz_mask(it.A->zero_mask);
+    I.nzB = nz_mask(it.B->zero_mask);
+  }
+  QD_CUDA(cudaMemcpyAsync(m->d_inst, m->h_inst, n * sizeof(Inst122), cudaMemcpyHostToDevice, st));
+  const DevLayout& L0 = items[0].L->dev;
+  for (const Bucket122& b : m->buckets) {
+    if (b.tw == 2)
+      k_122_tile<2, 256><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
+                                                       nullptr, 0, nullptr, 0.0, 0u, 0, nullptr, 0.0, 0u, 0, nullptr,
+                                                       0u, 0u, m->d_tinst + b.first, m->d_inst);
+    else
+      k_122_tile<1, 256><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
+                                                       nullptr, 0, nullptr, 0.0, 0u, 0, nullptr, 0.0, 0u, 0, nullptr,
+                                                       0u, 0u, m->d_tinst + b.first, m->d_inst);
+    ++items[0].L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+// Drop every merged list that involves layout L (called when L goes).
+void drop_merged_122(const qd_layout* L) {
+  std::lock_guard<std::mutex> lock(g_m122_mutex);
+  auto& mm = merged122();
+  for (auto it = mm.begin(); it != mm.end();) {
+    auto& ls = it->second.layouts;
+    if (std::find(ls.begin(), ls.end(), L) != ls.end()) {
+      if (it->second.d_task) cudaFree(it->second.d_task);
+      if (it->second.d_tinst) cudaFree(it->second.d_tinst);
+      if (it->second.d_inst) cudaFree(it->second.d_inst);
+      if (it->second.h_inst) cudaFreeHost(it->second.h_inst);
+      it = mm.erase(it);
+    } else {
+      ++it;
+    }
+  }
 }
 
 }  // namespace qd

@@ -365,12 +365,14 @@ __device__ __forceinline__ void w221_dot(const DevLayout& L, const W221Term& t, 
 }
 
 // One CTA per target whose two states share (m_l, m_s).  Phase 1: thread u
-// resolves the two w221 reads of leg state u into term descriptors and
-// coefficients (shared memory).  Phase 2: the CTA walks the live terms in
-// order; thread k takes the elements k, k + T221, ... of every term's dot
-// product (long ones run over up to n_p = 1,264 entries); one block sum at
-// the end.  Fixed assignment and order: deterministic.
+// resolves the two w221 reads of leg state u; a read whose dot product is
+// short (n_h = K <= 16 entries) is summed by the thread itself, a long one
+// (n_p entries, up to 1,264) is left as a term descriptor in shared memory.
+// Phase 2: the CTA walks the long terms in order, thread k taking the
+// entries k, k + T221, ... of each.  One block sum at the end.  Fixed
+// assignment and order: deterministic.
 constexpr int T221 = 128;
+constexpr int K221_SHORT = 32;
 
 __global__ void __launch_bounds__(T221) k_221_fused(DevLayout L, const int* __restrict__ targets, double hA,
                                                     double hB, const double* __restrict__ A,
@@ -378,45 +380,57 @@ __global__ void __launch_bounds__(T221) k_221_fused(DevLayout L, const int* __re
                                                     double* __restrict__ C) {
   extern __shared__ double sh221[];
   double* coef = sh221;                                      // [2m]
-  int4* term = reinterpret_cast<int4*>(sh221 + 2 * L.m);     // [2m]: {q | which << 16, sl, r, c}
+  int4* term = reinterpret_cast<int4*>(sh221 + 2 * L.m);     // [2m]: {q | which << 16, sl, r, c}; sl < 0: none
   __shared__ double red[T221 / 32];
   const int n = L.n, mp = L.mp, m = L.m;
   const i64 nhh = (i64)n * n, npp = (i64)mp * mp;
   const i64 t = __ldg(targets + blockIdx.x);
   int x, y;
   decode1b(n, mp, t, x, y);
+  double s = 0.0;
   for (int u = threadIdx.x; u < m; u += T221) {
     // the two reads of leg state u and their coefficients (commutators.f90:280-348)
     int w0, w1;
-    int a0, b0, c0, d0, a1, b1, c1, d1;
+    int a0, b0, c0, d0;
     double f0, f1;
     if (t < nhh) {  // fhh(h,h2): x = h, y = h2
       w0 = w1 = u < n ? 1 : 2;
-      a0 = u; b0 = y; c0 = u; d0 = x; a1 = u; b1 = x; c1 = u; d1 = y;
-      f0 = u < n ? hA : -hA;
-      f1 = u < n ? -hB : hB;
+      a0 = u; b0 = y; c0 = u; d0 = x;
     } else if (t < nhh + npp) {  // fpp(p,p2)
       w0 = w1 = 1;
-      a0 = u; b0 = y; c0 = u; d0 = x; a1 = u; b1 = x; c1 = u; d1 = y;
-      f0 = u < n ? hA : -hA;
-      f1 = u < n ? -hB : hB;
+      a0 = u; b0 = y; c0 = u; d0 = x;
     } else {  // fph(p,h)
       w0 = 2;
       w1 = 1;
-      a0 = u; b0 = x; c0 = u; d0 = y; a1 = u; b1 = x; c1 = u; d1 = y;
-      f0 = u < n ? hA : -hA;
-      f1 = u < n ? -hB : hB;
+      a0 = u; b0 = x; c0 = u; d0 = y;
     }
-    double s0, s1;
-    const W221Term t0 = w221_term(L, w0, zA, zB, a0, b0, c0, d0, s0);
-    const W221Term t1 = w221_term(L, w1, zA, zB, a1, b1, c1, d1, s1);
-    term[2 * u] = make_int4(t0.q | (t0.which << 16), t0.sl, t0.r, t0.c);
-    term[2 * u + 1] = make_int4(t1.q | (t1.which << 16), t1.sl, t1.r, t1.c);
-    coef[2 * u] = f0 * s0;
-    coef[2 * u + 1] = f1 * s1;
+    f0 = u < n ? hA : -hA;
+    f1 = u < n ? -hB : hB;
+    // second read: (u, x | u, y) in every case
+    for (int k = 0; k < 2; ++k) {
+      double sg;
+      const W221Term tt = k == 0 ? w221_term(L, w0, zA, zB, a0, b0, c0, d0, sg)
+                                 : w221_term(L, w1, zA, zB, u, x, u, y, sg);
+      const double cf = (k == 0 ? f0 : f1) * sg;
+      int4 d = make_int4(0, -1, 0, 0);
+      if (tt.sl >= 0) {
+        const double* pu;
+        const double* pv;
+        int K, su, sv;
+        w221_dot(L, tt, A, B, pu, pv, K, su, sv);
+        if (K <= K221_SHORT) {
+          double p = 0.0;
+          for (int j = 0; j < K; ++j) p += pu[(i64)j * su] * pv[(i64)j * sv];
+          s += cf * p;
+        } else {
+          d = make_int4(tt.q | (tt.which << 16), tt.sl, tt.r, tt.c);
+        }
+      }
+      term[2 * u + k] = d;
+      coef[2 * u + k] = cf;
+    }
   }
   __syncthreads();
-  double s = 0.0;
   for (int k = 0; k < 2 * m; ++k) {
     const int4 d = term[k];
     if (d.y < 0) continue;  // uniform: every thread reads the same descriptor

@@ -94,6 +94,20 @@ struct GTask {
   short ti, tj;
 };
 
+constexpr int NBUF = 7;
+struct Bufs {
+  const double* p[NBUF];
+};
+// One instance of a launch that covers several layouts' programs (batched
+// flows): its program tables, operand buffers, herm factors and masks.
+struct GInst {
+  const GProb* probs;
+  const GSeg* segs;
+  Bufs bufs;
+  double hv0, hv1;
+  unsigned maskA, maskB;
+};
+
 struct GemmProgram {
   std::vector<GProb> probs;
   std::vector<GSeg> segs;
@@ -209,6 +223,25 @@ int launch_axpy_norms(qd_layout* L, const double* a, double sa, const double* b,
 int launch_bch_decide(qd_layout* L, const double* norms, int* kidx, double conv, cudaGraphConditionalHandle hloop,
                       cudaGraphConditionalHandle hnext, int set_next);
 int prepare_program(qd_layout* L, GemmProgram& P, unsigned maskA, unsigned maskB);
+// one program of one instance in a batched launch
+struct GemmItem {
+  qd_layout* L;
+  GemmProgram* P;
+  const double* bufs[NBUF];
+  double hv0, hv1;
+  unsigned maskA, maskB;
+};
+int run_programs_batched(cudaStream_t st, const std::vector<GemmItem>& items);
+void drop_merged_gemm(const qd_layout* L);
+// commutator_122 of one instance in a batched launch
+struct Item122 {
+  qd_layout* L;
+  const qd_op* A;
+  const qd_op* B;
+  double* C;
+};
+int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items);
+void drop_merged_122(const qd_layout* L);
 int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B);
 std::string tuning_report_122(const qd_layout* L);
 double* scratch_operator(qd_layout* L);

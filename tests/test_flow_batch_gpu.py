@@ -1,7 +1,9 @@
 """Batched flows (qd_magnus_flow_batch): independent instances of different
-sizes run concurrently, one host thread and stream each, must give exactly
-what each gives alone; repeated flows on one layout reuse its workspaces;
-the stepping object (qd_flow_*) reproduces qd_magnus_flow."""
+sizes, run in lockstep with each BCH term's 122 tiles and ladder tasks of all
+instances in one launch per kernel (default), or one host thread and stream
+each, must give exactly what each gives alone; repeated flows on one layout
+reuse its workspaces; the stepping object (qd_flow_*) reproduces
+qd_magnus_flow."""
 import numpy as np
 import pytest
 
@@ -29,11 +31,13 @@ def test_batch_equals_separate(gpu, pandya):
     for P, H, HS in inst:
         _, res = qd.magnus_flow(H, HS, pandya=pandya, max_iter=300)
         alone.append((res.E0, res.iterations, res.commutators, HS.download()))
-    results, status = qd.magnus_flow_batch([(H, HS) for _, H, HS in inst], pandya=pandya, max_iter=300)
-    assert status == [0] * len(inst)
-    for (P, H, HS), r, (e0, it, nc, v) in zip(inst, results, alone):
-        assert r.E0 == e0 and r.iterations == it and r.commutators == nc
-        assert np.array_equal(HS.download(), v)
+    for streams in (False, True):
+        results, status = qd.magnus_flow_batch([(H, HS) for _, H, HS in inst], pandya=pandya, max_iter=300,
+                                               streams=streams)
+        assert status == [0] * len(inst)
+        for (P, H, HS), r, (e0, it, nc, v) in zip(inst, results, alone):
+            assert r.E0 == e0 and r.iterations == it and r.commutators == nc
+            assert np.array_equal(HS.download(), v)
 
 
 def test_repeated_flow_reuses_workspaces(gpu):
