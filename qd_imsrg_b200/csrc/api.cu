@@ -243,7 +243,7 @@ int stage_222(qd_layout* L, const qd_op* A, const qd_op* B, qd_op* C, const qd_c
       TRY(run_program(L, L->prog_pandya, zb, ETACC->herm, HCC->herm, 0u, 0u));
     }
     StageTimer tm(L, S_PANDYA_GATHER);
-    TRY(launch_pandya_gather(L, L->d_z, C->d));
+    TRY(launch_pandya_tiles(L, L->d_z, C->d));
   }
   C->zero_mask = 0;
   return QD_OK;
@@ -826,10 +826,19 @@ int qd_cc_download(const qd_cc* cc, double* host, int64_t n, int64_t* needed) {
   if (needed) *needed = cc->L->xsize;
   if (!host) return QD_OK;
   CHECK(n >= cc->L->xsize, QD_ERR_ARG, "qd_cc_download: buffer too small");
-  TRY(use_device(cc->L));
-  if (cc->L->xsize > 0)
-    QD_CUDA(cudaMemcpyAsync(host, cc->d, sizeof(double) * cc->L->xsize, cudaMemcpyDeviceToHost, cc->L->stream));
-  QD_CUDA(cudaStreamSynchronize(cc->L->stream));
+  const qd_layout* L = cc->L;
+  TRY(use_device(L));
+  if (L->xsize == 0) return QD_OK;
+  // device rows are group-major; the host gets the reference's (i, j) row order
+  std::vector<double> tmp((size_t)L->xsize);
+  QD_CUDA(cudaMemcpyAsync(tmp.data(), cc->d, sizeof(double) * L->xsize, cudaMemcpyDeviceToHost, L->stream));
+  QD_CUDA(cudaStreamSynchronize(L->stream));
+  for (int q = 0; q < L->ncc; ++q) {
+    const int r = L->ccdim[q].x, nb = L->ccdim[q].y, rb = L->ccab_base[q];
+    const i64 xo = L->ccxoff[q];
+    for (int c = 0; c < nb; ++c)
+      for (int t = 0; t < r; ++t) host[xo + L->ccref[rb + t] + (i64)c * r] = tmp[xo + t + (i64)c * r];
+  }
   return QD_OK;
 }
 
@@ -1586,7 +1595,7 @@ int commutator_batch(BatchCtx& bc, std::vector<CommItem>& items, bool pandya) {
       TRY(ensure_z(L));
       const double* zb[7] = {nullptr, nullptr, it.ACC->d, it.BCC->d, nullptr, nullptr, L->d_z};
       TRY(run_program(L, L->prog_pandya, zb, it.ACC->herm, it.BCC->herm, 0u, 0u));
-      TRY(launch_pandya_gather(L, L->d_z, it.C->d));
+      TRY(launch_pandya_tiles(L, L->d_z, it.C->d));
     }
     it.C->zero_mask = 0;
   }

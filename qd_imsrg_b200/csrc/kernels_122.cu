@@ -73,7 +73,11 @@ __device__ __forceinline__ int cnt_of(int c, int4 bd) { return c == 0 ? bd.x : (
 // Cell entries (one byte per cell of the n1 x n2 grid):
 //   valid << 3 | class << 1 | (sign < 0); 0 for the (t,t) cells of g = h.
 struct GpDesc {
-  int q, n1, n2, hg, hh, fg, fh, pstart, cstart, cnt[3];
+  int q, n1, n2, hg, hh, fg, fh, pstart, cstart, cntw;
+  // pairs of class c (0 hh, 1 ph, 2 pp), decoded from the packed word (no local array)
+  __device__ __forceinline__ int cnt(int c) const { return (cntw >> (10 * c)) & 0x3FF; }
+  // pairs of the classes before c
+  __device__ __forceinline__ int off(int c) const { return c == 0 ? 0 : (c == 1 ? cnt(0) : cnt(0) + cnt(1)); }
 };
 __device__ __forceinline__ GpDesc load_gp(const int4* __restrict__ gpd, int u) {
   const int4 a = __ldg(&gpd[2 * u]), b = __ldg(&gpd[2 * u + 1]);
@@ -87,9 +91,7 @@ __device__ __forceinline__ GpDesc load_gp(const int4* __restrict__ gpd, int u) {
   d.fh = b.x;
   d.pstart = b.y;
   d.cstart = b.z;
-  d.cnt[0] = b.w & 0x3FF;
-  d.cnt[1] = (b.w >> 10) & 0x3FF;
-  d.cnt[2] = (b.w >> 20) & 0x3FF;
+  d.cntw = b.w;
   return d;
 }
 
@@ -125,8 +127,21 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// q = a / b and r = a % b for 0 <= a < 2^22 - 1 and b >= 1, through one
+// single-precision reciprocal instead of an integer division: the exact value
+// of (a + 1/2) / b is q + (r + 1/2) / b, at least 1/(2b) away from an integer,
+// and the two correctly rounded float operations err by at most
+// (a + 1/2) / b * 2^-23 < 1/(2b); so truncation gives q.
+__device__ __forceinline__ int2 divmod_small(int a, int b) {
+  const int q = __float2int_rz(((float)a + 0.5f) * __frcp_rn((float)b));
+  return make_int2(q, a - q * b);
+}
+
+template <int TW>
+__device__ __forceinline__ constexpr int xb_of() { return TW == 2 ? 1 : 0; }
+
 // class of a pair from the kinds of its two states: 0 hh, 1 ph, 2 pp
-__device__ __forceinline__ int pair_class(bool hole1, bool hole2) { return (hole1 ? 0 : 1) + (hole2 ? 0 : 1); }
+__host__ __device__ __forceinline__ int pair_class(bool hole1, bool hole2) { return (hole1 ? 0 : 1) + (hole2 ? 0 : 1); }
 
 // Whether a leg's sum over the holes (t_hole) or the particles of its group
 // can add anything: the one-body factor F(k, t) of a sparse operand (no hh
@@ -134,21 +149,22 @@ __device__ __forceinline__ int pair_class(bool hole1, bool hole2) { return (hole
 // holes; the staged operand must be able to be non-zero on the cells reached,
 // whose class pair is (class of (t, other), fixed class) -- nz holds one bit
 // per class pair (c1 * 3 + c2, symmetric) of the operand's non-zero parts.
-__device__ __forceinline__ bool leg_ok(int sparse, bool k_hole, bool t_hole, bool other_hole, int cfix,
-                                       unsigned nz) {
+__host__ __device__ __forceinline__ bool leg_ok(int sparse, bool k_hole, bool t_hole, bool other_hole, int cfix,
+                                                unsigned nz) {
   if (sparse && k_hole == t_hole) return false;
   return (nz >> (pair_class(t_hole, other_hole) * 3 + cfix)) & 1u;
 }
 
-// sum over t of F(k, t) T[base + t * stride], holes [0, h) then particles
-// [h, n), each range only where allowed
-__device__ __forceinline__ double leg_sum(const double2* __restrict__ Frow, bool fx, const double* __restrict__ T,
-                                          int base, int stride, int n, int h, bool hole_ok, bool part_ok) {
+// Sum over t of F(k, t) T[base + t * stride] for one leg: F(k, .) is the
+// leg's one-body row (component fy: 0 FA, 1 FB), t runs over the holes
+// [0, h) of the leg's group when bit 1 of ok is set and over its particles
+// [h, n) when bit 0 is set.
+__device__ __forceinline__ double leg_sum(const double2* __restrict__ Frow, int fy, const double* __restrict__ T,
+                                          int base, int stride, int n, int h, unsigned ok) {
+  const int lo = (ok & 2u) ? 0 : h, hi = (ok & 1u) ? n : h;
+  const double* Fd = reinterpret_cast<const double*>(Frow) + fy;
   double y = 0.0;
-  if (hole_ok)
-    for (int t = 0; t < h; ++t) y += (fx ? Frow[t].x : Frow[t].y) * T[base + t * stride];
-  if (part_ok)
-    for (int t = h; t < n; ++t) y += (fx ? Frow[t].x : Frow[t].y) * T[base + t * stride];
+  for (int t = lo; t < hi; ++t) y += Fd[2 * t] * T[base + t * stride];
   return y;
 }
 
@@ -165,31 +181,33 @@ struct Inst122 {
   const double* A;
   double hA;
   unsigned zA;
-  int spA;
+  unsigned legA;
   const double* B;
   double hB;
   unsigned zB;
-  int spB;
+  unsigned legB;
   double* C;
-  unsigned nzA, nzB;
 };
 
 // Task: {tile, op}; op bit 0: the B term (FA x TB), bit 1: the A term
 // (-FB x TA), bit 2: accumulate into C instead of setting it.  op & 3 == 0
 // writes zeros.  TW = doubles per staged cell: 1 (one operand), 2 (A and B);
 // T122 = threads per CTA (picked per launch bucket by the autotuner below).
-template <int TW, int T122>
+// MULTI: the tasks come from several layouts and each names its instance in
+// tinst (a separate instantiation: the single-layout kernel keeps its
+// arguments in the parameter bank instead of registers).
+template <int TW, int T122, bool MULTI>
 __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, const int2* __restrict__ tasks,
                                                    const int2* __restrict__ tiles, const int4* __restrict__ gpd,
                                                    const int2* __restrict__ gpp,
                                                    const unsigned char* __restrict__ cinfo,
                                                    const double2* __restrict__ F, int nfent,
-                                                   const double* __restrict__ A, double hA, unsigned zA, int spA,
-                                                   const double* __restrict__ B, double hB, unsigned zB, int spB,
-                                                   double* __restrict__ C, unsigned nzA, unsigned nzB,
+                                                   const double* __restrict__ A, double hA, unsigned zA, unsigned legA,
+                                                   const double* __restrict__ B, double hB, unsigned zB, unsigned legB,
+                                                   double* __restrict__ C,
                                                    const int* __restrict__ tinst, const Inst122* __restrict__ insts) {
   extern __shared__ __align__(16) double sm122[];
-  if (tinst) {  // a task of several layouts' task lists: this instance's tables and operands
+  if constexpr (MULTI) {  // a task of several layouts' task lists: this instance's tables and operands
     const Inst122& I = insts[tinst[blockIdx.x]];
     L = I.L;
     tiles = I.tiles;
@@ -201,14 +219,12 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
     A = I.A;
     hA = I.hA;
     zA = I.zA;
-    spA = I.spA;
+    legA = I.legA;
     B = I.B;
     hB = I.hB;
     zB = I.zB;
-    spB = I.spB;
+    legB = I.legB;
     C = I.C;
-    nzA = I.nzA;
-    nzB = I.nzB;
   }
   const int2 task = tasks[blockIdx.x];
   const int2 tl = __ldg(&tiles[task.x]);
@@ -218,7 +234,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
   const int q = da.q;
   const int n1 = da.n1, n2 = da.n2, n3 = db.n1, n4 = db.n2;
   const int nr = n1 * n2, nc = n3 * n4, ld = nc | 1;
-  const int pa = da.cnt[0] + da.cnt[1] + da.cnt[2], pb = db.cnt[0] + db.cnt[1] + db.cnt[2];
+  const int pa = da.cnt(0) + da.cnt(1) + da.cnt(2), pb = db.cnt(0) + db.cnt(1) + db.cnt(2);
   const int4 bd = __ldg(&L.blk[q]);
   const i64* boff = L.boff + 6 * q;
   // shared memory: T [nr][ld][TW] | F1 F2 F3 F4 (double2) | row, column pairs (int2) | cell bytes
@@ -249,62 +265,59 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
 
   if (work) {
     // gather: region (c1 rows of S_a, c2 columns of S_b); the stored element
-    // is (P1,P2) of part (c1,c2) when c1 >= c2, else (P2,P1) of part (c2,c1)
+    // is (P1,P2) of part (c1,c2) when c1 >= c2, else (P2,P1) of part (c2,c1).
+    // The loops stay rolled: the kernel's code must fit the instruction cache.
+#pragma unroll 1
     for (int x = 0; x < 2; ++x) {
       if (x == 0 ? !useA : !useB) continue;
       const double* src = x == 0 ? A : B;
       const unsigned zm = x == 0 ? zA : zB;
       const int xo = TW == 2 ? x : 0;
-      int o1 = 0;
-#pragma unroll
-      for (int c1 = 0; c1 < 3; ++c1) {
-        const int r1 = da.cnt[c1];
-        int o2 = 0;
-#pragma unroll
-        for (int c2 = 0; c2 < 3; ++c2) {
-          const int r2 = db.cnt[c2];
-          const bool lower = c1 >= c2;
-          const int part = lower ? slot_of(c1, c2) : slot_of(c2, c1);
-          if (r1 > 0 && r2 > 0 && !((zm >> (P_HHHH + part)) & 1u)) {
-            const i64 base = __ldg(boff + part);
-            const i64 ldv = lower ? cnt_of(c1, bd) : cnt_of(c2, bd);
-            const int total = r1 * r2;
-            // e = fast + nf * slow, walked without dividing: the memory-contiguous
-            // index (rows for stored parts, columns for transposed ones) is fast
-            const int nf = lower ? r1 : r2;
-            int fa = tid % nf, sl = tid / nf;
-            const int dfa = T122 % nf, dsl = T122 / nf;
-            for (int e = tid; e < total; e += T122) {
-              const int p = lower ? fa : sl, u = lower ? sl : fa;
-              fa += dfa;
-              sl += dsl;
-              if (fa >= nf) {
-                fa -= nf;
-                ++sl;
-              }
-              const int2 P = pr[o1 + p], Q = pc[o2 + u];
-              const i64 addr = lower ? base + P.x + (i64)Q.x * ldv : base + Q.x + (i64)P.x * ldv;
-              const double* g = src + addr;
-              const int r = P.y & 0xFF, rm = ((P.y >> 8) & 0xFF) - 1;
-              const int s = Q.y & 0xFF, sm = ((Q.y >> 8) & 0xFF) - 1;
-              cp_async8(&T[(r * ld + s) * TW + xo], g);
-              if (rm >= 0) cp_async8(&T[(rm * ld + s) * TW + xo], g);
-              if (sm >= 0) {
-                cp_async8(&T[(r * ld + sm) * TW + xo], g);
-                if (rm >= 0) cp_async8(&T[(rm * ld + sm) * TW + xo], g);
-              }
-            }
+#pragma unroll 1
+      for (int rg = 0; rg < 9; ++rg) {
+        const int c1 = rg / 3, c2 = rg - 3 * c1;
+        const int r1 = da.cnt(c1), r2 = db.cnt(c2);
+        const bool lower = c1 >= c2;
+        const int part = lower ? slot_of(c1, c2) : slot_of(c2, c1);
+        if (r1 == 0 || r2 == 0 || ((zm >> (P_HHHH + part)) & 1u)) continue;
+        const int o1 = da.off(c1), o2 = db.off(c2);
+        const i64 base = __ldg(boff + part);
+        const i64 ldv = lower ? cnt_of(c1, bd) : cnt_of(c2, bd);
+        const int total = r1 * r2;
+        // e = fast + nf * slow, walked without dividing: the memory-contiguous
+        // index (rows for stored parts, columns for transposed ones) is fast
+        const int nf = lower ? r1 : r2;
+        const int2 i0 = divmod_small(tid, nf), di = divmod_small(T122, nf);
+        int fa = i0.y, sl = i0.x;
+        const int dfa = di.y, dsl = di.x;
+        for (int e = tid; e < total; e += T122) {
+          const int p = lower ? fa : sl, u = lower ? sl : fa;
+          fa += dfa;
+          sl += dsl;
+          if (fa >= nf) {
+            fa -= nf;
+            ++sl;
           }
-          o2 += r2;
+          const int2 P = pr[o1 + p], Q = pc[o2 + u];
+          const i64 addr = lower ? base + P.x + (i64)Q.x * ldv : base + Q.x + (i64)P.x * ldv;
+          const double* g = src + addr;
+          const int r = P.y & 0xFF, rm = ((P.y >> 8) & 0xFF) - 1;
+          const int s = Q.y & 0xFF, sm = ((Q.y >> 8) & 0xFF) - 1;
+          cp_async8(&T[(r * ld + s) * TW + xo], g);
+          if (rm >= 0) cp_async8(&T[(rm * ld + s) * TW + xo], g);
+          if (sm >= 0) {
+            cp_async8(&T[(r * ld + sm) * TW + xo], g);
+            if (rm >= 0) cp_async8(&T[(rm * ld + sm) * TW + xo], g);
+          }
         }
-        o1 += r1;
       }
     }
     cp_async_wait_all();
     __syncthreads();
     // orientation and herm signs in place; (t,t) cells and known-zero parts -> 0
-    int fs = tid % nc, fr = tid / nc;
-    const int dfs = T122 % nc, dfr = T122 / nc;
+    const int2 i0 = divmod_small(tid, nc), di = divmod_small(T122, nc);
+    int fs = i0.y, fr = i0.x;
+    const int dfs = di.y, dfr = di.x;
     for (int e = tid; e < nr * nc; e += T122) {
       const int r = fr, s = fs;
       fs += dfs;
@@ -318,6 +331,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
       const bool valid = (ci & cj & 8) != 0;
       const int part = c1 >= c2 ? slot_of(c1, c2) : slot_of(c2, c1);
       const double sg = ((ci ^ cj) & 1) ? -1.0 : 1.0;
+#pragma unroll 1
       for (int x = 0; x < 2; ++x) {
         if (x == 0 ? !useA : !useB) continue;
         const unsigned zm = x == 0 ? zA : zB;
@@ -330,74 +344,216 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
   }
 
   // stored output cells: regions with c1 >= c2, rows of S_a fastest
-  const int xa = 0, xb = TW == 2 ? 1 : 0;
-  int o1 = 0;
-#pragma unroll
-  for (int c1 = 0; c1 < 3; ++c1) {
-    const int r1 = da.cnt[c1];
-    int o2 = 0;
-#pragma unroll
-    for (int c2 = 0; c2 <= c1; ++c2) {
-      const int r2 = db.cnt[c2];
-      if (r1 > 0 && r2 > 0) {
-        const i64 base = __ldg(boff + slot_of(c1, c2));
-        const i64 ldc = cnt_of(c1, bd);
-        int p = tid % r1, u = tid / r1;
-        const int dp = T122 % r1, du = T122 / r1;
-        for (int e = tid; e < r1 * r2; e += T122) {
-          const int2 P = pr[o1 + p], Q = pc[o2 + u];
-          p += dp;
-          u += du;
-          if (p >= r1) {
-            p -= r1;
-            ++u;
-          }
-          double y = 0.0;
-          if (work) {
-            const int r = P.y & 0xFF, s = Q.y & 0xFF;
-            const int k1 = (P.y >> 17) & 15, k2 = (P.y >> 21) & 15;
-            const int l1 = (Q.y >> 17) & 15, l2 = (Q.y >> 21) & 15;
-            const bool h1 = k1 < da.hg, h2 = k2 < da.hh, h3 = l1 < db.hg, h4 = l2 < db.hh;
-            // leg t-ranges: holes [0, h) and particles [h, n) of the leg's group,
-            // each kept only if the one-body factor allows it (sparse: hole <->
-            // particle only) and the staged operand can be non-zero on the cells
-            // it reaches (class pairs of the operand's non-zero parts)
-            const int bL1 = (k2 * ld + s) * TW, sL1 = n2 * ld * TW;        // T((t,k2), s)
-            const int bL2 = (k1 * n2 * ld + s) * TW, sL2 = ld * TW;        // T((k1,t), s)
-            const int bL3 = (r * ld + l2) * TW, sL3 = n4 * TW;             // T(r, (t,l2))
-            const int bL4 = (r * ld + l1 * n4) * TW, sL4 = TW;             // T(r, (l1,t))
-            if (useB) {  // FA x TB
-              y += leg_sum(F1 + k1 * n1, true, T + xb, bL1, sL1, n1, da.hg,
-                           leg_ok(spA, h1, true, h2, c2, nzB), leg_ok(spA, h1, false, h2, c2, nzB));
-              y += leg_sum(F2 + k2 * n2, true, T + xb, bL2, sL2, n2, da.hh,
-                           leg_ok(spA, h2, true, h1, c2, nzB), leg_ok(spA, h2, false, h1, c2, nzB));
-              y -= leg_sum(F3 + l1 * n3, true, T + xb, bL3, sL3, n3, db.hg,
-                           leg_ok(spA, h3, true, h4, c1, nzB), leg_ok(spA, h3, false, h4, c1, nzB));
-              y -= leg_sum(F4 + l2 * n4, true, T + xb, bL4, sL4, n4, db.hh,
-                           leg_ok(spA, h4, true, h3, c1, nzB), leg_ok(spA, h4, false, h3, c1, nzB));
-            }
-            if (useA) {  // -FB x TA
-              y -= leg_sum(F1 + k1 * n1, false, T + xa, bL1, sL1, n1, da.hg,
-                           leg_ok(spB, h1, true, h2, c2, nzA), leg_ok(spB, h1, false, h2, c2, nzA));
-              y -= leg_sum(F2 + k2 * n2, false, T + xa, bL2, sL2, n2, da.hh,
-                           leg_ok(spB, h2, true, h1, c2, nzA), leg_ok(spB, h2, false, h1, c2, nzA));
-              y += leg_sum(F3 + l1 * n3, false, T + xa, bL3, sL3, n3, db.hg,
-                           leg_ok(spB, h3, true, h4, c1, nzA), leg_ok(spB, h3, false, h4, c1, nzA));
-              y += leg_sum(F4 + l2 * n4, false, T + xa, bL4, sL4, n4, db.hh,
-                           leg_ok(spB, h4, true, h3, c1, nzA), leg_ok(spB, h4, false, h3, c1, nzA));
-            }
-            if ((P.y ^ Q.y) & (1 << 16)) y = -y;
-          }
-          double* out = C + base + P.x + (i64)Q.x * ldc;
-          if (acc)
-            *out += y;
-          else
-            *out = y;
+#pragma unroll 1
+  for (int rg = 0; rg < 6; ++rg) {
+    const int c1 = rg < 1 ? 0 : (rg < 3 ? 1 : 2), c2 = rg - (c1 * (c1 + 1)) / 2;  // (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
+    const int r1 = da.cnt(c1), r2 = db.cnt(c2);
+    if (r1 == 0 || r2 == 0) continue;
+    const int o1 = da.off(c1), o2 = db.off(c2);
+    const i64 base = __ldg(boff + slot_of(c1, c2));
+    const i64 ldc = cnt_of(c1, bd);
+    // leg masks of this region (see leg_masks): bra legs fix class c2, ket legs c1
+    const unsigned okB = ((legB >> (8 * c2)) & 0xFFu) | (((legB >> (8 * c1)) & 0xFFu) << 8);
+    const unsigned okA = ((legA >> (8 * c2)) & 0xFFu) | (((legA >> (8 * c1)) & 0xFFu) << 8);
+    const int2 i0 = divmod_small(tid, r1), di = divmod_small(T122, r1);
+    int p = i0.y, u = i0.x;
+    const int dp = di.y, du = di.x;
+    for (int e = tid; e < r1 * r2; e += T122) {
+      const int2 P = pr[o1 + p], Q = pc[o2 + u];
+      p += dp;
+      u += du;
+      if (p >= r1) {
+        p -= r1;
+        ++u;
+      }
+      double y = 0.0;
+      if (work) {
+        const int r = P.y & 0xFF, s = Q.y & 0xFF;
+        const int k1 = (P.y >> 17) & 15, k2 = (P.y >> 21) & 15;
+        const int l1 = (Q.y >> 17) & 15, l2 = (Q.y >> 21) & 15;
+        const int h1 = k1 < da.hg, h2 = k2 < da.hh, h3 = l1 < db.hg, h4 = l2 < db.hh;
+        const int b1 = h1 * 4 + h2 * 2, b2 = h2 * 4 + h1 * 2, b3 = 8 + h3 * 4 + h4 * 2, b4 = 8 + h4 * 4 + h3 * 2;
+        const int bL1 = (k2 * ld + s) * TW, sL1 = n2 * ld * TW;  // T((t,k2), s)
+        const int bL2 = (k1 * n2 * ld + s) * TW, sL2 = ld * TW;  // T((k1,t), s)
+        const int bL3 = (r * ld + l2) * TW, sL3 = n4 * TW;       // T(r, (t,l2))
+        const int bL4 = (r * ld + l1 * n4) * TW, sL4 = TW;       // T(r, (l1,t))
+        if (useB) {  // FA x TB
+          const double* Tb = T + xb_of<TW>();
+          y += leg_sum(F1 + k1 * n1, 0, Tb, bL1, sL1, n1, da.hg, okB >> b1);
+          y += leg_sum(F2 + k2 * n2, 0, Tb, bL2, sL2, n2, da.hh, okB >> b2);
+          y -= leg_sum(F3 + l1 * n3, 0, Tb, bL3, sL3, n3, db.hg, okB >> b3);
+          y -= leg_sum(F4 + l2 * n4, 0, Tb, bL4, sL4, n4, db.hh, okB >> b4);
+        }
+        if (useA) {  // -FB x TA
+          y -= leg_sum(F1 + k1 * n1, 1, T, bL1, sL1, n1, da.hg, okA >> b1);
+          y -= leg_sum(F2 + k2 * n2, 1, T, bL2, sL2, n2, da.hh, okA >> b2);
+          y += leg_sum(F3 + l1 * n3, 1, T, bL3, sL3, n3, db.hg, okA >> b3);
+          y += leg_sum(F4 + l2 * n4, 1, T, bL4, sL4, n4, db.hh, okA >> b4);
+        }
+        if ((P.y ^ Q.y) & (1 << 16)) y = -y;
+      }
+      double* out = C + base + P.x + (i64)Q.x * ldc;
+      if (acc)
+        *out += y;
+      else
+        *out = y;
+    }
+  }
+}
+
+// ---- particle-hole channel of commutator_222 over the same tiles ----------
+// (src/commutators.f90:716-980, ME_general.f90:923-952.)  With Z = XCC - YCC
+// in cross-coupled coordinates and the stored output element oriented as the
+// cells (k1,k2) of S(g,h), (l1,l2) of S(g',h') -- states x = G_g[k1],
+// y = G_h[k2], u = G_g'[l1], v = G_h'[l2] --
+//   C += Z[(u,x),(y,v)] - Z[(u,y),(x,v)] + Z[(v,y),(x,u)] - Z[(v,x),(y,u)].
+// The cc rows are group-major (all rows (i in G1, j in G2) form one run), so
+// each term reads one dense sub-matrix of one cc block: rows G1 x G2 (one run
+// of |G1||G2| doubles per column), columns G3 x G4.  Term t (sign (-1)^t):
+//   t  rows (G1,G2)  columns (G3,G4)  element (rows; columns)
+//   0  (g', g)       (h, h')          (l1,k1; k2,l2)
+//   1  (g', h)       (g, h')          (l1,k2; k1,l2)
+//   2  (h', h)       (g, g')          (l2,k2; k1,l1)
+//   3  (h', g)       (h, g')          (l2,k1; k2,l1)
+// STAGED: per term the CTA copies its sub-matrix into shared memory
+// (cp.async, coalesced runs) and every stored cell adds its element to a
+// shared accumulator; the last term adds the sum into C.  Tiles too large
+// for that read the four elements of each cell from global memory.
+constexpr int TPD = 256;
+
+template <bool STAGED>
+__global__ void __launch_bounds__(TPD) k_pandya_tile(DevLayout L, const int* __restrict__ tasks,
+                                                     const int2* __restrict__ tiles, const int4* __restrict__ gpd,
+                                                     const int2* __restrict__ gpp, const int2* __restrict__ gpg,
+                                                     const int2* __restrict__ zrow, int ng,
+                                                     const double* __restrict__ Z, double* __restrict__ C) {
+  extern __shared__ __align__(16) double smp[];
+  const int2 tl = __ldg(&tiles[__ldg(&tasks[blockIdx.x])]);
+  const GpDesc da = load_gp(gpd, tl.x), db = load_gp(gpd, tl.y);
+  const int2 gb = __ldg(&gpg[tl.x]), gk = __ldg(&gpg[tl.y]);  // (g, h), (g', h')
+  const int n1 = da.n1, n2 = da.n2, n3 = db.n1, n4 = db.n2;
+  const int pa = da.cnt(0) + da.cnt(1) + da.cnt(2), pb = db.cnt(0) + db.cnt(1) + db.cnt(2);
+  const int q = da.q;
+  const int4 bd = __ldg(&L.blk[q]);
+  const i64* boff = L.boff + 6 * q;
+  int nst = 0;  // stored cells: regions c1 >= c2
+#pragma unroll 1
+  for (int c1 = 0; c1 < 3; ++c1)
+    for (int c2 = 0; c2 <= c1; ++c2) nst += da.cnt(c1) * db.cnt(c2);
+  const int zcap = STAGED ? n1 * n2 * n3 * n4 : 0;
+  double* Zs = smp;
+  double* Y = smp + zcap;
+  int2* pr = reinterpret_cast<int2*>(Y + (STAGED ? nst : 0));
+  int2* pc = pr + pa;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < pa; i += TPD) pr[i] = __ldg(&gpp[da.pstart + i]);
+  for (int i = tid; i < pb; i += TPD) pc[i] = __ldg(&gpp[db.pstart + i]);
+  __syncthreads();
+
+#pragma unroll 1
+  for (int term = 0; term < (STAGED ? 4 : 1); ++term) {
+    const double* zb = nullptr;
+    int nrow = 0, m2 = 0, m4 = 0;
+    i64 ldz = 0;
+    if (STAGED) {
+      int G1, G2, G3, G4, m1, m3;
+      if (term == 0) {
+        G1 = gk.x; G2 = gb.x; G3 = gb.y; G4 = gk.y; m1 = n3; m2 = n1; m3 = n2; m4 = n4;
+      } else if (term == 1) {
+        G1 = gk.x; G2 = gb.y; G3 = gb.x; G4 = gk.y; m1 = n3; m2 = n2; m3 = n1; m4 = n4;
+      } else if (term == 2) {
+        G1 = gk.y; G2 = gb.y; G3 = gb.x; G4 = gk.x; m1 = n4; m2 = n2; m3 = n1; m4 = n3;
+      } else {
+        G1 = gk.y; G2 = gb.x; G3 = gb.y; G4 = gk.x; m1 = n4; m2 = n1; m3 = n2; m4 = n3;
+      }
+      const int2 zr = __ldg(&zrow[G1 * ng + G2]);
+      const int cs = __ldg(&zrow[G3 * ng + G4]).y;
+      ldz = __ldg(&L.ccdim[zr.x]).x;
+      zb = Z + __ldg(&L.cczoff[zr.x]) + zr.y + (i64)cs * ldz;
+      nrow = m1 * m2;
+      const int total = nrow * m3 * m4;
+      const int2 i0 = divmod_small(tid, nrow), di = divmod_small(TPD, nrow);
+      int fr = i0.y, fc = i0.x;
+      const int dr = di.y, dc = di.x;
+      for (int e = tid; e < total; e += TPD) {
+        cp_async8(&Zs[e], zb + fr + (i64)fc * ldz);
+        fr += dr;
+        fc += dc;
+        if (fr >= nrow) {
+          fr -= nrow;
+          ++fc;
         }
       }
-      o2 += r2;
+      cp_async_wait_all();
+      __syncthreads();
     }
-    o1 += r1;
+    int j0 = 0;  // first accumulator slot of the region
+#pragma unroll 1
+    for (int rg = 0; rg < 6; ++rg) {
+      const int c1 = rg < 1 ? 0 : (rg < 3 ? 1 : 2), c2 = rg - (c1 * (c1 + 1)) / 2;
+      const int r1 = da.cnt(c1), r2 = db.cnt(c2);
+      if (r1 == 0 || r2 == 0) continue;
+      const int o1 = da.off(c1), o2 = db.off(c2);
+      const i64 base = __ldg(boff + slot_of(c1, c2));
+      const i64 ldc = cnt_of(c1, bd);
+      const int2 i0 = divmod_small(tid, r1), di = divmod_small(TPD, r1);
+      int p = i0.y, u = i0.x;
+      const int dp = di.y, du = di.x;
+      for (int e = tid; e < r1 * r2; e += TPD) {
+        const int2 P = pr[o1 + p], Q = pc[o2 + u];
+        const int k1 = (P.y >> 17) & 15, k2 = (P.y >> 21) & 15;
+        const int l1 = (Q.y >> 17) & 15, l2 = (Q.y >> 21) & 15;
+        double y;
+        if (STAGED) {
+          int zi, zj;
+          if (term == 0) {
+            zi = l1 * m2 + k1; zj = k2 * m4 + l2;
+          } else if (term == 1) {
+            zi = l1 * m2 + k2; zj = k1 * m4 + l2;
+          } else if (term == 2) {
+            zi = l2 * m2 + k2; zj = k1 * m4 + l1;
+          } else {
+            zi = l2 * m2 + k1; zj = k2 * m4 + l1;
+          }
+          const double z = Zs[zi + zj * nrow];
+          y = (term == 0 ? 0.0 : Y[j0 + e]) + ((term & 1) ? -z : z);
+          if (term < 3) Y[j0 + e] = y;
+        } else {
+          // the four elements straight from global memory
+          double t4[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            int G1, G2, G3, G4, a1, a2, a3, a4, s2, s4;
+            if (t == 0) {
+              G1 = gk.x; G2 = gb.x; G3 = gb.y; G4 = gk.y; a1 = l1; a2 = k1; a3 = k2; a4 = l2; s2 = n1; s4 = n4;
+            } else if (t == 1) {
+              G1 = gk.x; G2 = gb.y; G3 = gb.x; G4 = gk.y; a1 = l1; a2 = k2; a3 = k1; a4 = l2; s2 = n2; s4 = n4;
+            } else if (t == 2) {
+              G1 = gk.y; G2 = gb.y; G3 = gb.x; G4 = gk.x; a1 = l2; a2 = k2; a3 = k1; a4 = l1; s2 = n2; s4 = n3;
+            } else {
+              G1 = gk.y; G2 = gb.x; G3 = gb.y; G4 = gk.x; a1 = l2; a2 = k1; a3 = k2; a4 = l1; s2 = n1; s4 = n3;
+            }
+            const int2 zr = __ldg(&zrow[G1 * ng + G2]);
+            const int cs = __ldg(&zrow[G3 * ng + G4]).y;
+            const i64 r = __ldg(&L.ccdim[zr.x]).x;
+            t4[t] = __ldg(Z + __ldg(&L.cczoff[zr.x]) + zr.y + a1 * s2 + a2 + (cs + a3 * s4 + a4) * r);
+          }
+          y = t4[0] - t4[1] + t4[2] - t4[3];
+        }
+        p += dp;
+        u += du;
+        if (p >= r1) {
+          p -= r1;
+          ++u;
+        }
+        if (!STAGED || term == 3) {
+          if ((P.y ^ Q.y) & (1 << 16)) y = -y;
+          C[base + P.x + (i64)Q.x * ldc] += y;
+        }
+      }
+      j0 += r1 * r2;
+    }
+    if (STAGED) __syncthreads();  // the next term overwrites Zs
   }
 }
 
@@ -409,6 +565,12 @@ struct TileInfo {
   int nf, npair;     // F entries (double2) and pair entries of the two group pairs
   int nr, nc;
   unsigned parts;    // two-body parts the tile touches (bit = vectorize slot)
+  int nst;           // stored output cells
+};
+struct PdBucket {  // one launch of the particle-hole tile kernel
+  int first, count;
+  size_t smem;
+  bool staged;
 };
 struct Bucket122 {
   int tw;       // doubles per staged cell
@@ -424,6 +586,9 @@ struct TaskSet {
   std::vector<int2> h_task;  // host copy (merged launches of several layouts)
   std::vector<Bucket122> buckets;
   bool tuned = false;
+  int bounds_id = 0;           // which bucketing (see kBounds) the tuner kept
+  float ms_total = 0.f;        // tuned time of this bucketing
+  std::vector<TaskSet> alts;   // the other bucketings, until tuned
 };
 struct Plan122 {
   int4* d_gpd = nullptr;
@@ -435,6 +600,13 @@ struct Plan122 {
   int gmax = 0, nfent = 0;
   std::vector<TileInfo> tiles;
   std::map<std::pair<unsigned, unsigned>, TaskSet> sets;  // per (zero mask A, zero mask B)
+  // particle-hole channel: groups (g, h) of each group pair, the first cc row
+  // of each group pair (G1, G2) as {cc block, row}, the tasks (tile indices)
+  int2* d_gpg = nullptr;
+  int2* d_zrow = nullptr;
+  int ng = 0;
+  int* d_ptask = nullptr;
+  std::vector<PdBucket> pbuckets;
 };
 std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
@@ -494,7 +666,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
   for (int s = 0; s < m; ++s) sbase[s] = goff[L->gid[s]] + kpos[s] * gsz[L->gid[s]];
 
   std::vector<int4> gpd;
-  std::vector<int2> gpp;
+  std::vector<int2> gpp, gpg;
   std::vector<unsigned char> cinfo;
   struct GpHost {
     int n1, n2, cnt[3], nf, npair;
@@ -555,6 +727,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
       d.npair = d.cnt[0] + d.cnt[1] + d.cnt[2];
       gpd.push_back(int4{q, d.n1 | (d.n2 << 8) | ((g == h ? 1 : 0) << 16), holes[g] | (holes[h] << 8), goff[g]});
       gpd.push_back(int4{goff[h], (int)gpp.size(), (int)cinfo.size(), d.cnt[0] | (d.cnt[1] << 10) | (d.cnt[2] << 20)});
+      gpg.push_back(int2{g, h});
       gpp.insert(gpp.end(), plist[u].begin(), plist[u].end());
       cinfo.insert(cinfo.end(), cl[u].begin(), cl[u].end());
     }
@@ -581,6 +754,9 @@ static int plan_122(qd_layout* L, Plan122** out) {
         t.nf = A.nf + B.nf;
         t.npair = A.npair + B.npair;
         t.parts = parts;
+        t.nst = 0;
+        for (int c1 = 0; c1 < 3; ++c1)
+          for (int c2 = 0; c2 <= c1; ++c2) t.nst += A.cnt[c1] * B.cnt[c2];
         p.tiles.push_back(t);
       }
   }
@@ -596,10 +772,58 @@ static int plan_122(qd_layout* L, Plan122** out) {
       (rc = upload_vec(L, cinfo, &p.d_cinfo)) || (rc = upload_vec(L, th, &p.d_tiles)) ||
       (rc = upload_vec(L, sbase, &p.d_sbase)))
     return rc;
+  // particle-hole channel: first cc row of each (G1, G2) and the launches
+  p.ng = ngroup;
+  std::vector<int2> zrow((size_t)ngroup * ngroup);
+  for (int g1 = 0; g1 < ngroup; ++g1)
+    for (int g2 = 0; g2 < ngroup; ++g2)
+      zrow[(size_t)g1 * ngroup + g2] = L->ccmap[(size_t)L->gmem[L->gstart[g1]] * m + L->gmem[L->gstart[g2]]];
+  {
+    std::vector<std::pair<size_t, int>> lst;  // (shared memory, tile), staged tiles
+    std::vector<int> direct;
+    for (size_t i = 0; i < p.tiles.size(); ++i) {
+      const TileInfo& t = p.tiles[i];
+      const size_t sm = 8 * ((size_t)t.cells + t.nst + t.npair);
+      if (sm <= SMEM_MAX_122)
+        lst.push_back({sm, (int)i});
+      else
+        direct.push_back((int)i);
+    }
+    std::stable_sort(lst.begin(), lst.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<int> tasks;
+    const size_t bounds[4] = {24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122};
+    auto interval = [&](size_t sm) {
+      int l = 0;
+      while (l < 3 && sm > bounds[l]) ++l;
+      return l;
+    };
+    size_t i = 0;
+    while (i < lst.size()) {  // buckets: tiles of one size interval, largest first
+      const int l = interval(lst[i].first);
+      PdBucket b{(int)tasks.size(), 0, lst[i].first, true};
+      while (i < lst.size() && interval(lst[i].first) == l) tasks.push_back(lst[i++].second);
+      b.count = (int)tasks.size() - b.first;
+      p.pbuckets.push_back(b);
+    }
+    if (!direct.empty()) {
+      PdBucket b{(int)tasks.size(), (int)direct.size(), 0, false};
+      for (int t : direct) {
+        tasks.push_back(t);
+        b.smem = std::max(b.smem, 8 * (size_t)p.tiles[t].npair);
+      }
+      p.pbuckets.push_back(b);
+    }
+    int rc2;
+    if ((rc2 = upload_vec(L, gpg, &p.d_gpg)) || (rc2 = upload_vec(L, zrow, &p.d_zrow)) ||
+        (rc2 = upload_vec(L, tasks, &p.d_ptask)))
+      return rc2;
+  }
   QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)std::max(1, p.nfent)));
   L->ws_bytes += (i64)sizeof(double2) * 2 * p.nfent;
-  for (const void* fn : {(const void*)k_122_tile<1, 128>, (const void*)k_122_tile<2, 128>,
-                         (const void*)k_122_tile<1, 256>, (const void*)k_122_tile<2, 256>}) {
+  for (const void* fn : {(const void*)k_122_tile<1, 128, false>, (const void*)k_122_tile<2, 128, false>,
+                         (const void*)k_122_tile<1, 256, false>, (const void*)k_122_tile<2, 256, false>,
+                         (const void*)k_122_tile<1, 256, true>, (const void*)k_122_tile<2, 256, true>,
+                         (const void*)k_pandya_tile<true>, (const void*)k_pandya_tile<false>}) {
     cudaFuncAttributes fa;
     QD_CUDA(cudaFuncGetAttributes(&fa, fn));
     QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -614,6 +838,55 @@ static int plan_122(qd_layout* L, Plan122** out) {
 // buckets of similar shared memory (largest first).  A tile that needs both
 // terms but does not fit with both operands staged runs as a B task that
 // sets C and an A task (in a later launch) that accumulates.
+// Bucketings the autotuner chooses from: the size bounds (bytes of shared
+// memory) that split each list into launches.  More buckets give small tiles
+// more CTAs per SM; fewer keep the tiles of one column strip in one launch.
+constexpr int kNumBounds = 3;
+const size_t kBounds[kNumBounds][4] = {{24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122},
+                                       {56 * 1024, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122},
+                                       {SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122}};
+
+// One bucketing of the task lists: buckets by size bound (largest first),
+// and within a bucket the tiles sharing a column strip (block q, column
+// group pair b) together: their gathers read the same columns, whose memory
+// atoms also hold neighbouring group pairs' rows, so concurrent CTAs hit in
+// L2.
+static int build_variant(qd_layout* L, const Plan122* p, std::vector<std::pair<size_t, int2>> lst_in[3], int bid,
+                         TaskSet& ts) {
+  std::vector<int2> all;
+  const size_t* bounds = kBounds[bid];
+  ts.bounds_id = bid;
+  for (int l = 0; l < 3; ++l) {
+    std::vector<std::pair<size_t, int2>> v = lst_in[l];
+    std::stable_sort(v.begin(), v.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    size_t i = 0;
+    while (i < v.size()) {
+      // bucket: tasks down to the next size bound below the first one
+      const size_t top = v[i].first;
+      size_t lower = 0;
+      for (int k = 0; k < 4; ++k)
+        if (bounds[k] < top) lower = std::max(lower, bounds[k]);
+      Bucket122 b;
+      b.tw = l == 1 ? 2 : 1;
+      b.list = l;
+      b.first = (int)all.size();
+      b.smem = top;
+      while (i < v.size() && v[i].first > lower) all.push_back(v[i++].second);
+      b.count = (int)all.size() - b.first;
+      ts.buckets.push_back(b);
+    }
+  }
+  for (const Bucket122& bk : ts.buckets)
+    std::stable_sort(all.begin() + bk.first, all.begin() + bk.first + bk.count, [&](const int2& x, const int2& y) {
+      const TileInfo &tx = p->tiles[x.x], &ty = p->tiles[y.x];
+      return tx.b != ty.b ? tx.b < ty.b : tx.a < ty.a;
+    });
+  int rc = upload_vec(L, all, &ts.d_task);
+  if (rc) return rc;
+  ts.h_task = all;
+  return QD_OK;
+}
+
 static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet** out) {
   std::lock_guard<std::mutex> lock(g_plan_mutex);
   auto key = std::make_pair(zA, zB);
@@ -643,39 +916,11 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
     }
   }
   TaskSet ts;
-  std::vector<int2> all;
-  const size_t bounds[4] = {24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122};
-  for (int l = 0; l < 3; ++l) {
-    auto& v = lst[l];
-    std::stable_sort(v.begin(), v.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-    size_t i = 0;
-    while (i < v.size()) {
-      // bucket: tasks down to the next size bound below the first one
-      const size_t top = v[i].first;
-      size_t lower = 0;
-      for (size_t bnd : bounds)
-        if (bnd < top) lower = bnd;
-      Bucket122 b;
-      b.tw = l == 1 ? 2 : 1;
-      b.list = l;
-      b.first = (int)all.size();
-      b.smem = top;
-      while (i < v.size() && v[i].first > lower) all.push_back(v[i++].second);
-      b.count = (int)all.size() - b.first;
-      ts.buckets.push_back(b);
-    }
+  for (int bid = 0; bid < kNumBounds; ++bid) {
+    TaskSet& v = bid == 0 ? ts : (ts.alts.emplace_back(), ts.alts.back());
+    int rc = build_variant(L, p, lst, bid, v);
+    if (rc) return rc;
   }
-  // within a bucket, tiles sharing a column strip (block q, column group pair
-  // b) run together: their gathers read the same columns, whose memory atoms
-  // also hold neighbouring group pairs' rows, so concurrent CTAs hit in L2
-  for (const Bucket122& bk : ts.buckets)
-    std::stable_sort(all.begin() + bk.first, all.begin() + bk.first + bk.count, [&](const int2& x, const int2& y) {
-      const TileInfo &tx = p->tiles[x.x], &ty = p->tiles[y.x];
-      return tx.b != ty.b ? tx.b < ty.b : tx.a < ty.a;
-    });
-  int rc = upload_vec(L, all, &ts.d_task);
-  if (rc) return rc;
-  ts.h_task = all;
   p->sets[key] = ts;
   *out = &p->sets[key];
   return QD_OK;
@@ -687,10 +932,13 @@ void drop_122_plan(const qd_layout* L) {
   if (it == plans().end()) return;
   Plan122& p = it->second;
   for (void* ptr : {(void*)p.d_gpd, (void*)p.d_gpp, (void*)p.d_cinfo, (void*)p.d_tiles, (void*)p.d_sbase,
-                    (void*)p.d_ftab})
+                    (void*)p.d_ftab, (void*)p.d_gpg, (void*)p.d_zrow, (void*)p.d_ptask})
     if (ptr) cudaFree(ptr);
-  for (auto& kv : p.sets)
+  for (auto& kv : p.sets) {
     if (kv.second.d_task) cudaFree(kv.second.d_task);
+    for (TaskSet& t : kv.second.alts)
+      if (t.d_task) cudaFree(t.d_task);
+  }
   plans().erase(it);
 }
 
@@ -705,15 +953,29 @@ static unsigned nz_mask(unsigned zmask) {
   return nz;
 }
 
+// Leg masks of one term, per launch: byte cfix (0..2) holds bit
+// kh * 4 + oh * 2 + th, set when a leg with fixed class cfix can add anything
+// whose fixed state has kind kh, whose other state on the same side has kind
+// oh and whose summed states have kind th (1 = hole); `sparse` is the one-body
+// factor's sparsity, zstaged the zero-part mask of the staged operand.
+static unsigned leg_masks(int sparse, unsigned zstaged) {
+  const unsigned nz = nz_mask(zstaged);
+  unsigned m = 0;
+  for (int cfix = 0; cfix < 3; ++cfix)
+    for (int bits = 0; bits < 8; ++bits)
+      if (leg_ok(sparse, (bits >> 2) & 1, bits & 1, (bits >> 1) & 1, cfix, nz)) m |= 1u << (8 * cfix + bits);
+  return m;
+}
+
 static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, const Bucket122& b, int threads,
                          const qd_op* A, const qd_op* B, int spA, int spB, double* C) {
+  // the B term (FA x TB) and the A term (-FB x TA)
+  const unsigned legB = leg_masks(spA, B->zero_mask), legA = leg_masks(spB, A->zero_mask);
 #define QD_122_LAUNCH(TW, NT)                                                                                   \
-  k_122_tile<TW, NT><<<b.count, NT, b.smem, L->stream>>>(L->dev, ts->d_task + b.first, p->d_tiles, p->d_gpd,   \
+  k_122_tile<TW, NT, false><<<b.count, NT, b.smem, L->stream>>>(L->dev, ts->d_task + b.first, p->d_tiles, p->d_gpd,   \
                                                          p->d_gpp, p->d_cinfo, p->d_ftab, p->nfent, A->d,       \
-                                                         (double)A->herm, A->zero_mask, spA, B->d,              \
-                                                         (double)B->herm, B->zero_mask, spB, C,                \
-                                                         nz_mask(A->zero_mask), nz_mask(B->zero_mask), nullptr, \
-                                                         nullptr)
+                                                         (double)A->herm, A->zero_mask, legA, B->d,             \
+                                                         (double)B->herm, B->zero_mask, legB, C, nullptr, nullptr)
   if (b.tw == 2) {
     if (threads == 128) QD_122_LAUNCH(2, 128); else QD_122_LAUNCH(2, 256);
   } else {
@@ -730,13 +992,9 @@ static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, cons
 // writing into a scratch operator of the layout, and keeps the faster size
 // per bucket.  Every output cell is summed by one thread in a fixed order
 // whatever the CTA size, so the choice never changes a result.
-static int tune_122(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, const qd_op* B, int spA, int spB) {
-  double* scratch = scratch_operator(L);
-  if (!scratch) return QD_OK;  // no scratch: keep the defaults
-  cudaEvent_t e0, e1;
-  QD_CUDA(cudaEventCreate(&e0));
-  QD_CUDA(cudaEventCreate(&e1));
-  const long long n0 = L->nlaunch;
+static int tune_variant(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, const qd_op* B, int spA, int spB,
+                        double* scratch, cudaEvent_t e0, cudaEvent_t e1) {
+  ts->ms_total = 0.f;
   for (Bucket122& b : ts->buckets) {
     for (int v = 0; v < 2; ++v) {
       const int threads = v ? 256 : 128;
@@ -753,6 +1011,55 @@ static int tune_122(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, const
       b.ms[v] = best;
     }
     b.threads = b.ms[0] < b.ms[1] ? 128 : 256;
+    ts->ms_total += std::min(b.ms[0], b.ms[1]);
+  }
+  return QD_OK;
+}
+
+// Autotuner: the first launch of a task set times, for every bucketing
+// (kBounds), every bucket with 128- and 256-thread CTAs (CUDA events, best of
+// two runs each) on the real operands, writing into a scratch operator of
+// the layout; it keeps the CTA size per bucket and the bucketing with the
+// least total time.  Every output cell is summed by one thread in a fixed
+// order whatever the bucketing or CTA size, so the choice never changes a
+// result.
+static int tune_122(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, const qd_op* B, int spA, int spB) {
+  double* scratch = scratch_operator(L);
+  if (!scratch) return QD_OK;  // no scratch: keep the defaults
+  cudaEvent_t e0, e1;
+  QD_CUDA(cudaEventCreate(&e0));
+  QD_CUDA(cudaEventCreate(&e1));
+  const long long n0 = L->nlaunch;
+  TRY(tune_variant(L, p, ts, A, B, spA, spB, scratch, e0, e1));
+  for (TaskSet& alt : ts->alts) TRY(tune_variant(L, p, &alt, A, B, spA, spB, scratch, e0, e1));
+  int best = -1;
+  float tbest = ts->ms_total;
+  for (size_t k = 0; k < ts->alts.size(); ++k)
+    if (ts->alts[k].ms_total < tbest) {
+      tbest = ts->alts[k].ms_total;
+      best = (int)k;
+    }
+  // keep the winner in *ts; the others stay in alts for the report (their task arrays are freed)
+  std::vector<TaskSet> others;
+  TaskSet win;
+  if (best >= 0) {
+    win = ts->alts[best];
+    ts->alts[best] = TaskSet();
+    TaskSet cur = *ts;
+    cur.alts.clear();
+    others.push_back(cur);
+  }
+  for (TaskSet& t : ts->alts)
+    if (t.d_task || !t.buckets.empty()) others.push_back(t);
+  if (best >= 0) {
+    *ts = win;
+  }
+  ts->alts.clear();
+  for (TaskSet& t : others) {
+    if (t.d_task) cudaFree(t.d_task);
+    t.d_task = nullptr;
+    t.h_task.clear();
+    ts->alts.push_back(t);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -769,8 +1076,15 @@ std::string tuning_report_122(const qd_layout* L) {
   std::string out;
   char line[256];
   for (const auto& kv : it->second.sets) {
-    snprintf(line, sizeof(line), "commutator_122 masks A=0x%03x B=0x%03x:\n", kv.first.first, kv.first.second);
+    const TaskSet& ts = kv.second;
+    snprintf(line, sizeof(line), "commutator_122 masks A=0x%03x B=0x%03x: bucketing %d kept (%.4f ms)",
+             kv.first.first, kv.first.second, ts.bounds_id, ts.ms_total);
     out += line;
+    for (const TaskSet& t : ts.alts) {
+      snprintf(line, sizeof(line), ", bucketing %d %.4f ms", t.bounds_id, t.ms_total);
+      out += line;
+    }
+    out += "\n";
     for (const Bucket122& b : kv.second.buckets) {
       snprintf(line, sizeof(line), "  tiles %6d staged %d smem %6zu B: 128 thr %.4f ms, 256 thr %.4f ms -> %d\n",
                b.count, b.tw, b.smem, b.ms[0], b.ms[1], b.threads);
@@ -824,6 +1138,29 @@ int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   ++L->nlaunch;
   if (!ts->tuned && !L->prof.on && !capturing(L->stream)) TRY(tune_122(L, p, ts, A, B, spA, spB));
   for (const Bucket122& b : ts->buckets) TRY(launch_bucket(L, p, ts, b, b.threads, A, B, spA, spB, C));
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
+int prepare_pandya(qd_layout* L) {
+  Plan122* p;
+  return plan_122(L, &p);
+}
+
+int launch_pandya_tiles(qd_layout* L, const double* Z, double* C) {
+  Plan122* p;
+  int rc = plan_122(L, &p);
+  if (rc) return rc;
+  for (const PdBucket& b : p->pbuckets) {
+    if (b.count == 0) continue;
+    if (b.staged)
+      k_pandya_tile<true><<<b.count, TPD, b.smem, L->stream>>>(L->dev, p->d_ptask + b.first, p->d_tiles, p->d_gpd,
+                                                               p->d_gpp, p->d_gpg, p->d_zrow, p->ng, Z, C);
+    else
+      k_pandya_tile<false><<<b.count, TPD, b.smem, L->stream>>>(L->dev, p->d_ptask + b.first, p->d_tiles, p->d_gpd,
+                                                                p->d_gpp, p->d_gpg, p->d_zrow, p->ng, Z, C);
+    ++L->nlaunch;
+  }
   QD_CUDA(cudaGetLastError());
   return QD_OK;
 }
@@ -952,26 +1289,24 @@ int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
     I.A = it.A->d;
     I.hA = (double)it.A->herm;
     I.zA = it.A->zero_mask;
-    I.spA = spars(it.A);
+    I.legA = leg_masks(spars(it.B), it.A->zero_mask);
     I.B = it.B->d;
     I.hB = (double)it.B->herm;
     I.zB = it.B->zero_mask;
-    I.spB = spars(it.B);
+    I.legB = leg_masks(spars(it.A), it.B->zero_mask);
     I.C = it.C;
-    I.nzA = nz_mask(it.A->zero_mask);
-    I.nzB = nz_mask(it.B->zero_mask);
   }
   QD_CUDA(cudaMemcpyAsync(m->d_inst, m->h_inst, n * sizeof(Inst122), cudaMemcpyHostToDevice, st));
   const DevLayout& L0 = items[0].L->dev;
   for (const Bucket122& b : m->buckets) {
     if (b.tw == 2)
-      k_122_tile<2, 256><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
-                                                       nullptr, 0, nullptr, 0.0, 0u, 0, nullptr, 0.0, 0u, 0, nullptr,
-                                                       0u, 0u, m->d_tinst + b.first, m->d_inst);
+      k_122_tile<2, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
+                                                       nullptr, 0, nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
+                                                       m->d_tinst + b.first, m->d_inst);
     else
-      k_122_tile<1, 256><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
-                                                       nullptr, 0, nullptr, 0.0, 0u, 0, nullptr, 0.0, 0u, 0, nullptr,
-                                                       0u, 0u, m->d_tinst + b.first, m->d_inst);
+      k_122_tile<1, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
+                                                       nullptr, 0, nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
+                                                       m->d_tinst + b.first, m->d_inst);
     ++items[0].L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());

@@ -398,61 +398,14 @@ int launch_calc_cc(qd_layout* L, const qd_op* H, double* X) {
   return QD_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Particle-hole channel of commutator_222 (src/commutators.f90:716-980):
-// with legs (1,2|3,4) of the stored element and Z = XCC - YCC,
-//   C += Z[31](r31,r24) - Z[32](r32,r14) + Z[42](r42,r13) - Z[41](r41,r23).
-// Stored pairs are (a<b); the reference's particle-first naming of ph pairs
-// with pre = -1 is the same element by antisymmetry.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double zget(const DevLayout& L, const double* __restrict__ Z, int x, int y, int u, int v) {
-  int2 a = __ldg(&L.ccmap[x * L.m + y]);
-  int2 b = __ldg(&L.ccmap[u * L.m + v]);
-  int r = __ldg(&L.ccdim[a.x]).x;
-  return Z[__ldg(&L.cczoff[a.x]) + a.y + (i64)b.y * r];
-}
-
-__device__ __forceinline__ void decode2b(const DevLayout& L, i64 e, int& q, int& part, int& row, int& col) {
-  int s = find_seg(L.s2off, L.ns2, e);
-  int id = __ldg(L.s2id + s);
-  q = id >> 3;
-  part = P_HHHH + (id & 7);
-  i64 loc = e - __ldg(L.s2off + s);
-  int rows = part_rows(part, __ldg(&L.blk[q]));
-  row = (int)(loc % rows);
-  col = (int)(loc / rows);
-}
-
-__global__ void k_pandya_gather(DevLayout L, const double* __restrict__ Z, double* __restrict__ C) {
-  i64 e = L.o2 + (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= L.neq) return;
-  int q, part, row, col;
-  decode2b(L, e, q, part, row, col);
-  int cb, ck;
-  part_classes(part, cb, ck);
-  int2 br = block_pair(L, q, cb, row), kt = block_pair(L, q, ck, col);
-  const int b1 = br.x, b2 = br.y, k1 = kt.x, k2 = kt.y;
-  double X = zget(L, Z, k1, b1, b2, k2) - zget(L, Z, k1, b2, b1, k2) + zget(L, Z, k2, b2, b1, k1) -
-             zget(L, Z, k2, b1, b2, k1);
-  C[e] += X;
-}
-
-int launch_pandya_gather(qd_layout* L, const double* Z, double* C) {
-  i64 n2 = L->neq - L->dev.o2;
-  if (n2 > 0) {
-    k_pandya_gather<<<(unsigned)((n2 + 255) / 256), 256, 0, L->stream>>>(L->dev, Z, C);
-    ++L->nlaunch;
-  }
-  QD_CUDA(cudaGetLastError());
-  return QD_OK;
-}
-
+// Device memory of the particle-hole channel: Z and the tile plan that
+// re-couples it (built here, ahead of any stream capture).
 int ensure_z(qd_layout* L) {
   if (!L->d_z && L->zsize > 0) {
     QD_CUDA(cudaMalloc(&L->d_z, sizeof(double) * L->zsize));
     L->ws_bytes += sizeof(double) * L->zsize;
   }
-  return QD_OK;
+  return prepare_pandya(L);
 }
 
 }  // namespace qd

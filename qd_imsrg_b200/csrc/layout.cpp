@@ -165,8 +165,12 @@ int layout_build(qd_layout* L, int nbody, int emax, const double* eig) {
   L->gstart[keys.size()] = (int)L->gmem.size();
 
   // build_cross_coupled: ML in [-MLmax, MLmax], MS in [-2, 2]; rows are all
-  // ordered pairs (i,j) with ml_i-ml_j = ML, ms_i-ms_j = MS in loop order;
-  // columns are the (hole i, particle j) pairs among them.
+  // ordered pairs (i,j) with ml_i-ml_j = ML, ms_i-ms_j = MS; columns are the
+  // (hole i, particle j) pairs among them, in loop order.  The reference
+  // orders the rows by (i, j); here they go by the (ml,ms) group of i first,
+  // so that the rows (i in G1, j in G2) are one run and a product block
+  // Z[(G1,G2),(G3,G4)] is a dense sub-matrix.  ccref keeps the reference
+  // row of each row (for downloads).
   int mlmax_sp = 0;
   for (int s = 0; s < m; ++s) mlmax_sp = std::max(mlmax_sp, L->qn[3 * s + 1]);
   L->mlmax = 2 * mlmax_sp;
@@ -174,6 +178,7 @@ int layout_build(qd_layout* L, int nbody, int emax, const double* eig) {
   L->ccmap.assign((size_t)m * m, int2{-1, -1});
   L->ccdim.assign(L->ncc, int2{0, 0});
   L->ccab.clear();
+  L->ccref.clear();
   L->cchp.clear();
   L->ccab_base.assign(L->ncc + 1, 0);
   L->cchp_base.assign(L->ncc + 1, 0);
@@ -186,18 +191,30 @@ int layout_build(qd_layout* L, int nbody, int emax, const double* eig) {
       L->ccab_base[cq] = (int)L->ccab.size();
       L->cchp_base[cq] = (int)L->cchp.size();
       int r = 0, nb = 0;
+      // reference row of (i, j): position in the (i, j) loop order
+      std::vector<int> refrow;
       for (int i = 0; i < m; ++i)
         for (int j = 0; j < m; ++j) {
           if (L->qn[3 * i + 1] - L->qn[3 * j + 1] != ML) continue;
           if (L->qn[3 * i + 2] - L->qn[3 * j + 2] != MS) continue;
-          L->ccmap[(size_t)i * m + j] = int2{cq, r};
-          L->ccab.push_back(int2{i, j});
-          ++r;
+          refrow.push_back(i * m + j);
           if (i < n && j >= n) {
             L->cchp.push_back(int2{i, j});
             ++nb;
           }
         }
+      std::vector<int> refpos((size_t)m * m, -1);
+      for (size_t t = 0; t < refrow.size(); ++t) refpos[refrow[t]] = (int)t;
+      for (size_t g = 0; g < keys.size(); ++g)
+        for (int i : mem[g])
+          for (int j = 0; j < m; ++j) {
+            if (L->qn[3 * i + 1] - L->qn[3 * j + 1] != ML) continue;
+            if (L->qn[3 * i + 2] - L->qn[3 * j + 2] != MS) continue;
+            L->ccmap[(size_t)i * m + j] = int2{cq, r};
+            L->ccab.push_back(int2{i, j});
+            L->ccref.push_back(refpos[(size_t)i * m + j]);
+            ++r;
+          }
       L->ccdim[cq] = int2{r, nb};
       L->ccxoff[cq] = xo;
       L->cczoff[cq] = zo;

@@ -150,6 +150,10 @@ struct qd_layout {
   std::vector<int> ptab, gid, gstart, gmem;
   std::vector<int2> ccmap, ccdim, ccab, cchp;
   std::vector<int> ccab_base, cchp_base;
+  // Rows of a cc block are ordered by the (ml,ms) group of their first state,
+  // then (i, j): the rows (i in G1, j in G2) form one run.  ccref maps each
+  // row (indexed like ccab) to its row in the reference's (i, j) loop order.
+  std::vector<int> ccref;
   std::vector<qd::i64> ccxoff, cczoff;
   qd::i64 xsize = 0, zsize = 0;
   std::vector<qd::i64> s2off, pcum;
@@ -259,7 +263,10 @@ int launch_221_trace(qd_layout* L, const qd_op* A, const qd_op* B, const qd_op* 
 int launch_221_fused(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
 int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C);
 int launch_calc_cc(qd_layout* L, const qd_op* H, double* X);
-int launch_pandya_gather(qd_layout* L, const double* Z, double* C);
+// Particle-hole channel (commutators.f90:716-980): C += the four re-coupled
+// Z terms, over the commutator_122 tiles (kernels_122.cu).
+int launch_pandya_tiles(qd_layout* L, const double* Z, double* C);
+int prepare_pandya(qd_layout* L);
 int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
                 unsigned maskB);
 void fill_random(const qd_layout* L, int herm, uint64_t seed, double sigma, int conserve, double* out);
