@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--nbody", type=int, default=NBODY)
     ap.add_argument("--emax", type=int, default=EMAX)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="flow: launch every kernel eagerly (a profiler then lists every launch)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-stride", type=int, default=8)
     ap.add_argument("--batch-max-iter", type=int, default=300, help="batch: flow step limit per instance")
@@ -512,6 +514,8 @@ def run_flow(args, world, rank, local):
     P = qd.Layout(args.nbody, args.emax, eig=eig, device=local)
     stream = torch.cuda.Stream(device=device)
     P.set_stream(stream.cuda_stream)
+    if args.no_graphs:
+        P.set_graphs(False)
     H, HS = qd.FullHam(P, 1, vec), qd.FullHam(P, 1)
 
     def flow():
@@ -581,6 +585,7 @@ def run_flow(args, world, rank, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic: Coulomb TBMEs from v_int and Hartree-Fock computed on the host",
                 "config": {"workload": flow_desc(args), "form": form_name(args.split),
+                           "cuda_graphs": not args.no_graphs,
                            "chosen_form": "plain FP64 block contractions, BCH terms replayed as CUDA graphs: on "
                                           "this ladders-only flow the split form (--split S) and the learned "
                                           "warm start (--workload warmstart) measure slower",

@@ -66,14 +66,12 @@ __device__ __forceinline__ int cnt_of(int c, int4 bd) { return c == 0 ? bd.x : (
 
 // Group-pair descriptor (two int4 per group pair u):
 //   d0 = {q, n1 | n2 << 8 | (g == h) << 16, holes(g) | holes(h) << 8, F offset of g}
-//   d1 = {F offset of h, first pair entry, first cell entry, cnt_hh | cnt_ph << 10 | cnt_pp << 20}
+//   d1 = {F offset of h, first pair entry, 0, cnt_hh | cnt_ph << 10 | cnt_pp << 20}
 // Pair entries (int2, sorted by class then index within the class):
 //   {index w within its class, primary cell | (mirror cell + 1) << 8 | (sign < 0) << 16 |
 //    k1 << 17 | k2 << 21}, the primary cell being (k1, k2) = k1 * n2 + k2
-// Cell entries (one byte per cell of the n1 x n2 grid):
-//   valid << 3 | class << 1 | (sign < 0); 0 for the (t,t) cells of g = h.
 struct GpDesc {
-  int q, n1, n2, hg, hh, fg, fh, pstart, cstart, cntw;
+  int q, n1, n2, hg, hh, fg, fh, pstart, cntw;
   // pairs of class c (0 hh, 1 ph, 2 pp), decoded from the packed word (no local array)
   __device__ __forceinline__ int cnt(int c) const { return (cntw >> (10 * c)) & 0x3FF; }
   // pairs of the classes before c
@@ -90,7 +88,6 @@ __device__ __forceinline__ GpDesc load_gp(const int4* __restrict__ gpd, int u) {
   d.fg = a.w;
   d.fh = b.x;
   d.pstart = b.y;
-  d.cstart = b.z;
   d.cntw = b.w;
   return d;
 }
@@ -126,6 +123,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N committed groups of this thread are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // q = a / b and r = a % b for 0 <= a < 2^22 - 1 and b >= 1, through one
 // single-precision reciprocal instead of an integer division: the exact value
@@ -175,7 +176,6 @@ struct Inst122 {
   const int2* tiles;
   const int4* gpd;
   const int2* gpp;
-  const unsigned char* cinfo;
   const double2* F;
   int nfent;
   const double* A;
@@ -200,7 +200,6 @@ template <int TW, int T122, bool MULTI>
 __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, const int2* __restrict__ tasks,
                                                    const int2* __restrict__ tiles, const int4* __restrict__ gpd,
                                                    const int2* __restrict__ gpp,
-                                                   const unsigned char* __restrict__ cinfo,
                                                    const double2* __restrict__ F, int nfent,
                                                    const double* __restrict__ A, double hA, unsigned zA, unsigned legA,
                                                    const double* __restrict__ B, double hB, unsigned zB, unsigned legB,
@@ -213,7 +212,6 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
     tiles = I.tiles;
     gpd = I.gpd;
     gpp = I.gpp;
-    cinfo = I.cinfo;
     F = I.F;
     nfent = I.nfent;
     A = I.A;
@@ -237,7 +235,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
   const int pa = da.cnt(0) + da.cnt(1) + da.cnt(2), pb = db.cnt(0) + db.cnt(1) + db.cnt(2);
   const int4 bd = __ldg(&L.blk[q]);
   const i64* boff = L.boff + 6 * q;
-  // shared memory: T [nr][ld][TW] | F1 F2 F3 F4 (double2) | row, column pairs (int2) | cell bytes
+  // shared memory: T [nr][ld][TW] | F1 F2 F3 F4 (double2) | row, column pairs (int2)
   double* T = sm122;
   const int tsz = (nr * ld * TW + 1) & ~1;
   double2* F1 = reinterpret_cast<double2*>(sm122 + tsz);
@@ -246,8 +244,6 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
   double2* F4 = F3 + n3 * n3;
   int2* pr = reinterpret_cast<int2*>(F4 + n4 * n4);
   int2* pc = pr + pa;
-  unsigned char* cr = reinterpret_cast<unsigned char*>(pc + pb);
-  unsigned char* cc = cr + nr;
   const int tid = threadIdx.x;
   const bool work = useA || useB;
 
@@ -256,22 +252,27 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
     for (int i = tid; i < n2 * n2; i += T122) F2[i] = __ldg(&F[da.fh + i]);
     for (int i = tid; i < n3 * n3; i += T122) F3[i] = __ldg(&F[nfent + db.fg + i]);
     for (int i = tid; i < n4 * n4; i += T122) F4[i] = __ldg(&F[nfent + db.fh + i]);
-    for (int i = tid; i < nr; i += T122) cr[i] = __ldg(&cinfo[da.cstart + i]);
-    for (int i = tid; i < nc; i += T122) cc[i] = __ldg(&cinfo[db.cstart + i]);
   }
   for (int i = tid; i < pa; i += T122) pr[i] = __ldg(&gpp[da.pstart + i]);
   for (int i = tid; i < pb; i += T122) pc[i] = __ldg(&gpp[db.pstart + i]);
   __syncthreads();
 
   if (work) {
+    // Cells that no stored element reaches -- the (t,t) cells of g = h and
+    // the parts known to be zero -- stay 0: zero the tile first.
+    for (int i = 2 * tid; i < tsz; i += 2 * T122) *reinterpret_cast<double2*>(T + i) = make_double2(0.0, 0.0);
+    __syncthreads();
     // gather: region (c1 rows of S_a, c2 columns of S_b); the stored element
-    // is (P1,P2) of part (c1,c2) when c1 >= c2, else (P2,P1) of part (c2,c1).
+    // is (P1,P2) of part (c1,c2) when c1 >= c2, else (P2,P1) of part (c2,c1),
+    // taken with herm.  It lands on its cell with the orientation sign of the
+    // two pairs, and on the mirror cells (g = h) with the opposite ones.
     // The loops stay rolled: the kernel's code must fit the instruction cache.
 #pragma unroll 1
     for (int x = 0; x < 2; ++x) {
       if (x == 0 ? !useA : !useB) continue;
       const double* src = x == 0 ? A : B;
       const unsigned zm = x == 0 ? zA : zB;
+      const double hx = x == 0 ? hA : hB;
       const int xo = TW == 2 ? x : 0;
 #pragma unroll 1
       for (int rg = 0; rg < 9; ++rg) {
@@ -281,8 +282,9 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
         const int part = lower ? slot_of(c1, c2) : slot_of(c2, c1);
         if (r1 == 0 || r2 == 0 || ((zm >> (P_HHHH + part)) & 1u)) continue;
         const int o1 = da.off(c1), o2 = db.off(c2);
-        const i64 base = __ldg(boff + part);
+        const double* srcp = src + __ldg(boff + part);
         const i64 ldv = lower ? cnt_of(c1, bd) : cnt_of(c2, bd);
+        const double hf = lower ? 1.0 : hx;
         const int total = r1 * r2;
         // e = fast + nf * slow, walked without dividing: the memory-contiguous
         // index (rows for stored parts, columns for transposed ones) is fast
@@ -290,6 +292,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
         const int2 i0 = divmod_small(tid, nf), di = divmod_small(T122, nf);
         int fa = i0.y, sl = i0.x;
         const int dfa = di.y, dsl = di.x;
+#pragma unroll 4
         for (int e = tid; e < total; e += T122) {
           const int p = lower ? fa : sl, u = lower ? sl : fa;
           fa += dfa;
@@ -299,45 +302,18 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
             ++sl;
           }
           const int2 P = pr[o1 + p], Q = pc[o2 + u];
-          const i64 addr = lower ? base + P.x + (i64)Q.x * ldv : base + Q.x + (i64)P.x * ldv;
-          const double* g = src + addr;
+          const i64 addr = lower ? P.x + (i64)Q.x * ldv : Q.x + (i64)P.x * ldv;
+          const double v = hf * __ldg(srcp + addr);
+          const double sv = ((P.y ^ Q.y) & (1 << 16)) ? -v : v;
           const int r = P.y & 0xFF, rm = ((P.y >> 8) & 0xFF) - 1;
           const int s = Q.y & 0xFF, sm = ((Q.y >> 8) & 0xFF) - 1;
-          cp_async8(&T[(r * ld + s) * TW + xo], g);
-          if (rm >= 0) cp_async8(&T[(rm * ld + s) * TW + xo], g);
+          T[(r * ld + s) * TW + xo] = sv;
+          if (rm >= 0) T[(rm * ld + s) * TW + xo] = -sv;
           if (sm >= 0) {
-            cp_async8(&T[(r * ld + sm) * TW + xo], g);
-            if (rm >= 0) cp_async8(&T[(rm * ld + sm) * TW + xo], g);
+            T[(r * ld + sm) * TW + xo] = -sv;
+            if (rm >= 0) T[(rm * ld + sm) * TW + xo] = sv;
           }
         }
-      }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    // orientation and herm signs in place; (t,t) cells and known-zero parts -> 0
-    const int2 i0 = divmod_small(tid, nc), di = divmod_small(T122, nc);
-    int fs = i0.y, fr = i0.x;
-    const int dfs = di.y, dfr = di.x;
-    for (int e = tid; e < nr * nc; e += T122) {
-      const int r = fr, s = fs;
-      fs += dfs;
-      fr += dfr;
-      if (fs >= nc) {
-        fs -= nc;
-        ++fr;
-      }
-      const int ci = cr[r], cj = cc[s];
-      const int c1 = (ci >> 1) & 3, c2 = (cj >> 1) & 3;
-      const bool valid = (ci & cj & 8) != 0;
-      const int part = c1 >= c2 ? slot_of(c1, c2) : slot_of(c2, c1);
-      const double sg = ((ci ^ cj) & 1) ? -1.0 : 1.0;
-#pragma unroll 1
-      for (int x = 0; x < 2; ++x) {
-        if (x == 0 ? !useA : !useB) continue;
-        const unsigned zm = x == 0 ? zA : zB;
-        const double f = c1 < c2 ? sg * (x == 0 ? hA : hB) : sg;
-        double* t = &T[(r * ld + s) * TW + (TW == 2 ? x : 0)];
-        *t = (valid && !((zm >> (P_HHHH + part)) & 1u)) ? f * *t : 0.0;
       }
     }
     __syncthreads();
@@ -415,13 +391,77 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
 //   1  (g', h)       (g, h')          (l1,k2; k1,l2)
 //   2  (h', h)       (g, g')          (l2,k2; k1,l1)
 //   3  (h', g)       (h, g')          (l2,k1; k2,l1)
-// STAGED: per term the CTA copies its sub-matrix into shared memory
-// (cp.async, coalesced runs) and every stored cell adds its element to a
-// shared accumulator; the last term adds the sum into C.  Tiles too large
-// for that read the four elements of each cell from global memory.
+// Modes (per launch bucket, by the tile's size):
+//   PD_ALL4   the four sub-matrices staged at once (one wait), one pass over
+//             the stored cells adds the four elements into C;
+//   PD_PAIRS  two buffers: terms 0,1 in flight, then term t+2 is copied
+//             while term t is added into a shared accumulator per cell;
+//   PD_SINGLE one buffer and the accumulator, the terms one after another;
+//   PD_DIRECT no staging: each cell reads its four elements from global
+//             memory (tiles too large for the others).
+// Every cell adds the four terms in the order 0, 1, 2, 3 in all modes.
 constexpr int TPD = 256;
+enum { PD_DIRECT = 0, PD_ALL4 = 1, PD_PAIRS = 2, PD_SINGLE = 3 };
 
-template <bool STAGED>
+struct PdTerm {  // geometry of one term's sub-matrix
+  const double* zb;  // element (0, 0)
+  i64 ldz;           // leading dimension of the cc block
+  int nrow, ncol, m2, m4;
+};
+
+__device__ __forceinline__ PdTerm pd_term(int t, const DevLayout& L, const int2* __restrict__ zrow, int ng,
+                                          const double* __restrict__ Z, int2 gb, int2 gk, int n1, int n2, int n3,
+                                          int n4) {
+  int G1, G2, G3, G4, m1, m3;
+  PdTerm d;
+  if (t == 0) {
+    G1 = gk.x; G2 = gb.x; G3 = gb.y; G4 = gk.y; m1 = n3; d.m2 = n1; m3 = n2; d.m4 = n4;
+  } else if (t == 1) {
+    G1 = gk.x; G2 = gb.y; G3 = gb.x; G4 = gk.y; m1 = n3; d.m2 = n2; m3 = n1; d.m4 = n4;
+  } else if (t == 2) {
+    G1 = gk.y; G2 = gb.y; G3 = gb.x; G4 = gk.x; m1 = n4; d.m2 = n2; m3 = n1; d.m4 = n3;
+  } else {
+    G1 = gk.y; G2 = gb.x; G3 = gb.y; G4 = gk.x; m1 = n4; d.m2 = n1; m3 = n2; d.m4 = n3;
+  }
+  const int2 zr = __ldg(&zrow[G1 * ng + G2]);
+  const int cs = __ldg(&zrow[G3 * ng + G4]).y;
+  d.ldz = __ldg(&L.ccdim[zr.x]).x;
+  d.zb = Z + __ldg(&L.cczoff[zr.x]) + zr.y + (i64)cs * d.ldz;
+  d.nrow = m1 * d.m2;
+  d.ncol = m3 * d.m4;
+  return d;
+}
+
+// (row, column) of the cell's element in term t's sub-matrix
+__device__ __forceinline__ int2 pd_rc(int t, const PdTerm& d, int k1, int k2, int l1, int l2) {
+  if (t == 0) return make_int2(l1 * d.m2 + k1, k2 * d.m4 + l2);
+  if (t == 1) return make_int2(l1 * d.m2 + k2, k1 * d.m4 + l2);
+  if (t == 2) return make_int2(l2 * d.m2 + k2, k1 * d.m4 + l1);
+  return make_int2(l2 * d.m2 + k1, k2 * d.m4 + l1);
+}
+// its position in the staged copy (column-major, nrow rows)
+__device__ __forceinline__ int pd_index(int t, const PdTerm& d, int k1, int k2, int l1, int l2) {
+  const int2 ij = pd_rc(t, d, k1, k2, l1, l2);
+  return ij.x + ij.y * d.nrow;
+}
+
+// copy term d's sub-matrix into dst (runs of nrow doubles, coalesced)
+__device__ __forceinline__ void pd_stage(const PdTerm& d, double* dst, int tid) {
+  const int total = d.nrow * d.ncol;
+  const int2 i0 = divmod_small(tid, d.nrow), di = divmod_small(TPD, d.nrow);
+  int fr = i0.y, fc = i0.x;
+  for (int e = tid; e < total; e += TPD) {
+    cp_async8(&dst[e], d.zb + fr + (i64)fc * d.ldz);
+    fr += di.y;
+    fc += di.x;
+    if (fr >= d.nrow) {
+      fr -= d.nrow;
+      ++fc;
+    }
+  }
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(TPD) k_pandya_tile(DevLayout L, const int* __restrict__ tasks,
                                                      const int2* __restrict__ tiles, const int4* __restrict__ gpd,
                                                      const int2* __restrict__ gpp, const int2* __restrict__ gpg,
@@ -432,6 +472,7 @@ __global__ void __launch_bounds__(TPD) k_pandya_tile(DevLayout L, const int* __r
   const GpDesc da = load_gp(gpd, tl.x), db = load_gp(gpd, tl.y);
   const int2 gb = __ldg(&gpg[tl.x]), gk = __ldg(&gpg[tl.y]);  // (g, h), (g', h')
   const int n1 = da.n1, n2 = da.n2, n3 = db.n1, n4 = db.n2;
+  const int cells = n1 * n2 * n3 * n4;
   const int pa = da.cnt(0) + da.cnt(1) + da.cnt(2), pb = db.cnt(0) + db.cnt(1) + db.cnt(2);
   const int q = da.q;
   const int4 bd = __ldg(&L.blk[q]);
@@ -440,53 +481,44 @@ __global__ void __launch_bounds__(TPD) k_pandya_tile(DevLayout L, const int* __r
 #pragma unroll 1
   for (int c1 = 0; c1 < 3; ++c1)
     for (int c2 = 0; c2 <= c1; ++c2) nst += da.cnt(c1) * db.cnt(c2);
-  const int zcap = STAGED ? n1 * n2 * n3 * n4 : 0;
+  // shared memory: sub-matrix buffers | accumulator | row, column pairs
+  constexpr int NBUF = MODE == PD_ALL4 ? 4 : (MODE == PD_PAIRS ? 2 : (MODE == PD_SINGLE ? 1 : 0));
+  constexpr bool ACCUM = MODE == PD_PAIRS || MODE == PD_SINGLE;
   double* Zs = smp;
-  double* Y = smp + zcap;
-  int2* pr = reinterpret_cast<int2*>(Y + (STAGED ? nst : 0));
+  double* Y = smp + NBUF * cells;
+  int2* pr = reinterpret_cast<int2*>(Y + (ACCUM ? nst : 0));
   int2* pc = pr + pa;
   const int tid = threadIdx.x;
   for (int i = tid; i < pa; i += TPD) pr[i] = __ldg(&gpp[da.pstart + i]);
   for (int i = tid; i < pb; i += TPD) pc[i] = __ldg(&gpp[db.pstart + i]);
+  PdTerm d[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) d[t] = pd_term(t, L, zrow, ng, Z, gb, gk, n1, n2, n3, n4);
+  if (MODE == PD_ALL4) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) pd_stage(d[t], Zs + t * cells, tid);
+    cp_async_wait_all();
+  } else if (MODE == PD_PAIRS) {
+    pd_stage(d[0], Zs, tid);
+    cp_async_commit();
+    pd_stage(d[1], Zs + cells, tid);
+    cp_async_commit();
+    cp_async_wait_group<1>();
+  } else if (MODE == PD_SINGLE) {
+    pd_stage(d[0], Zs, tid);
+    cp_async_wait_all();
+  }
   __syncthreads();
 
+  // passes over the stored cells: ALL4 and DIRECT one (all terms), PAIRS and
+  // SINGLE one per term
+  constexpr int NPASS = ACCUM ? 4 : 1;
 #pragma unroll 1
-  for (int term = 0; term < (STAGED ? 4 : 1); ++term) {
-    const double* zb = nullptr;
-    int nrow = 0, m2 = 0, m4 = 0;
-    i64 ldz = 0;
-    if (STAGED) {
-      int G1, G2, G3, G4, m1, m3;
-      if (term == 0) {
-        G1 = gk.x; G2 = gb.x; G3 = gb.y; G4 = gk.y; m1 = n3; m2 = n1; m3 = n2; m4 = n4;
-      } else if (term == 1) {
-        G1 = gk.x; G2 = gb.y; G3 = gb.x; G4 = gk.y; m1 = n3; m2 = n2; m3 = n1; m4 = n4;
-      } else if (term == 2) {
-        G1 = gk.y; G2 = gb.y; G3 = gb.x; G4 = gk.x; m1 = n4; m2 = n2; m3 = n1; m4 = n3;
-      } else {
-        G1 = gk.y; G2 = gb.x; G3 = gb.y; G4 = gk.x; m1 = n4; m2 = n1; m3 = n2; m4 = n3;
-      }
-      const int2 zr = __ldg(&zrow[G1 * ng + G2]);
-      const int cs = __ldg(&zrow[G3 * ng + G4]).y;
-      ldz = __ldg(&L.ccdim[zr.x]).x;
-      zb = Z + __ldg(&L.cczoff[zr.x]) + zr.y + (i64)cs * ldz;
-      nrow = m1 * m2;
-      const int total = nrow * m3 * m4;
-      const int2 i0 = divmod_small(tid, nrow), di = divmod_small(TPD, nrow);
-      int fr = i0.y, fc = i0.x;
-      const int dr = di.y, dc = di.x;
-      for (int e = tid; e < total; e += TPD) {
-        cp_async8(&Zs[e], zb + fr + (i64)fc * ldz);
-        fr += dr;
-        fc += dc;
-        if (fr >= nrow) {
-          fr -= nrow;
-          ++fc;
-        }
-      }
-      cp_async_wait_all();
-      __syncthreads();
-    }
+  for (int pass = 0; pass < NPASS; ++pass) {
+    const double* buf = Zs + (MODE == PD_PAIRS ? (pass & 1) * cells : 0);
+    // this pass's term geometry (recomputed: an array indexed by the pass
+    // would live in local memory)
+    const PdTerm dp = ACCUM ? pd_term(pass, L, zrow, ng, Z, gb, gk, n1, n2, n3, n4) : d[0];
     int j0 = 0;  // first accumulator slot of the region
 #pragma unroll 1
     for (int rg = 0; rg < 6; ++rg) {
@@ -498,62 +530,60 @@ __global__ void __launch_bounds__(TPD) k_pandya_tile(DevLayout L, const int* __r
       const i64 ldc = cnt_of(c1, bd);
       const int2 i0 = divmod_small(tid, r1), di = divmod_small(TPD, r1);
       int p = i0.y, u = i0.x;
-      const int dp = di.y, du = di.x;
       for (int e = tid; e < r1 * r2; e += TPD) {
         const int2 P = pr[o1 + p], Q = pc[o2 + u];
-        const int k1 = (P.y >> 17) & 15, k2 = (P.y >> 21) & 15;
-        const int l1 = (Q.y >> 17) & 15, l2 = (Q.y >> 21) & 15;
-        double y;
-        if (STAGED) {
-          int zi, zj;
-          if (term == 0) {
-            zi = l1 * m2 + k1; zj = k2 * m4 + l2;
-          } else if (term == 1) {
-            zi = l1 * m2 + k2; zj = k1 * m4 + l2;
-          } else if (term == 2) {
-            zi = l2 * m2 + k2; zj = k1 * m4 + l1;
-          } else {
-            zi = l2 * m2 + k1; zj = k2 * m4 + l1;
-          }
-          const double z = Zs[zi + zj * nrow];
-          y = (term == 0 ? 0.0 : Y[j0 + e]) + ((term & 1) ? -z : z);
-          if (term < 3) Y[j0 + e] = y;
-        } else {
-          // the four elements straight from global memory
-          double t4[4];
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            int G1, G2, G3, G4, a1, a2, a3, a4, s2, s4;
-            if (t == 0) {
-              G1 = gk.x; G2 = gb.x; G3 = gb.y; G4 = gk.y; a1 = l1; a2 = k1; a3 = k2; a4 = l2; s2 = n1; s4 = n4;
-            } else if (t == 1) {
-              G1 = gk.x; G2 = gb.y; G3 = gb.x; G4 = gk.y; a1 = l1; a2 = k2; a3 = k1; a4 = l2; s2 = n2; s4 = n4;
-            } else if (t == 2) {
-              G1 = gk.y; G2 = gb.y; G3 = gb.x; G4 = gk.x; a1 = l2; a2 = k2; a3 = k1; a4 = l1; s2 = n2; s4 = n3;
-            } else {
-              G1 = gk.y; G2 = gb.x; G3 = gb.y; G4 = gk.x; a1 = l2; a2 = k1; a3 = k2; a4 = l1; s2 = n1; s4 = n3;
-            }
-            const int2 zr = __ldg(&zrow[G1 * ng + G2]);
-            const int cs = __ldg(&zrow[G3 * ng + G4]).y;
-            const i64 r = __ldg(&L.ccdim[zr.x]).x;
-            t4[t] = __ldg(Z + __ldg(&L.cczoff[zr.x]) + zr.y + a1 * s2 + a2 + (cs + a3 * s4 + a4) * r);
-          }
-          y = t4[0] - t4[1] + t4[2] - t4[3];
-        }
-        p += dp;
-        u += du;
+        p += di.y;
+        u += di.x;
         if (p >= r1) {
           p -= r1;
           ++u;
         }
-        if (!STAGED || term == 3) {
+        const int k1 = (P.y >> 17) & 15, k2 = (P.y >> 21) & 15;
+        const int l1 = (Q.y >> 17) & 15, l2 = (Q.y >> 21) & 15;
+        double y;
+        bool last = true;
+        if (MODE == PD_ALL4) {
+          y = Zs[pd_index(0, d[0], k1, k2, l1, l2)];
+          y -= Zs[cells + pd_index(1, d[1], k1, k2, l1, l2)];
+          y += Zs[2 * cells + pd_index(2, d[2], k1, k2, l1, l2)];
+          y -= Zs[3 * cells + pd_index(3, d[3], k1, k2, l1, l2)];
+        } else if (MODE == PD_DIRECT) {
+          double z[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const int2 ij = pd_rc(t, d[t], k1, k2, l1, l2);
+            z[t] = __ldg(d[t].zb + ij.x + (i64)ij.y * d[t].ldz);
+          }
+          y = z[0] - z[1] + z[2] - z[3];
+        } else {
+          const double z = buf[pd_index(pass, dp, k1, k2, l1, l2)];
+          y = (pass == 0 ? 0.0 : Y[j0 + e]) + ((pass & 1) ? -z : z);
+          last = pass == 3;
+          if (!last) Y[j0 + e] = y;
+        }
+        if (last) {
           if ((P.y ^ Q.y) & (1 << 16)) y = -y;
           C[base + P.x + (i64)Q.x * ldc] += y;
         }
       }
       j0 += r1 * r2;
     }
-    if (STAGED) __syncthreads();  // the next term overwrites Zs
+    if (MODE == PD_PAIRS && pass < 3) {
+      __syncthreads();  // buffer (pass & 1) is free again
+      if (pass < 2) {   // term pass + 2 into it, while term pass + 1 lands
+        pd_stage(pd_term(pass + 2, L, zrow, ng, Z, gb, gk, n1, n2, n3, n4), Zs + (pass & 1) * cells, tid);
+        cp_async_commit();
+        cp_async_wait_group<1>();
+      } else {
+        cp_async_wait_group<0>();
+      }
+      __syncthreads();
+    } else if (MODE == PD_SINGLE && pass < 3) {
+      __syncthreads();
+      pd_stage(pd_term(pass + 1, L, zrow, ng, Z, gb, gk, n1, n2, n3, n4), Zs, tid);
+      cp_async_wait_all();
+      __syncthreads();
+    }
   }
 }
 
@@ -570,7 +600,7 @@ struct TileInfo {
 struct PdBucket {  // one launch of the particle-hole tile kernel
   int first, count;
   size_t smem;
-  bool staged;
+  int mode;  // PD_ALL4, PD_PAIRS, PD_SINGLE or PD_DIRECT
 };
 struct Bucket122 {
   int tw;       // doubles per staged cell
@@ -579,7 +609,7 @@ struct Bucket122 {
   size_t smem;
   int list = 0;          // 0 one operand (sets C), 1 both operands, 2 one operand (accumulates)
   int threads = 256;    // CTA size (autotuned)
-  float ms[2] = {0, 0};  // measured time of the 128- and 256-thread variants
+  float ms[3] = {0, 0, 0};  // measured time of the 64-, 128- and 256-thread variants
 };
 struct TaskSet {
   int2* d_task = nullptr;
@@ -593,7 +623,6 @@ struct TaskSet {
 struct Plan122 {
   int4* d_gpd = nullptr;
   int2* d_gpp = nullptr;
-  unsigned char* d_cinfo = nullptr;
   int2* d_tiles = nullptr;
   int* d_sbase = nullptr;
   double2* d_ftab = nullptr;
@@ -619,7 +648,7 @@ std::mutex g_plan_mutex;
 size_t tile_smem(const TileInfo& t, int tw) {
   const size_t ld = (size_t)(t.nc | 1);
   const size_t tsz = ((size_t)t.nr * ld * tw + 1) & ~(size_t)1;
-  return 8 * tsz + 16 * (size_t)t.nf + 8 * (size_t)t.npair + (size_t)t.nr + (size_t)t.nc;
+  return 8 * tsz + 16 * (size_t)t.nf + 8 * (size_t)t.npair;
 }
 
 template <class T>
@@ -667,7 +696,6 @@ static int plan_122(qd_layout* L, Plan122** out) {
 
   std::vector<int4> gpd;
   std::vector<int2> gpp, gpg;
-  std::vector<unsigned char> cinfo;
   struct GpHost {
     int n1, n2, cnt[3], nf, npair;
   };
@@ -678,7 +706,6 @@ static int plan_122(qd_layout* L, Plan122** out) {
     std::map<std::pair<int, int>, int> idx;
     std::vector<std::pair<int, int>> order;
     std::vector<std::vector<int2>> plist;  // {w, packed cells}
-    std::vector<std::vector<unsigned char>> cl;
     std::vector<GpHost> gh;
     for (int P = 0; P < ntot; ++P) {
       const int2 pr = L->pairs[pb + P];  // 0-based states, pr.x < pr.y
@@ -690,7 +717,6 @@ static int plan_122(qd_layout* L, Plan122** out) {
       if (ins.second) {
         order.push_back({g, h});
         plist.emplace_back();
-        cl.emplace_back((size_t)gsz[g] * gsz[h], (unsigned char)0);
         gh.push_back(GpHost{gsz[g], gsz[h], {0, 0, 0}, 0, 0});
       }
       const int u = ins.first->second;
@@ -711,8 +737,6 @@ static int plan_122(qd_layout* L, Plan122** out) {
         return QD_ERR_ARG;
       }
       plist[u].push_back(int2{w, r | ((rm + 1) << 8) | (neg << 16) | (kpos[t1] << 17) | (kpos[t2] << 21)});
-      cl[u][r] = (unsigned char)(8 | (c << 1) | neg);
-      if (rm >= 0) cl[u][rm] = (unsigned char)(8 | (c << 1) | (1 - neg));
       gh[u].cnt[c] += 1;
     }
     const int u0 = (int)gpd.size() / 2;
@@ -726,10 +750,9 @@ static int plan_122(qd_layout* L, Plan122** out) {
       d.nf = d.n1 * d.n1 + d.n2 * d.n2;
       d.npair = d.cnt[0] + d.cnt[1] + d.cnt[2];
       gpd.push_back(int4{q, d.n1 | (d.n2 << 8) | ((g == h ? 1 : 0) << 16), holes[g] | (holes[h] << 8), goff[g]});
-      gpd.push_back(int4{goff[h], (int)gpp.size(), (int)cinfo.size(), d.cnt[0] | (d.cnt[1] << 10) | (d.cnt[2] << 20)});
+      gpd.push_back(int4{goff[h], (int)gpp.size(), 0, d.cnt[0] | (d.cnt[1] << 10) | (d.cnt[2] << 20)});
       gpg.push_back(int2{g, h});
       gpp.insert(gpp.end(), plist[u].begin(), plist[u].end());
-      cinfo.insert(cinfo.end(), cl[u].begin(), cl[u].end());
     }
     // tiles: every ordered pair of group pairs with at least one stored
     // output cell (a row class >= a column class)
@@ -769,7 +792,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
   for (size_t i = 0; i < p.tiles.size(); ++i) th[i] = int2{p.tiles[i].a, p.tiles[i].b};
   int rc;
   if ((rc = upload_vec(L, gpd, &p.d_gpd)) || (rc = upload_vec(L, gpp, &p.d_gpp)) ||
-      (rc = upload_vec(L, cinfo, &p.d_cinfo)) || (rc = upload_vec(L, th, &p.d_tiles)) ||
+      (rc = upload_vec(L, th, &p.d_tiles)) ||
       (rc = upload_vec(L, sbase, &p.d_sbase)))
     return rc;
   // particle-hole channel: first cc row of each (G1, G2) and the launches
@@ -779,38 +802,45 @@ static int plan_122(qd_layout* L, Plan122** out) {
     for (int g2 = 0; g2 < ngroup; ++g2)
       zrow[(size_t)g1 * ngroup + g2] = L->ccmap[(size_t)L->gmem[L->gstart[g1]] * m + L->gmem[L->gstart[g2]]];
   {
-    std::vector<std::pair<size_t, int>> lst;  // (shared memory, tile), staged tiles
-    std::vector<int> direct;
+    // per tile the first mode that fits: all four terms staged, two buffers
+    // (each while at least three CTAs fit an SM), one buffer, none; buckets
+    // by mode, then by size interval, largest first
+    struct PdT {
+      int mode;
+      size_t sm;
+      int tile;
+    };
+    std::vector<PdT> lst;
     for (size_t i = 0; i < p.tiles.size(); ++i) {
       const TileInfo& t = p.tiles[i];
-      const size_t sm = 8 * ((size_t)t.cells + t.nst + t.npair);
-      if (sm <= SMEM_MAX_122)
-        lst.push_back({sm, (int)i});
+      const size_t c = (size_t)t.cells, ns = (size_t)t.nst, np = (size_t)t.npair;
+      const size_t s4 = 8 * (4 * c + np), s2 = 8 * (2 * c + ns + np), s1 = 8 * (c + ns + np);
+      const size_t third = SMEM_MAX_122 / 3;
+      if (s4 <= third)
+        lst.push_back({PD_ALL4, s4, (int)i});
+      else if (s2 <= third)
+        lst.push_back({PD_PAIRS, s2, (int)i});
+      else if (s1 <= SMEM_MAX_122)
+        lst.push_back({PD_SINGLE, s1, (int)i});
       else
-        direct.push_back((int)i);
+        lst.push_back({PD_DIRECT, 8 * np, (int)i});
     }
-    std::stable_sort(lst.begin(), lst.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-    std::vector<int> tasks;
     const size_t bounds[4] = {24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122};
     auto interval = [&](size_t sm) {
       int l = 0;
       while (l < 3 && sm > bounds[l]) ++l;
       return l;
     };
+    std::stable_sort(lst.begin(), lst.end(), [&](const PdT& x, const PdT& y) {
+      return x.mode != y.mode ? x.mode < y.mode : x.sm > y.sm;
+    });
+    std::vector<int> tasks;
     size_t i = 0;
-    while (i < lst.size()) {  // buckets: tiles of one size interval, largest first
-      const int l = interval(lst[i].first);
-      PdBucket b{(int)tasks.size(), 0, lst[i].first, true};
-      while (i < lst.size() && interval(lst[i].first) == l) tasks.push_back(lst[i++].second);
+    while (i < lst.size()) {
+      const int mode = lst[i].mode, l = interval(lst[i].sm);
+      PdBucket b{(int)tasks.size(), 0, lst[i].sm, mode};
+      while (i < lst.size() && lst[i].mode == mode && interval(lst[i].sm) == l) tasks.push_back(lst[i++].tile);
       b.count = (int)tasks.size() - b.first;
-      p.pbuckets.push_back(b);
-    }
-    if (!direct.empty()) {
-      PdBucket b{(int)tasks.size(), (int)direct.size(), 0, false};
-      for (int t : direct) {
-        tasks.push_back(t);
-        b.smem = std::max(b.smem, 8 * (size_t)p.tiles[t].npair);
-      }
       p.pbuckets.push_back(b);
     }
     int rc2;
@@ -820,10 +850,12 @@ static int plan_122(qd_layout* L, Plan122** out) {
   }
   QD_CUDA(cudaMalloc(&p.d_ftab, sizeof(double2) * 2 * (size_t)std::max(1, p.nfent)));
   L->ws_bytes += (i64)sizeof(double2) * 2 * p.nfent;
-  for (const void* fn : {(const void*)k_122_tile<1, 128, false>, (const void*)k_122_tile<2, 128, false>,
+  for (const void* fn : {(const void*)k_122_tile<1, 64, false>, (const void*)k_122_tile<2, 64, false>,
+                         (const void*)k_122_tile<1, 128, false>, (const void*)k_122_tile<2, 128, false>,
                          (const void*)k_122_tile<1, 256, false>, (const void*)k_122_tile<2, 256, false>,
                          (const void*)k_122_tile<1, 256, true>, (const void*)k_122_tile<2, 256, true>,
-                         (const void*)k_pandya_tile<true>, (const void*)k_pandya_tile<false>}) {
+                         (const void*)k_pandya_tile<PD_ALL4>, (const void*)k_pandya_tile<PD_PAIRS>,
+                         (const void*)k_pandya_tile<PD_SINGLE>, (const void*)k_pandya_tile<PD_DIRECT>}) {
     cudaFuncAttributes fa;
     QD_CUDA(cudaFuncGetAttributes(&fa, fn));
     QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -841,10 +873,12 @@ static int plan_122(qd_layout* L, Plan122** out) {
 // Bucketings the autotuner chooses from: the size bounds (bytes of shared
 // memory) that split each list into launches.  More buckets give small tiles
 // more CTAs per SM; fewer keep the tiles of one column strip in one launch.
-constexpr int kNumBounds = 3;
-const size_t kBounds[kNumBounds][4] = {{24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122},
-                                       {56 * 1024, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122},
-                                       {SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122}};
+constexpr int kNumBounds = 4, kBoundsLen = 6;
+const size_t kBounds[kNumBounds][kBoundsLen] = {
+    {24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122},
+    {56 * 1024, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122},
+    {SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122, SMEM_MAX_122},
+    {8 * 1024, 16 * 1024, 24 * 1024, 56 * 1024, 112 * 1024, SMEM_MAX_122}};
 
 // One bucketing of the task lists: buckets by size bound (largest first),
 // and within a bucket the tiles sharing a column strip (block q, column
@@ -864,7 +898,7 @@ static int build_variant(qd_layout* L, const Plan122* p, std::vector<std::pair<s
       // bucket: tasks down to the next size bound below the first one
       const size_t top = v[i].first;
       size_t lower = 0;
-      for (int k = 0; k < 4; ++k)
+      for (int k = 0; k < kBoundsLen; ++k)
         if (bounds[k] < top) lower = std::max(lower, bounds[k]);
       Bucket122 b;
       b.tw = l == 1 ? 2 : 1;
@@ -931,7 +965,7 @@ void drop_122_plan(const qd_layout* L) {
   auto it = plans().find(L);
   if (it == plans().end()) return;
   Plan122& p = it->second;
-  for (void* ptr : {(void*)p.d_gpd, (void*)p.d_gpp, (void*)p.d_cinfo, (void*)p.d_tiles, (void*)p.d_sbase,
+  for (void* ptr : {(void*)p.d_gpd, (void*)p.d_gpp, (void*)p.d_tiles, (void*)p.d_sbase,
                     (void*)p.d_ftab, (void*)p.d_gpg, (void*)p.d_zrow, (void*)p.d_ptask})
     if (ptr) cudaFree(ptr);
   for (auto& kv : p.sets) {
@@ -973,13 +1007,13 @@ static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, cons
   const unsigned legB = leg_masks(spA, B->zero_mask), legA = leg_masks(spB, A->zero_mask);
 #define QD_122_LAUNCH(TW, NT)                                                                                   \
   k_122_tile<TW, NT, false><<<b.count, NT, b.smem, L->stream>>>(L->dev, ts->d_task + b.first, p->d_tiles, p->d_gpd,   \
-                                                         p->d_gpp, p->d_cinfo, p->d_ftab, p->nfent, A->d,       \
+                                                         p->d_gpp, p->d_ftab, p->nfent, A->d,                   \
                                                          (double)A->herm, A->zero_mask, legA, B->d,             \
                                                          (double)B->herm, B->zero_mask, legB, C, nullptr, nullptr)
   if (b.tw == 2) {
-    if (threads == 128) QD_122_LAUNCH(2, 128); else QD_122_LAUNCH(2, 256);
+    if (threads == 64) QD_122_LAUNCH(2, 64); else if (threads == 128) QD_122_LAUNCH(2, 128); else QD_122_LAUNCH(2, 256);
   } else {
-    if (threads == 128) QD_122_LAUNCH(1, 128); else QD_122_LAUNCH(1, 256);
+    if (threads == 64) QD_122_LAUNCH(1, 64); else if (threads == 128) QD_122_LAUNCH(1, 128); else QD_122_LAUNCH(1, 256);
   }
 #undef QD_122_LAUNCH
   ++L->nlaunch;
@@ -987,17 +1021,17 @@ static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, cons
   return QD_OK;
 }
 
-// Autotuner: the first launch of a task set times every bucket with 128- and
-// 256-thread CTAs (CUDA events, best of two runs each) on the real operands,
-// writing into a scratch operator of the layout, and keeps the faster size
+// Autotuner: the first launch of a task set times every bucket with 64-, 128-
+// and 256-thread CTAs (CUDA events, best of two runs each) on the real operands,
+// writing into a scratch operator of the layout, and keeps the fastest size
 // per bucket.  Every output cell is summed by one thread in a fixed order
 // whatever the CTA size, so the choice never changes a result.
 static int tune_variant(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, const qd_op* B, int spA, int spB,
                         double* scratch, cudaEvent_t e0, cudaEvent_t e1) {
   ts->ms_total = 0.f;
   for (Bucket122& b : ts->buckets) {
-    for (int v = 0; v < 2; ++v) {
-      const int threads = v ? 256 : 128;
+    for (int v = 0; v < 3; ++v) {
+      const int threads = 64 << v;
       float best = 1e30f;
       for (int rep = 0; rep < 2; ++rep) {
         QD_CUDA(cudaEventRecord(e0, L->stream));
@@ -1010,14 +1044,17 @@ static int tune_variant(qd_layout* L, Plan122* p, TaskSet* ts, const qd_op* A, c
       }
       b.ms[v] = best;
     }
-    b.threads = b.ms[0] < b.ms[1] ? 128 : 256;
-    ts->ms_total += std::min(b.ms[0], b.ms[1]);
+    int v = 0;
+    for (int k = 1; k < 3; ++k)
+      if (b.ms[k] < b.ms[v]) v = k;
+    b.threads = 64 << v;
+    ts->ms_total += b.ms[v];
   }
   return QD_OK;
 }
 
 // Autotuner: the first launch of a task set times, for every bucketing
-// (kBounds), every bucket with 128- and 256-thread CTAs (CUDA events, best of
+// (kBounds), every bucket with 64-, 128- and 256-thread CTAs (CUDA events, best of
 // two runs each) on the real operands, writing into a scratch operator of
 // the layout; it keeps the CTA size per bucket and the bucketing with the
 // least total time.  Every output cell is summed by one thread in a fixed
@@ -1086,8 +1123,9 @@ std::string tuning_report_122(const qd_layout* L) {
     }
     out += "\n";
     for (const Bucket122& b : kv.second.buckets) {
-      snprintf(line, sizeof(line), "  tiles %6d staged %d smem %6zu B: 128 thr %.4f ms, 256 thr %.4f ms -> %d\n",
-               b.count, b.tw, b.smem, b.ms[0], b.ms[1], b.threads);
+      snprintf(line, sizeof(line),
+               "  tiles %6d staged %d smem %6zu B: 64 thr %.4f ms, 128 thr %.4f ms, 256 thr %.4f ms -> %d\n",
+               b.count, b.tw, b.smem, b.ms[0], b.ms[1], b.ms[2], b.threads);
       out += line;
     }
   }
@@ -1153,12 +1191,16 @@ int launch_pandya_tiles(qd_layout* L, const double* Z, double* C) {
   if (rc) return rc;
   for (const PdBucket& b : p->pbuckets) {
     if (b.count == 0) continue;
-    if (b.staged)
-      k_pandya_tile<true><<<b.count, TPD, b.smem, L->stream>>>(L->dev, p->d_ptask + b.first, p->d_tiles, p->d_gpd,
-                                                               p->d_gpp, p->d_gpg, p->d_zrow, p->ng, Z, C);
-    else
-      k_pandya_tile<false><<<b.count, TPD, b.smem, L->stream>>>(L->dev, p->d_ptask + b.first, p->d_tiles, p->d_gpd,
-                                                                p->d_gpp, p->d_gpg, p->d_zrow, p->ng, Z, C);
+#define QD_PD_LAUNCH(M)                                                                                       \
+  k_pandya_tile<M><<<b.count, TPD, b.smem, L->stream>>>(L->dev, p->d_ptask + b.first, p->d_tiles, p->d_gpd, \
+                                                        p->d_gpp, p->d_gpg, p->d_zrow, p->ng, Z, C)
+    switch (b.mode) {
+      case PD_ALL4: QD_PD_LAUNCH(PD_ALL4); break;
+      case PD_PAIRS: QD_PD_LAUNCH(PD_PAIRS); break;
+      case PD_SINGLE: QD_PD_LAUNCH(PD_SINGLE); break;
+      default: QD_PD_LAUNCH(PD_DIRECT); break;
+    }
+#undef QD_PD_LAUNCH
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());
@@ -1283,7 +1325,6 @@ int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
     I.tiles = p->d_tiles;
     I.gpd = p->d_gpd;
     I.gpp = p->d_gpp;
-    I.cinfo = p->d_cinfo;
     I.F = p->d_ftab;
     I.nfent = p->nfent;
     I.A = it.A->d;
@@ -1300,12 +1341,12 @@ int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
   const DevLayout& L0 = items[0].L->dev;
   for (const Bucket122& b : m->buckets) {
     if (b.tw == 2)
-      k_122_tile<2, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
-                                                       nullptr, 0, nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
+      k_122_tile<2, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr, 0,
+                                                       nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
                                                        m->d_tinst + b.first, m->d_inst);
     else
-      k_122_tile<1, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr,
-                                                       nullptr, 0, nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
+      k_122_tile<1, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr, 0,
+                                                       nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
                                                        m->d_tinst + b.first, m->d_inst);
     ++items[0].L->nlaunch;
   }
