@@ -207,8 +207,27 @@ int qd_dgam(const qd_op* H, qd_op* DER, qd_cc* HCC, qd_cc* ETACC);
  * and pphh parts of ([H, Q+] + [H, Q-]) / 2 with Q+- the amplitudes as
  * herm +-1 operators (particle-hole channel on).  The Lanczos driver
  * (ARPACK dsaupd) stays on the host, as in the reference; its vector maps to
- * Q through the host's unwrap/rewrap.  Non-scalar targets are not covered. */
+ * Q through the host's unwrap/rewrap.  Any target, non-scalar ones included:
+ * qd_eom_matvec_target.                                                     */
 int qd_eom_matvec(const qd_op* H, const qd_op* Q, qd_op* HQ);
+/* EOM vector dimension for the target (ml, ms) (Mltarg, Mstarg of the
+ * reference, src/EOM_IMSRG.f90:21-22: Ml = m_l(a) - m_l(i), Ms = s(a) - s(i)
+ * with s = +-1): *n1 1p1h and *n2 2p2h entries, counted as unwrap
+ * (src/EOM_IMSRG.f90:815-884) counts them.  Host only; works on QD_HOST_ONLY
+ * layouts.                                                                  */
+int qd_eom_dim(const qd_layout* L, int ml, int ms, int64_t* n1, int64_t* n2);
+/* matvec_prod (src/EOM_IMSRG.f90:551-649) for any target (ml, ms): d_w = the
+ * rewrap of HQ_comm_1b / HQ_comm_2b (src/commutators.f90:1162-1272) of H and
+ * the excitation operator unwrapped from d_v.  d_v and d_w are device arrays
+ * of n = n1 + n2 doubles in the reference's unwrap order (1p1h entries,
+ * particle outer and hole inner, then 2p2h entries, a < b outer and i < j
+ * inner); the ARPACK loop (dsaupd reverse communication,
+ * src/EOM_IMSRG.f90:243-255) stays on the host and copies its work vectors
+ * to and from them.  Asynchronous on the layout's stream.  The first call
+ * for a target builds its tables (and synchronises); they are kept until
+ * the layout is destroyed.  Returns QD_ERR_ARG when n does not match the
+ * target's dimension.                                                       */
+int qd_eom_matvec_target(const qd_op* H, int ml, int ms, const double* d_v, double* d_w, int64_t n);
 
 /* ---- cross-coupled (Pandya) matrices ----------------------------------------
  * calc_cc src/commutators.f90:1135-1159, copy_cc src/IMSRG_tools.f90:437-461 */

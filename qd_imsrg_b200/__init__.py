@@ -33,7 +33,7 @@ __all__ = [
     "commutator_122", "commutator_222", "commutator", "calc_cc", "build_white", "add_arrays",
     "copy_arrays", "set_to_zero", "mat_2_norm", "mbpt2", "hf_e2", "bch_expand", "magnus_expand",
     "euler_step", "magnus_flow", "random_operator", "tbme_write", "hf_hamiltonian", "v_int",
-    "Flow", "magnus_flow_batch", "dgam", "eom_matvec", "gemm_split", "hamiltonian_write", "hamiltonian_read",
+    "Flow", "magnus_flow_batch", "dgam", "eom_matvec", "eom_dim", "eom_matvec_target", "gemm_split", "hamiltonian_write", "hamiltonian_read",
     "export_hamiltonian", "import_hamiltonian",
 ]
 
@@ -292,6 +292,37 @@ def eom_matvec(H: FullHam, Q: FullHam, HQ: FullHam) -> None:
     scalar target: HQ's fph and Vpphh = the ph and pphh parts of [H, Q] for
     the excitation amplitudes in Q's fph and Vpphh; other parts zero."""
     check(lib().qd_eom_matvec(H.h, Q.h, HQ.h))
+
+
+def eom_dim(layout: Layout, ml: int, ms: int) -> tuple[int, int]:
+    """(1p1h, 2p2h) entries of the EOM vector for the target (Mltarg, Mstarg)
+    = (ml, ms), as unwrap (EOM_IMSRG.f90:815-884) counts them."""
+    n1, n2 = C.c_int64(), C.c_int64()
+    check(lib().qd_eom_dim(layout.h, int(ml), int(ms), C.byref(n1), C.byref(n2)))
+    return n1.value, n2.value
+
+
+def eom_matvec_target(H: FullHam, ml: int, ms: int, v, w=None):
+    """matvec_prod (EOM_IMSRG.f90:551-649) for the target (ml, ms): w = the
+    rewrap of HQ_comm_1b/2b of H and the excitation unwrapped from v, both in
+    the reference's unwrap order.  v, w: float64 CUDA tensors (torch) of
+    n1 + n2 entries on H's device (w is allocated when None); or a numpy v,
+    in which case a numpy w is returned (copied through the device)."""
+    import torch
+
+    host = isinstance(v, np.ndarray)
+    if host:
+        v = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).cuda()
+    if v.dtype != torch.float64 or not v.is_cuda or not v.is_contiguous() or v.dim() != 1:
+        raise ValueError("v must be a contiguous 1-D float64 CUDA tensor")
+    if w is None:
+        w = torch.empty_like(v)
+    # v and w are written on torch's stream, read and written on the layout's
+    torch.cuda.current_stream(v.device).synchronize()
+    check(lib().qd_eom_matvec_target(H.h, int(ml), int(ms), C.c_void_p(v.data_ptr()), C.c_void_p(w.data_ptr()),
+                                     int(v.numel())))
+    H.layout.synchronize()
+    return w.cpu().numpy() if host else w
 
 
 def calc_cc(H: FullHam, HCC: CCMat) -> None:

@@ -125,6 +125,8 @@ SIGNATURES = {
     "qd_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i64, C.c_float, C.POINTER(C.c_float), _vp]),
     "qd_dgam": (C.c_int, [_vp, _vp, _vp, _vp]),
     "qd_eom_matvec": (C.c_int, [_vp, _vp, _vp]),
+    "qd_eom_dim": (C.c_int, [_vp, C.c_int, C.c_int, _ip64, _ip64]),
+    "qd_eom_matvec_target": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _i64]),
     "qd_hamiltonian_write": (C.c_int, [_vp, _vp, C.c_char_p]),
     "qd_hamiltonian_read": (C.c_int, [_vp, _vp, C.c_char_p]),
     "qd_export_hamiltonian": (C.c_int, [_vp, C.c_char_p]),

@@ -85,6 +85,7 @@ void layout_finish(qd_layout* L) {
   drop_merged_gemm(L);
   drop_merged_122(L);
   drop_122_plan(L);
+  drop_eom_plans(L);
   layout_free_device(L);
   delete L;
 }

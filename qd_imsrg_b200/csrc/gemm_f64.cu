@@ -735,6 +735,33 @@ int build_programs(qd_layout* L) {
   return QD_OK;
 }
 
+// Ladder sums of the EOM product for a non-scalar target (eom.cu): per bra
+// block q with ket block partner[q] (pairs of M_q minus the target), the
+// npp(q) x nhh(partner[q]) output Wb[q] = Vpppp[q] Qb[q] + Qb[q] Vhhhh[partner[q]]
+// (the c<d and k<l sums of HQ_comm_2b, src/commutators.f90:1246-1258).
+// Buffers: H = BA, the amplitude matrices Qb = BB, the output Wb = BO0.
+int build_eom_ladders(qd_layout* L, const std::vector<int>& partner, const std::vector<i64>& qoff, GemmProgram& P) {
+  Builder b(P);
+  for (int q = 0; q < L->nblock; ++q) {
+    const int q2 = partner[q];
+    if (q2 < 0) continue;
+    const int np = L->blk[q].z, nh2 = L->blk[q2].x;
+    if (np == 0 || nh2 == 0) continue;
+    b.prob(np, nh2, qoff[q], np, GM_SET, BO0);
+    b.seg(BA, L->boff[6 * q + 1], np, N_, P_PPPP, BB, qoff[q], np, N_, -1, np, 1.0);
+    b.seg(BB, qoff[q], np, N_, -1, BA, L->boff[6 * q2 + 0], nh2, N_, P_HHHH, nh2, 1.0);
+  }
+  size_t pb = std::max<size_t>(1, P.probs.size()) * sizeof(GProb);
+  size_t sb = std::max<size_t>(1, P.segs.size()) * sizeof(GSeg);
+  QD_CUDA(cudaMalloc(&P.d_probs, pb));
+  QD_CUDA(cudaMalloc(&P.d_segs, sb));
+  if (!P.probs.empty())
+    QD_CUDA(cudaMemcpy(P.d_probs, P.probs.data(), P.probs.size() * sizeof(GProb), cudaMemcpyHostToDevice));
+  if (!P.segs.empty())
+    QD_CUDA(cudaMemcpy(P.d_segs, P.segs.data(), P.segs.size() * sizeof(GSeg), cudaMemcpyHostToDevice));
+  return QD_OK;
+}
+
 static bool seg_active_host(const GSeg& s, unsigned mA, unsigned mB) {
   auto dead = [&](int src, int dep) {
     if (dep < 0) return false;
@@ -828,6 +855,15 @@ int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double 
   int rc = build_programs(L);
   if (rc) return rc;
   if (L->split_slices > 0) return run_program_split(L, P, bufs, hv0, hv1, maskA, maskB);
+  return run_program_f64(L, P, bufs, hv0, hv1, maskA, maskB);
+}
+
+// P in FP64 on the DMMA pipe whatever the layout's form (P's tables must be
+// on the device: build_programs or build_eom_ladders).
+int run_program_f64(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
+                    unsigned maskB) {
+  int rc = build_programs(L);  // sets the kernels' shared-memory limits
+  if (rc) return rc;
   GTask *d_tasks = nullptr, *d_short = nullptr;
   int nt = 0, ns = 0;
   if ((rc = get_tasks(L, P, maskA, maskB, &d_tasks, &nt, &d_short, &ns))) return rc;

@@ -269,6 +269,10 @@ int launch_pandya_tiles(qd_layout* L, const double* Z, double* C);
 int prepare_pandya(qd_layout* L);
 int run_program(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
                 unsigned maskB);
+int run_program_f64(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
+                    unsigned maskB);
+int build_eom_ladders(qd_layout* L, const std::vector<int>& partner, const std::vector<i64>& qoff, GemmProgram& P);
+void drop_eom_plans(const qd_layout* L);
 void fill_random(const qd_layout* L, int herm, uint64_t seed, double sigma, int conserve, double* out);
 int run_program_split(qd_layout* L, GemmProgram& P, const double* const* bufs, double hv0, double hv1, unsigned maskA,
                       unsigned maskB);

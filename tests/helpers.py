@@ -107,3 +107,32 @@ def synth_hamiltonian(L, rng, gap=2.0, vs=0.05, fs=0.05):
     v[o:o + mp * n] *= fs / vs
     v[0] = 0.0
     return v
+
+
+
+def eom_scalar_positions(O):
+    """Positions in the vectorize array of the scalar-target EOM vector's
+    entries, in the reference's unwrap order (EOM_IMSRG.f90:815-884): the
+    1p1h entries in fph, then the 2p2h entries in each block's Vpphh.
+    O: an oracle.Layout (the library's layout has the same blocks)."""
+    n, m = O.n, O.m
+    mp = m - n
+    qn = O.qn
+    pp, hh = {}, {}
+    for q in range(O.nblock):
+        for k, (a, b) in enumerate(O.pairs(q + 1, 2)):
+            pp[(int(a), int(b))] = (q, k)
+        for k, (i, j) in enumerate(O.pairs(q + 1, 0)):
+            hh[(int(i), int(j))] = (q, k)
+    o_fph = 1 + n * n + mp * mp
+    pos = [o_fph + (a - n - 1) + (i - 1) * mp for a in range(n + 1, m + 1) for i in range(1, n + 1)
+           if tuple(qn[a - 1][1:]) == tuple(qn[i - 1][1:])]
+    for a in range(n + 1, m + 1):
+        for b in range(a + 1, m + 1):
+            qa = pp[(a, b)]
+            for i in range(1, n + 1):
+                for j in range(i + 1, n + 1):
+                    qh = hh[(i, j)]
+                    if qa[0] == qh[0]:
+                        pos.append(int(O.offs[qa[0], 2]) + qa[1] + qh[1] * int(O.dims[qa[0], 2]))
+    return np.array(pos, np.int64)

@@ -67,3 +67,38 @@ def test_matvec_is_commutator_average(n, R):
     assert got1.size > 0 and got2.size > 0
     assert np.linalg.norm(got1 - want1) <= 1e-12 * np.linalg.norm(want1)
     assert np.linalg.norm(got2 - want2) <= 1e-12 * np.linalg.norm(want2)
+
+
+@pytest.mark.parametrize("n,R", [(2, 3), (6, 4)])
+def test_dense_ladder_storage_matches_blocked_at_the_scalar_target(n, R):
+    """matvec_prod with the reference's dense storage of the ladder operator
+    (unwrap, Q_elem over fermionic_tp_index) equals the blocked restatement at
+    (Mltarg, Mstarg) = (0, 0): the unwrap order and the signs agree."""
+    from helpers import eom_scalar_positions
+    from oracle.eom import _targets, eom_dim, matvec_prod
+
+    O = oracle.Layout(n, R)
+    rng = np.random.default_rng(5 + n + R)
+    h = numpy_random_op(O, 1, rng)
+    H = oracle.Op(O, 1, h)
+    n1, n2 = eom_dim(O, 0, 0)
+    v = rng.standard_normal(n1 + n2)
+    w = matvec_prod(O, H, h, 1, 0, 0, v)
+    q = np.zeros(O.neq)
+    q[eom_scalar_positions(O)] = v
+    ref = HQ(O, H, h, 1, oracle.Op(O, 1, q), q)
+    one, two = _targets(O, 0, 0)
+    want = [ref.comm_1b(ix + n, jx) for ix, jx in one] + [ref.comm_2b(a + n, b + n, i, j) for a, b, i, j in two]
+    assert np.array_equal(np.array(want), w)
+
+
+@pytest.mark.parametrize("n,R", [(6, 5), (12, 6)])
+def test_eom_dim_counts_as_unwrap(n, R):
+    import qd_imsrg_b200 as qd
+    from oracle.eom import eom_dim
+
+    O = oracle.Layout(n, R)
+    L = qd.Layout(n, R, device=qd.HOST_ONLY)
+    for t in [(0, 0), (1, 0), (-1, 2), (2, -2), (3, 0), (-4, 0), (0, 2)]:
+        assert qd.eom_dim(L, *t) == eom_dim(O, *t)
+    L.close()
