@@ -758,6 +758,10 @@ def run_warmstart(args, world, rank, local):
             evals.append({"hw": hw, "why": str(e)})
             continue
         try:
+            # one untimed flow first: the layout's first flow builds its plans,
+            # tunes commutator_122 and captures the BCH step graphs, which the
+            # timed cold and warm flows then both find ready
+            ws.cold_flow(inst)
             cold = ws.cold_flow(inst)
             warms = [ws.warm_flow(mlp, inst, st) for st in s_targets]
             evals.append({"hw": hw, "E_HF": inst.E_HF, "cold": cold, "warm": warms[0], "sweep": warms[1:],
