@@ -242,10 +242,11 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
   double2* F2 = F1 + n1 * n1;
   double2* F3 = F2 + n2 * n2;
   double2* F4 = F3 + n3 * n3;
-  int2* pr = reinterpret_cast<int2*>(F4 + n4 * n4);
-  int2* pc = pr + pa;
   const int tid = threadIdx.x;
   const bool work = useA || useB;
+  // a task that writes zeros stages nothing: its shared memory holds the pair lists alone
+  int2* pr = work ? reinterpret_cast<int2*>(F4 + n4 * n4) : reinterpret_cast<int2*>(sm122);
+  int2* pc = pr + pa;
 
   if (work) {
     for (int i = tid; i < n1 * n1; i += T122) F1[i] = __ldg(&F[da.fg + i]);
@@ -596,6 +597,7 @@ struct TileInfo {
   int nr, nc;
   unsigned parts;    // two-body parts the tile touches (bit = vectorize slot)
   int nst;           // stored output cells
+  bool holefree;     // none of the four (m_l, m_s) groups holds a hole
 };
 struct PdBucket {  // one launch of the particle-hole tile kernel
   int first, count;
@@ -650,6 +652,8 @@ size_t tile_smem(const TileInfo& t, int tw) {
   const size_t tsz = ((size_t)t.nr * ld * tw + 1) & ~(size_t)1;
   return 8 * tsz + 16 * (size_t)t.nf + 8 * (size_t)t.npair;
 }
+// a task that only writes zeros keeps just the two pair lists
+size_t zero_smem(const TileInfo& t) { return 8 * (size_t)t.npair; }
 
 template <class T>
 int upload_vec(qd_layout* L, const std::vector<T>& vec, T** dptr) {
@@ -777,6 +781,8 @@ static int plan_122(qd_layout* L, Plan122** out) {
         t.nf = A.nf + B.nf;
         t.npair = A.npair + B.npair;
         t.parts = parts;
+        t.holefree = holes[order[a].first] == 0 && holes[order[a].second] == 0 && holes[order[b].first] == 0 &&
+                     holes[order[b].second] == 0;
         t.nst = 0;
         for (int c1 = 0; c1 < 3; ++c1)
           for (int c2 = 0; c2 <= c1; ++c2) t.nst += A.cnt[c1] * B.cnt[c2];
@@ -931,12 +937,18 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
   }
   const unsigned one = (1u << P_FHH) | (1u << P_FPP) | (1u << P_FPH);
   const bool fa0 = (zA & one) == one, fb0 = (zB & one) == one;  // a one-body part entirely zero
+  // a one-body part without hh and pp entries (the Magnus generator's) couples
+  // holes to particles only: on a tile whose four groups hold no hole every
+  // leg of its term sums over nothing
+  const unsigned hp = (1u << P_FHH) | (1u << P_FPP);
+  const bool spa = (zA & hp) == hp, spb = (zB & hp) == hp;
   const unsigned za2 = (zA >> P_HHHH) & 63u, zb2 = (zB >> P_HHHH) & 63u;
   // lists: 0 one operand (set), 1 both operands (set), 2 one operand (accumulate)
   std::vector<std::pair<size_t, int2>> lst[3];
   for (size_t i = 0; i < p->tiles.size(); ++i) {
     const TileInfo& t = p->tiles[i];
-    const bool nb = !fa0 && (t.parts & ~zb2), na = !fb0 && (t.parts & ~za2);
+    const bool nb = !fa0 && (t.parts & ~zb2) && !(spa && t.holefree);
+    const bool na = !fb0 && (t.parts & ~za2) && !(spb && t.holefree);
     const int op = (nb ? 1 : 0) | (na ? 2 : 0);
     if (op == 3) {
       if (tile_smem(t, 2) <= SMEM_MAX_122) {
@@ -946,7 +958,7 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
         lst[2].push_back({tile_smem(t, 1), int2{(int)i, 2 | 4}});
       }
     } else {
-      lst[0].push_back({tile_smem(t, 1), int2{(int)i, op}});  // op 0: zeros (the carve-out is kept)
+      lst[0].push_back({op ? tile_smem(t, 1) : zero_smem(t), int2{(int)i, op}});  // op 0: writes zeros
     }
   }
   TaskSet ts;
@@ -1255,7 +1267,8 @@ int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
         for (const Bucket122& b : tsv[i]->buckets)
           for (int k = b.first; k < b.first + b.count; ++k) {
             const int2 t = tsv[i]->h_task[k];
-            lists[b.list].push_back({tile_smem(pl[i]->tiles[t.x], b.tw), {t, (int)i}});
+            const TileInfo& ti = pl[i]->tiles[t.x];
+            lists[b.list].push_back({t.y == 0 ? zero_smem(ti) : tile_smem(ti, b.tw), {t, (int)i}});
           }
       }
       std::vector<int2> ht;
