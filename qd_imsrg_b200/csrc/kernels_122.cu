@@ -156,6 +156,27 @@ __host__ __device__ __forceinline__ bool leg_ok(int sparse, bool k_hole, bool t_
   return (nz >> (pair_class(t_hole, other_hole) * 3 + cfix)) & 1u;
 }
 
+// Bit 31 of a term's leg mask: its one-body factor couples holes to
+// particles only, so every leg changes the class of the pair it acts on.
+constexpr unsigned LEG_SPARSE = 1u << 31;
+
+// Regions (c1 * 3 + c2) of the staged operand that the legs of a tile read
+// when every leg changes the class of its pair by one: the four neighbours of
+// each stored output region (c1 >= c2) of the tile.  All regions otherwise.
+__device__ __forceinline__ unsigned regions_read(unsigned leg, const int ca[3], const int cb[3]) {
+  if (!(leg & LEG_SPARSE)) return 0x1FFu;
+  unsigned need = 0;
+  for (int c1 = 0; c1 < 3; ++c1)
+    for (int c2 = 0; c2 <= c1; ++c2) {
+      if (ca[c1] == 0 || cb[c2] == 0) continue;
+      if (c1 > 0) need |= 1u << ((c1 - 1) * 3 + c2);
+      if (c1 < 2) need |= 1u << ((c1 + 1) * 3 + c2);
+      if (c2 > 0) need |= 1u << (c1 * 3 + c2 - 1);
+      if (c2 < 2) need |= 1u << (c1 * 3 + c2 + 1);
+    }
+  return need;
+}
+
 // Sum over t of F(k, t) T[base + t * stride] for one leg: F(k, .) is the
 // leg's one-body row (component fy: 0 FA, 1 FB), t runs over the holes
 // [0, h) of the leg's group when bit 1 of ok is set and over its particles
@@ -268,11 +289,18 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
     // taken with herm.  It lands on its cell with the orientation sign of the
     // two pairs, and on the mirror cells (g = h) with the opposite ones.
     // The loops stay rolled: the kernel's code must fit the instruction cache.
+    int ca[3], cb[3];
+    for (int c = 0; c < 3; ++c) {
+      ca[c] = da.cnt(c);
+      cb[c] = db.cnt(c);
+    }
 #pragma unroll 1
     for (int x = 0; x < 2; ++x) {
       if (x == 0 ? !useA : !useB) continue;
       const double* src = x == 0 ? A : B;
       const unsigned zm = x == 0 ? zA : zB;
+      // the A term's legs carry FB (legA), the B term's FA (legB)
+      const unsigned need = regions_read(x == 0 ? legA : legB, ca, cb);
       const double hx = x == 0 ? hA : hB;
       const int xo = TW == 2 ? x : 0;
 #pragma unroll 1
@@ -281,7 +309,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
         const int r1 = da.cnt(c1), r2 = db.cnt(c2);
         const bool lower = c1 >= c2;
         const int part = lower ? slot_of(c1, c2) : slot_of(c2, c1);
-        if (r1 == 0 || r2 == 0 || ((zm >> (P_HHHH + part)) & 1u)) continue;
+        if (r1 == 0 || r2 == 0 || ((zm >> (P_HHHH + part)) & 1u) || !((need >> rg) & 1u)) continue;
         const int o1 = da.off(c1), o2 = db.off(c2);
         const double* srcp = src + __ldg(boff + part);
         const i64 ldv = lower ? cnt_of(c1, bd) : cnt_of(c2, bd);
@@ -1006,7 +1034,7 @@ static unsigned nz_mask(unsigned zmask) {
 // factor's sparsity, zstaged the zero-part mask of the staged operand.
 static unsigned leg_masks(int sparse, unsigned zstaged) {
   const unsigned nz = nz_mask(zstaged);
-  unsigned m = 0;
+  unsigned m = sparse ? LEG_SPARSE : 0u;
   for (int cfix = 0; cfix < 3; ++cfix)
     for (int bits = 0; bits < 8; ++bits)
       if (leg_ok(sparse, (bits >> 2) & 1, bits & 1, (bits >> 1) & 1, cfix, nz)) m |= 1u << (8 * cfix + bits);
