@@ -160,15 +160,23 @@ __host__ __device__ __forceinline__ bool leg_ok(int sparse, bool k_hole, bool t_
 // particles only, so every leg changes the class of the pair it acts on.
 constexpr unsigned LEG_SPARSE = 1u << 31;
 
+// Stored output regions (c1 >= c2) in the order of the output loop:
+// (0,0) (1,0) (1,1) (2,0) (2,1) (2,2) -> 0..5; bit r of an output mask.
+__host__ __device__ __forceinline__ int out_region(int c1, int c2) { return (c1 * (c1 + 1)) / 2 + c2; }
+constexpr unsigned OUT_ALL = 0x3Fu;
+// without ppph and pppp, which k_122_ppph / k_122_pppp write for a generator-like A
+constexpr unsigned OUT_NO_PP = 0x0Fu;
+
 // Regions (c1 * 3 + c2) of the staged operand that the legs of a tile read
 // when every leg changes the class of its pair by one: the four neighbours of
-// each stored output region (c1 >= c2) of the tile.  All regions otherwise.
-__device__ __forceinline__ unsigned regions_read(unsigned leg, const int ca[3], const int cb[3]) {
+// each stored output region (c1 >= c2) of the tile that the launch writes.
+// All regions otherwise.
+__device__ __forceinline__ unsigned regions_read(unsigned leg, const int ca[3], const int cb[3], unsigned outmask) {
   if (!(leg & LEG_SPARSE)) return 0x1FFu;
   unsigned need = 0;
   for (int c1 = 0; c1 < 3; ++c1)
     for (int c2 = 0; c2 <= c1; ++c2) {
-      if (ca[c1] == 0 || cb[c2] == 0) continue;
+      if (ca[c1] == 0 || cb[c2] == 0 || !((outmask >> out_region(c1, c2)) & 1u)) continue;
       if (c1 > 0) need |= 1u << ((c1 - 1) * 3 + c2);
       if (c1 < 2) need |= 1u << ((c1 + 1) * 3 + c2);
       if (c2 > 0) need |= 1u << (c1 * 3 + c2 - 1);
@@ -208,6 +216,7 @@ struct Inst122 {
   unsigned zB;
   unsigned legB;
   double* C;
+  unsigned outmask;
 };
 
 // Task: {tile, op}; op bit 0: the B term (FA x TB), bit 1: the A term
@@ -224,7 +233,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
                                                    const double2* __restrict__ F, int nfent,
                                                    const double* __restrict__ A, double hA, unsigned zA, unsigned legA,
                                                    const double* __restrict__ B, double hB, unsigned zB, unsigned legB,
-                                                   double* __restrict__ C,
+                                                   double* __restrict__ C, unsigned outmask,
                                                    const int* __restrict__ tinst, const Inst122* __restrict__ insts) {
   extern __shared__ __align__(16) double sm122[];
   if constexpr (MULTI) {  // a task of several layouts' task lists: this instance's tables and operands
@@ -244,6 +253,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
     zB = I.zB;
     legB = I.legB;
     C = I.C;
+    outmask = I.outmask;
   }
   const int2 task = tasks[blockIdx.x];
   const int2 tl = __ldg(&tiles[task.x]);
@@ -300,7 +310,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
       const double* src = x == 0 ? A : B;
       const unsigned zm = x == 0 ? zA : zB;
       // the A term's legs carry FB (legA), the B term's FA (legB)
-      const unsigned need = regions_read(x == 0 ? legA : legB, ca, cb);
+      const unsigned need = regions_read(x == 0 ? legA : legB, ca, cb, outmask);
       const double hx = x == 0 ? hA : hB;
       const int xo = TW == 2 ? x : 0;
 #pragma unroll 1
@@ -353,7 +363,7 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
   for (int rg = 0; rg < 6; ++rg) {
     const int c1 = rg < 1 ? 0 : (rg < 3 ? 1 : 2), c2 = rg - (c1 * (c1 + 1)) / 2;  // (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
     const int r1 = da.cnt(c1), r2 = db.cnt(c2);
-    if (r1 == 0 || r2 == 0) continue;
+    if (r1 == 0 || r2 == 0 || !((outmask >> rg) & 1u)) continue;
     const int o1 = da.off(c1), o2 = db.off(c2);
     const i64 base = __ldg(boff + slot_of(c1, c2));
     const i64 ldc = cnt_of(c1, bd);
@@ -403,6 +413,141 @@ __global__ void __launch_bounds__(T122, 1024 / T122) k_122_tile(DevLayout L, con
       else
         *out = y;
     }
+  }
+}
+
+// ---- commutator_122 for a generator-like A --------------------------------
+// When A's one-body part holds only fph (no hh or pp entries) and its
+// two-body part only Vpphh -- the Magnus generator Omega, the White
+// generator eta -- the leg sums above collapse, on the two largest output
+// parts of a block, to a few columns (or rows) of B each: every term dropped
+// is an exact zero (FA couples holes to particles only; A's other parts are
+// zero).  With fA(p, h) = A's fph, fB(p, h) = B's fph, pairs indexed within
+// the block, s the ordering sign of a pair (v_elem's), hA, hB the herm
+// factors and only holes t in G(x) or particles as stated:
+//   C_pppp = hB W^T - hA W,
+//     W(:, (a,b)) = sum_{t in G(a)} fA(a,t) B_ppph(:, (t,b)) - sum_{t in G(b)} fA(b,t) B_ppph(:, (t,a));
+//   C_ppph(:, (h,p)) = - sum_{particles t in G(h)} s fA(t,h) B_pppp(:, (t,p))
+//                      - sum_{t in G(p)} s [hA fA(p,t) B_pphh(:, (h,t)) - hB fB(p,t) A_pphh(:, (h,t))]
+//   C_ppph((a,b), :) += sum_{t in G(a)} fA(a,t) B_phph((t,b), :) - sum_{t in G(b)} fA(b,t) B_phph((t,a), :).
+// (Both checked against the oracle's commutator_122 in numpy before this
+// kernel was written.)  B_ppph and B_phph are small (L2 resident); the
+// kernels stream C_pppp and C_ppph out once.  Term tables (per layout):
+//   pp pair: {ph index of (t, b) or (t, a), t | (a or b - n) << 8 | neg << 20}
+//   ph pair: {column, hole | (particle - n) << 8 | neg << 20, kind}: kind 0 a
+//            B_pppp column with coefficient -s fA(t, h); kind 1 an hh column
+//            (h, t) of B_pphh and A_pphh.
+__host__ __device__ __forceinline__ bool gen_like(unsigned zmask) {
+  return (zmask | (1u << P_FPH) | (1u << P_PPHH)) == ALL_PARTS;
+}
+
+constexpr int SP_T = 256, SP_B = 64, SP_LD = SP_B + 1;
+
+__device__ __forceinline__ double sp_coef(const DevLayout& L, const double* __restrict__ f, int code) {
+  const double v = __ldg(&f[L.o_fph + ((code >> 8) & 0xFFF) + (i64)(code & 0xFF) * L.mp]);
+  return (code >> 20) & 1 ? -v : v;
+}
+
+// One task = the tile pair (I, J), (J, I) of a block's C_pppp (64 x 64 each).
+__global__ void __launch_bounds__(SP_T) k_122_pppp(DevLayout L, const int4* __restrict__ tasks,
+                                                  const int* __restrict__ ppbase, const int* __restrict__ ppstart,
+                                                  const int2* __restrict__ ppterm, const double* __restrict__ A,
+                                                  double hA, const double* __restrict__ B, double hB, unsigned zB,
+                                                  double* __restrict__ C) {
+  extern __shared__ double spw[];  // W1[c][r] = W(I0 + r, J0 + c), W2[c][r] = W(J0 + r, I0 + c)
+  const int4 t = tasks[blockIdx.x];
+  const int q = t.x, I0 = t.y * SP_B, J0 = t.z * SP_B;
+  const int4 bd = __ldg(&L.blk[q]);
+  const int np = bd.z;
+  const i64* boff = L.boff + 6 * q;
+  const bool live = !((zB >> P_PPPH) & 1u);
+  const double* X = B + __ldg(boff + 4);  // B_ppph, np x nph
+  const int pb = __ldg(&ppbase[q]);
+  const int tid = threadIdx.x, r = tid & (SP_B - 1), cg = tid >> 6;
+  const bool diag = t.y == t.z;
+  for (int pass = 0; pass < (diag ? 1 : 2); ++pass) {
+    const int R0 = pass == 0 ? I0 : J0, C0 = pass == 0 ? J0 : I0;
+    double* W = spw + pass * SP_B * SP_LD;
+    const int row = R0 + r;
+    for (int cc = cg; cc < SP_B; cc += SP_T / SP_B) {
+      const int col = C0 + cc;
+      double w = 0.0;
+      if (live && row < np && col < np) {
+        const int e1 = __ldg(&ppstart[pb + col + 1]);
+        for (int e = __ldg(&ppstart[pb + col]); e < e1; ++e) {
+          const int2 tm = __ldg(&ppterm[e]);
+          w += sp_coef(L, A, tm.y) * X[row + (i64)tm.x * np];
+        }
+      }
+      W[cc * SP_LD + r] = w;
+    }
+  }
+  __syncthreads();
+  const double* W1 = spw;
+  const double* W2 = diag ? spw : spw + SP_B * SP_LD;
+  double* out = C + __ldg(boff + 1);
+  for (int idx = tid; idx < SP_B * SP_B; idx += SP_T) {
+    const int rr = idx & (SP_B - 1), c = idx >> 6;
+    if (I0 + rr < np && J0 + c < np)  // C(I0 + rr, J0 + c) = hB W(J0 + c, I0 + rr) - hA W(I0 + rr, J0 + c)
+      out[(I0 + rr) + (i64)(J0 + c) * np] = hB * W2[rr * SP_LD + c] - hA * W1[c * SP_LD + rr];
+  }
+  if (diag) return;
+  for (int idx = tid; idx < SP_B * SP_B; idx += SP_T) {
+    const int rr = idx & (SP_B - 1), c = idx >> 6;
+    if (J0 + rr < np && I0 + c < np)  // C(J0 + rr, I0 + c) = hB W(I0 + c, J0 + rr) - hA W(J0 + rr, I0 + c)
+      out[(J0 + rr) + (i64)(I0 + c) * np] = hB * W1[rr * SP_LD + c] - hA * W2[c * SP_LD + rr];
+  }
+}
+
+// One task = a 64 x 64 tile of a block's C_ppph (rows pp pairs, columns ph pairs).
+__global__ void __launch_bounds__(SP_T) k_122_ppph(DevLayout L, const int4* __restrict__ tasks,
+                                                  const int* __restrict__ ppbase, const int* __restrict__ ppstart,
+                                                  const int2* __restrict__ ppterm, const int* __restrict__ phbase,
+                                                  const int* __restrict__ phstart, const int4* __restrict__ phterm,
+                                                  const double* __restrict__ A, double hA, unsigned zA,
+                                                  const double* __restrict__ B, double hB, unsigned zB,
+                                                  double* __restrict__ C) {
+  const int4 t = tasks[blockIdx.x];
+  const int q = t.x, I0 = t.y * SP_B, J0 = t.z * SP_B;
+  const int4 bd = __ldg(&L.blk[q]);
+  const int nh = bd.x, nb = bd.y, np = bd.z;
+  const i64* boff = L.boff + 6 * q;
+  const double* Bpppp = B + __ldg(boff + 1);
+  const double* Bpphh = B + __ldg(boff + 2);
+  const double* Bphph = B + __ldg(boff + 3);
+  const double* Apphh = A + __ldg(boff + 2);
+  const bool lpp = !((zB >> P_PPPP) & 1u), lbh = !((zB >> P_PPHH) & 1u) && nh > 0;
+  const bool lah = !((zA >> P_PPHH) & 1u) && nh > 0, lph = !((zB >> P_PHPH) & 1u);
+  const int pb = __ldg(&ppbase[q]), hb = __ldg(&phbase[q]);
+  const int tid = threadIdx.x, r = tid & (SP_B - 1), cg = tid >> 6;
+  const int row = I0 + r;
+  if (row >= np) return;  // no barrier below
+  const int er0 = __ldg(&ppstart[pb + row]), er1 = __ldg(&ppstart[pb + row + 1]);
+  double* out = C + __ldg(boff + 4);
+  for (int cc = cg; cc < SP_B; cc += SP_T / SP_B) {
+    const int col = J0 + cc;
+    if (col >= nb) break;
+    double y = 0.0;
+    // the column's legs (ket): columns of B_pppp, B_pphh, A_pphh
+    const int e1 = __ldg(&phstart[hb + col + 1]);
+    for (int e = __ldg(&phstart[hb + col]); e < e1; ++e) {
+      const int4 tm = __ldg(&phterm[e]);
+      if (tm.z == 0) {
+        if (lpp) y -= sp_coef(L, A, tm.y) * Bpppp[row + (i64)tm.x * np];
+      } else {
+        const double sg = ((tm.y >> 20) & 1) ? -1.0 : 1.0;
+        const int fo = ((tm.y >> 8) & 0xFFF) + (tm.y & 0xFF) * L.mp;
+        if (lbh) y -= sg * hA * __ldg(&A[L.o_fph + fo]) * Bpphh[row + (i64)tm.x * np];
+        if (lah) y += sg * hB * __ldg(&B[L.o_fph + fo]) * Apphh[row + (i64)tm.x * np];
+      }
+    }
+    // the row's legs (bra): rows of B_phph
+    if (lph)
+      for (int e = er0; e < er1; ++e) {
+        const int2 tm = __ldg(&ppterm[e]);
+        y += sp_coef(L, A, tm.y) * Bphph[tm.x + (i64)col * nb];
+      }
+    out[row + (i64)col * np] = y;
   }
 }
 
@@ -626,6 +771,7 @@ struct TileInfo {
   unsigned parts;    // two-body parts the tile touches (bit = vectorize slot)
   int nst;           // stored output cells
   bool holefree;     // none of the four (m_l, m_s) groups holds a hole
+  unsigned outs;     // stored output regions of the tile (bit out_region(c1, c2))
 };
 struct PdBucket {  // one launch of the particle-hole tile kernel
   int first, count;
@@ -646,6 +792,7 @@ struct TaskSet {
   std::vector<int2> h_task;  // host copy (merged launches of several layouts)
   std::vector<Bucket122> buckets;
   bool tuned = false;
+  unsigned outmask = OUT_ALL;  // output regions the tiles write (OUT_NO_PP: A generator-like)
   int bounds_id = 0;           // which bucketing (see kBounds) the tuner kept
   float ms_total = 0.f;        // tuned time of this bucketing
   std::vector<TaskSet> alts;   // the other bucketings, until tuned
@@ -666,6 +813,15 @@ struct Plan122 {
   int ng = 0;
   int* d_ptask = nullptr;
   std::vector<PdBucket> pbuckets;
+  // generator-like A: term tables of k_122_pppp / k_122_ppph and their tasks
+  int* d_ppbase = nullptr;   // per block: first pp pair
+  int* d_ppstart = nullptr;  // per pp pair: first term (one more entry at the end)
+  int2* d_ppterm = nullptr;
+  int* d_phbase = nullptr;   // per block: first ph pair
+  int* d_phstart = nullptr;  // per ph pair: first term (one more entry at the end)
+  int4* d_phterm = nullptr;
+  int4* d_sptask = nullptr;  // C_pppp tile pairs, then C_ppph tiles
+  int nsp_pppp = 0, nsp_ppph = 0;
 };
 std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
@@ -801,6 +957,10 @@ static int plan_122(qd_layout* L, Plan122** out) {
             }
         if (!out) continue;
         TileInfo t;
+        t.outs = 0;
+        for (int c1 = 0; c1 < 3; ++c1)
+          for (int c2 = 0; c2 <= c1; ++c2)
+            if (A.cnt[c1] > 0 && B.cnt[c2] > 0) t.outs |= 1u << out_region(c1, c2);
         t.a = u0 + (int)a;
         t.b = u0 + (int)b;
         t.nr = A.n1 * A.n2;
@@ -829,6 +989,73 @@ static int plan_122(qd_layout* L, Plan122** out) {
       (rc = upload_vec(L, th, &p.d_tiles)) ||
       (rc = upload_vec(L, sbase, &p.d_sbase)))
     return rc;
+  // generator-like A: per block its pp and ph pairs' terms (see k_122_pppp)
+  {
+    const int n = L->n;
+    std::vector<int> ppbase(L->nblock), phbase(L->nblock), ppstart(1, 0), phstart(1, 0);
+    std::vector<int2> ppterm;
+    std::vector<int4> phterm, sptask[2];
+    int npp_all = 0, nph_all = 0;
+    for (int q = 0; q < L->nblock; ++q) {
+      const int nh = L->blk[q].x, nb = L->blk[q].y, np = L->blk[q].z, pb = L->pbase[q];
+      ppbase[q] = npp_all;
+      phbase[q] = nph_all;
+      npp_all += np;
+      nph_all += nb;
+      std::map<std::pair<int, int>, int> ihh, iph, ipp;
+      for (int k = 0; k < nh; ++k) ihh[{L->pairs[pb + k].x, L->pairs[pb + k].y}] = k;
+      for (int k = 0; k < nb; ++k) iph[{L->pairs[pb + nh + k].x, L->pairs[pb + nh + k].y}] = k;
+      for (int k = 0; k < np; ++k) ipp[{L->pairs[pb + nh + nb + k].x, L->pairs[pb + nh + nb + k].y}] = k;
+      auto code = [&](int hole, int part, bool neg) { return hole | ((part - n) << 8) | ((neg ? 1 : 0) << 20); };
+      auto members = [&](int x) { return std::make_pair(L->gstart[L->gid[x]], L->gstart[L->gid[x] + 1]); };
+      for (int k = 0; k < np; ++k) {  // pp pair (a, b): +fA(a,t) (t,b), -fA(b,t) (t,a), holes t
+        const int a = L->pairs[pb + nh + nb + k].x, b = L->pairs[pb + nh + nb + k].y;
+        for (int side = 0; side < 2; ++side) {
+          const int x = side == 0 ? a : b, y = side == 0 ? b : a;
+          const auto mr = members(x);
+          for (int u = mr.first; u < mr.second; ++u) {
+            const int tt = L->gmem[u];
+            if (tt >= n) continue;
+            auto f = iph.find({tt, y});
+            if (f != iph.end()) ppterm.push_back(int2{f->second, code(tt, x, side == 1)});
+          }
+        }
+        ppstart.push_back((int)ppterm.size());
+      }
+      for (int k = 0; k < nb; ++k) {  // ph pair (h, p)
+        const int hh = L->pairs[pb + nh + k].x, pp = L->pairs[pb + nh + k].y;
+        auto mr = members(hh);
+        for (int u = mr.first; u < mr.second; ++u) {  // particles t in G(h): B_pppp column (t, p)
+          const int tt = L->gmem[u];
+          if (tt < n || tt == pp) continue;
+          auto f = ipp.find({std::min(tt, pp), std::max(tt, pp)});
+          if (f != ipp.end()) phterm.push_back(int4{f->second, code(hh, tt, tt > pp), 0, 0});
+        }
+        mr = members(pp);
+        for (int u = mr.first; u < mr.second; ++u) {  // holes t in G(p): hh column (h, t)
+          const int tt = L->gmem[u];
+          if (tt >= n || tt == hh) continue;
+          auto f = ihh.find({std::min(hh, tt), std::max(hh, tt)});
+          if (f != ihh.end()) phterm.push_back(int4{f->second, code(tt, pp, hh > tt), 1, 0});
+        }
+        phstart.push_back((int)phterm.size());
+      }
+      const int tr = (np + SP_B - 1) / SP_B, tc = (nb + SP_B - 1) / SP_B;
+      for (int i = 0; i < tr; ++i)
+        for (int j = i; j < tr; ++j) sptask[0].push_back(int4{q, i, j, 0});
+      for (int i = 0; i < tr; ++i)
+        for (int j = 0; j < tc; ++j) sptask[1].push_back(int4{q, i, j, 1});
+    }
+    p.nsp_pppp = (int)sptask[0].size();
+    p.nsp_ppph = (int)sptask[1].size();
+    std::vector<int4> all = sptask[0];
+    all.insert(all.end(), sptask[1].begin(), sptask[1].end());
+    if ((rc = upload_vec(L, ppbase, &p.d_ppbase)) || (rc = upload_vec(L, ppstart, &p.d_ppstart)) ||
+        (rc = upload_vec(L, ppterm, &p.d_ppterm)) || (rc = upload_vec(L, phbase, &p.d_phbase)) ||
+        (rc = upload_vec(L, phstart, &p.d_phstart)) || (rc = upload_vec(L, phterm, &p.d_phterm)) ||
+        (rc = upload_vec(L, all, &p.d_sptask)))
+      return rc;
+  }
   // particle-hole channel: first cc row of each (G1, G2) and the launches
   p.ng = ngroup;
   std::vector<int2> zrow((size_t)ngroup * ngroup);
@@ -889,7 +1116,8 @@ static int plan_122(qd_layout* L, Plan122** out) {
                          (const void*)k_122_tile<1, 256, false>, (const void*)k_122_tile<2, 256, false>,
                          (const void*)k_122_tile<1, 256, true>, (const void*)k_122_tile<2, 256, true>,
                          (const void*)k_pandya_tile<PD_ALL4>, (const void*)k_pandya_tile<PD_PAIRS>,
-                         (const void*)k_pandya_tile<PD_SINGLE>, (const void*)k_pandya_tile<PD_DIRECT>}) {
+                         (const void*)k_pandya_tile<PD_SINGLE>, (const void*)k_pandya_tile<PD_DIRECT>,
+                         (const void*)k_122_pppp}) {
     cudaFuncAttributes fa;
     QD_CUDA(cudaFuncGetAttributes(&fa, fn));
     QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -973,8 +1201,10 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
   const unsigned za2 = (zA >> P_HHHH) & 63u, zb2 = (zB >> P_HHHH) & 63u;
   // lists: 0 one operand (set), 1 both operands (set), 2 one operand (accumulate)
   std::vector<std::pair<size_t, int2>> lst[3];
+  const unsigned outmask = gen_like(zA) ? OUT_NO_PP : OUT_ALL;
   for (size_t i = 0; i < p->tiles.size(); ++i) {
     const TileInfo& t = p->tiles[i];
+    if (!(t.outs & outmask)) continue;  // every output of the tile comes from k_122_pppp / k_122_ppph
     const bool nb = !fa0 && (t.parts & ~zb2) && !(spa && t.holefree);
     const bool na = !fb0 && (t.parts & ~za2) && !(spb && t.holefree);
     const int op = (nb ? 1 : 0) | (na ? 2 : 0);
@@ -992,6 +1222,7 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
   TaskSet ts;
   for (int bid = 0; bid < kNumBounds; ++bid) {
     TaskSet& v = bid == 0 ? ts : (ts.alts.emplace_back(), ts.alts.back());
+    v.outmask = outmask;
     int rc = build_variant(L, p, lst, bid, v);
     if (rc) return rc;
   }
@@ -1006,7 +1237,9 @@ void drop_122_plan(const qd_layout* L) {
   if (it == plans().end()) return;
   Plan122& p = it->second;
   for (void* ptr : {(void*)p.d_gpd, (void*)p.d_gpp, (void*)p.d_tiles, (void*)p.d_sbase,
-                    (void*)p.d_ftab, (void*)p.d_gpg, (void*)p.d_zrow, (void*)p.d_ptask})
+                    (void*)p.d_ftab, (void*)p.d_gpg, (void*)p.d_zrow, (void*)p.d_ptask, (void*)p.d_ppbase,
+                    (void*)p.d_ppstart, (void*)p.d_ppterm, (void*)p.d_phbase, (void*)p.d_phstart,
+                    (void*)p.d_phterm, (void*)p.d_sptask})
     if (ptr) cudaFree(ptr);
   for (auto& kv : p.sets) {
     if (kv.second.d_task) cudaFree(kv.second.d_task);
@@ -1049,7 +1282,8 @@ static int launch_bucket(qd_layout* L, const Plan122* p, const TaskSet* ts, cons
   k_122_tile<TW, NT, false><<<b.count, NT, b.smem, L->stream>>>(L->dev, ts->d_task + b.first, p->d_tiles, p->d_gpd,   \
                                                          p->d_gpp, p->d_ftab, p->nfent, A->d,                   \
                                                          (double)A->herm, A->zero_mask, legA, B->d,             \
-                                                         (double)B->herm, B->zero_mask, legB, C, nullptr, nullptr)
+                                                         (double)B->herm, B->zero_mask, legB, C, ts->outmask,   \
+                                                         nullptr, nullptr)
   if (b.tw == 2) {
     if (threads == 64) QD_122_LAUNCH(2, 64); else if (threads == 128) QD_122_LAUNCH(2, 128); else QD_122_LAUNCH(2, 256);
   } else {
@@ -1202,6 +1436,26 @@ int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B) {
   return QD_OK;
 }
 
+// C_pppp and C_ppph of every block for a generator-like A (k_122_pppp,
+// k_122_ppph) on stream st.
+static int launch_122_gen(qd_layout* L, const Plan122* p, const qd_op* A, const qd_op* B, double* C,
+                          cudaStream_t st) {
+  if (p->nsp_pppp > 0) {
+    k_122_pppp<<<p->nsp_pppp, SP_T, 2 * SP_B * SP_LD * sizeof(double), st>>>(
+        L->dev, p->d_sptask, p->d_ppbase, p->d_ppstart, p->d_ppterm, A->d, (double)A->herm, B->d, (double)B->herm,
+        B->zero_mask, C);
+    ++L->nlaunch;
+  }
+  if (p->nsp_ppph > 0) {
+    k_122_ppph<<<p->nsp_ppph, SP_T, 0, st>>>(L->dev, p->d_sptask + p->nsp_pppp, p->d_ppbase, p->d_ppstart,
+                                             p->d_ppterm, p->d_phbase, p->d_phstart, p->d_phterm, A->d,
+                                             (double)A->herm, A->zero_mask, B->d, (double)B->herm, B->zero_mask, C);
+    ++L->nlaunch;
+  }
+  QD_CUDA(cudaGetLastError());
+  return QD_OK;
+}
+
 int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   Plan122* p;
   int rc = plan_122(L, &p);
@@ -1215,6 +1469,7 @@ int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
                                                   (double)B->herm, p->d_ftab, p->gmax, p->nfent);
   ++L->nlaunch;
   if (!ts->tuned && !L->prof.on && !capturing(L->stream)) TRY(tune_122(L, p, ts, A, B, spA, spB));
+  if (ts->outmask != OUT_ALL) TRY(launch_122_gen(L, p, A, B, C, L->stream));
   for (const Bucket122& b : ts->buckets) TRY(launch_bucket(L, p, ts, b, b.threads, A, B, spA, spB, C));
   QD_CUDA(cudaGetLastError());
   return QD_OK;
@@ -1377,17 +1632,19 @@ int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
     I.zB = it.B->zero_mask;
     I.legB = leg_masks(spars(it.A), it.B->zero_mask);
     I.C = it.C;
+    I.outmask = tsv[i]->outmask;
+    if (I.outmask != OUT_ALL) TRY(launch_122_gen(it.L, p, it.A, it.B, it.C, st));
   }
   QD_CUDA(cudaMemcpyAsync(m->d_inst, m->h_inst, n * sizeof(Inst122), cudaMemcpyHostToDevice, st));
   const DevLayout& L0 = items[0].L->dev;
   for (const Bucket122& b : m->buckets) {
     if (b.tw == 2)
       k_122_tile<2, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr, 0,
-                                                       nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
+                                                       nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr, 0u,
                                                        m->d_tinst + b.first, m->d_inst);
     else
       k_122_tile<1, 256, true><<<b.count, 256, b.smem, st>>>(L0, m->d_task + b.first, nullptr, nullptr, nullptr, nullptr, 0,
-                                                       nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr,
+                                                       nullptr, 0.0, 0u, 0u, nullptr, 0.0, 0u, 0u, nullptr, 0u,
                                                        m->d_tinst + b.first, m->d_inst);
     ++items[0].L->nlaunch;
   }
