@@ -164,8 +164,8 @@ constexpr unsigned LEG_SPARSE = 1u << 31;
 // (0,0) (1,0) (1,1) (2,0) (2,1) (2,2) -> 0..5; bit r of an output mask.
 __host__ __device__ __forceinline__ int out_region(int c1, int c2) { return (c1 * (c1 + 1)) / 2 + c2; }
 constexpr unsigned OUT_ALL = 0x3Fu;
-// without ppph and pppp, which k_122_ppph / k_122_pppp write for a generator-like A
-constexpr unsigned OUT_NO_PP = 0x0Fu;
+// none: k_122_pppp and k_122_gen write every part for a generator-like A
+constexpr unsigned OUT_NONE = 0u;
 
 // Regions (c1 * 3 + c2) of the staged operand that the legs of a tile read
 // when every leg changes the class of its pair by one: the four neighbours of
@@ -499,55 +499,77 @@ __global__ void __launch_bounds__(SP_T) k_122_pppp(DevLayout L, const int4* __re
   }
 }
 
-// One task = a 64 x 64 tile of a block's C_ppph (rows pp pairs, columns ph pairs).
-__global__ void __launch_bounds__(SP_T) k_122_ppph(DevLayout L, const int4* __restrict__ tasks,
-                                                  const int* __restrict__ ppbase, const int* __restrict__ ppstart,
-                                                  const int2* __restrict__ ppterm, const int* __restrict__ phbase,
-                                                  const int* __restrict__ phstart, const int4* __restrict__ phterm,
-                                                  const double* __restrict__ A, double hA, unsigned zA,
-                                                  const double* __restrict__ B, double hB, unsigned zB,
-                                                  double* __restrict__ C) {
+// The other five parts of a block for a generator-like A, one 64 x 64 tile
+// of one part per task {q, part, ti, tj}: every output element (R, c) is
+//   sum over the terms of its row pair of coef * M[idx + c ld] (M[c + idx ld] transposed)
+// + sum over the terms of its column pair of coef * M[R + idx ld] (M[idx + R ld] transposed),
+// M a stored part of A or B in block q with ld rows.  Term {idx, coefficient
+// offset, flags, source}: flags bit 0 negate, 1 times hA, 2 times hB, 3 the
+// coefficient is B's entry (else A's); source (operand << 4) | (T << 3) | slot.
+// The closed forms (derived from the leg sums, each checked against the
+// oracle's commutator_122 in numpy first), with s an ordering sign:
+//   ppph rows (a,b): +-fA(a|b,t) B_phph((t,b|a), .);  columns (h,p):
+//        -s fA(t,h) B_pppp(., (t,p)) [particles t in G(h)],
+//        -s hA fA(p,t) B_pphh(., (h,t)) + s hB fB(p,t) A_pphh(., (h,t)) [holes t in G(p)]
+//   pphh rows (a,b): +-fA(a|b,t) B_phhh((t,b|a), .) - s hB fppB(t,a|b) A_pphh((t,b)|(a,t), .);
+//        columns (k,l): +-fA(t,k|l) B_ppph(., (l|k,t)) + s hB fhhB(k|l,t) A_pphh(., (t,l)|(k,t))
+//   phhh rows (h,p): s hA fA(t,h) B_pphh((t,p), .) - s hB fB(t,h) A_pphh((t,p), .) + s fA(p,t) B_hhhh((h,t), .);
+//        columns (k,l): +-fA(t,k|l) B_phph(., (l|k,t))
+//   phph rows (h,p): s hA fA(t,h) B_ppph((t,p), .) + s hB fA(p,t) B_phhh(., (h,t))^T;
+//        columns (k,l): -s hB fA(t,k) B_ppph((t,l), .)^T - s hA fA(l,t) B_phhh(., (k,t))
+//   hhhh rows (a,b): -+hA fA(t,a|b) B_phhh((b|a,t), .);  columns (k,l): +-hB fA(t,k|l) B_phhh((l|k,t), .)^T
+struct GenTables {
+  const int* gbase;   // 3 * nblock: first hh, ph, pp pair of each block
+  const int* rstart;  // per part: per row pair its first term (one more entry at the end)
+  const int* cstart;
+  const int4* rterm;
+  const int4* cterm;
+  int rso[6], cso[6];  // offset of each part's start array (slot order)
+};
+
+__device__ __forceinline__ double gen_term(const DevLayout& L, const int4& tm, const double* __restrict__ A,
+                                           double hA, unsigned zA, const double* __restrict__ B, double hB,
+                                           unsigned zB, int q, int4 bd, int fixed, bool row_term) {
+  const int opd = tm.w >> 4, slot = tm.w & 7;
+  const bool tr = (tm.w >> 3) & 1;
+  if ((((opd ? zB : zA) >> (P_HHHH + slot)) & 1u)) return 0.0;
+  const double* M = (opd ? B : A) + __ldg(L.boff + 6 * q + slot);
+  const i64 ld = part_rows(P_HHHH + slot, bd);
+  double c = __ldg(&((tm.z >> 3) & 1 ? B : A)[tm.y]);
+  if (tm.z & 2) c *= hA;
+  if (tm.z & 4) c *= hB;
+  if (tm.z & 1) c = -c;
+  // row term: fixed = output column; column term: fixed = output row
+  const i64 e = (row_term != tr) ? tm.x + (i64)fixed * ld : fixed + (i64)tm.x * ld;
+  return c * M[e];
+}
+
+__global__ void __launch_bounds__(SP_T) k_122_gen(DevLayout L, const int4* __restrict__ tasks, GenTables G,
+                                                 const double* __restrict__ A, double hA, unsigned zA,
+                                                 const double* __restrict__ B, double hB, unsigned zB,
+                                                 double* __restrict__ C) {
   const int4 t = tasks[blockIdx.x];
-  const int q = t.x, I0 = t.y * SP_B, J0 = t.z * SP_B;
+  const int q = t.x, slot = t.y, I0 = t.z * SP_B, J0 = t.w * SP_B;
   const int4 bd = __ldg(&L.blk[q]);
-  const int nh = bd.x, nb = bd.y, np = bd.z;
-  const i64* boff = L.boff + 6 * q;
-  const double* Bpppp = B + __ldg(boff + 1);
-  const double* Bpphh = B + __ldg(boff + 2);
-  const double* Bphph = B + __ldg(boff + 3);
-  const double* Apphh = A + __ldg(boff + 2);
-  const bool lpp = !((zB >> P_PPPP) & 1u), lbh = !((zB >> P_PPHH) & 1u) && nh > 0;
-  const bool lah = !((zA >> P_PPHH) & 1u) && nh > 0, lph = !((zB >> P_PHPH) & 1u);
-  const int pb = __ldg(&ppbase[q]), hb = __ldg(&phbase[q]);
+  int cr, cc;
+  part_classes(P_HHHH + slot, cr, cc);
+  const int nrow = part_rows(P_HHHH + slot, bd), ncol = cc == 0 ? bd.x : (cc == 1 ? bd.y : bd.z);
   const int tid = threadIdx.x, r = tid & (SP_B - 1), cg = tid >> 6;
   const int row = I0 + r;
-  if (row >= np) return;  // no barrier below
-  const int er0 = __ldg(&ppstart[pb + row]), er1 = __ldg(&ppstart[pb + row + 1]);
-  double* out = C + __ldg(boff + 4);
-  for (int cc = cg; cc < SP_B; cc += SP_T / SP_B) {
-    const int col = J0 + cc;
-    if (col >= nb) break;
+  if (row >= nrow) return;  // no barrier below
+  const int* rs = G.rstart + G.rso[slot] + __ldg(&G.gbase[cr * L.nblock + q]);
+  const int* cs = G.cstart + G.cso[slot] + __ldg(&G.gbase[cc * L.nblock + q]);
+  const int er0 = __ldg(&rs[row]), er1 = __ldg(&rs[row + 1]);
+  double* out = C + __ldg(L.boff + 6 * q + slot);
+  for (int k = cg; k < SP_B; k += SP_T / SP_B) {
+    const int col = J0 + k;
+    if (col >= ncol) break;
     double y = 0.0;
-    // the column's legs (ket): columns of B_pppp, B_pphh, A_pphh
-    const int e1 = __ldg(&phstart[hb + col + 1]);
-    for (int e = __ldg(&phstart[hb + col]); e < e1; ++e) {
-      const int4 tm = __ldg(&phterm[e]);
-      if (tm.z == 0) {
-        if (lpp) y -= sp_coef(L, A, tm.y) * Bpppp[row + (i64)tm.x * np];
-      } else {
-        const double sg = ((tm.y >> 20) & 1) ? -1.0 : 1.0;
-        const int fo = ((tm.y >> 8) & 0xFFF) + (tm.y & 0xFF) * L.mp;
-        if (lbh) y -= sg * hA * __ldg(&A[L.o_fph + fo]) * Bpphh[row + (i64)tm.x * np];
-        if (lah) y += sg * hB * __ldg(&B[L.o_fph + fo]) * Apphh[row + (i64)tm.x * np];
-      }
-    }
-    // the row's legs (bra): rows of B_phph
-    if (lph)
-      for (int e = er0; e < er1; ++e) {
-        const int2 tm = __ldg(&ppterm[e]);
-        y += sp_coef(L, A, tm.y) * Bphph[tm.x + (i64)col * nb];
-      }
-    out[row + (i64)col * np] = y;
+    const int e1 = __ldg(&cs[col + 1]);
+    for (int e = __ldg(&cs[col]); e < e1; ++e)
+      y += gen_term(L, __ldg(&G.cterm[e]), A, hA, zA, B, hB, zB, q, bd, row, false);
+    for (int e = er0; e < er1; ++e) y += gen_term(L, __ldg(&G.rterm[e]), A, hA, zA, B, hB, zB, q, bd, col, true);
+    out[row + (i64)col * nrow] = y;
   }
 }
 
@@ -792,7 +814,7 @@ struct TaskSet {
   std::vector<int2> h_task;  // host copy (merged launches of several layouts)
   std::vector<Bucket122> buckets;
   bool tuned = false;
-  unsigned outmask = OUT_ALL;  // output regions the tiles write (OUT_NO_PP: A generator-like)
+  unsigned outmask = OUT_ALL;  // output regions the tiles write (OUT_NONE: A generator-like)
   int bounds_id = 0;           // which bucketing (see kBounds) the tuner kept
   float ms_total = 0.f;        // tuned time of this bucketing
   std::vector<TaskSet> alts;   // the other bucketings, until tuned
@@ -813,15 +835,18 @@ struct Plan122 {
   int ng = 0;
   int* d_ptask = nullptr;
   std::vector<PdBucket> pbuckets;
-  // generator-like A: term tables of k_122_pppp / k_122_ppph and their tasks
+  // generator-like A: term tables of k_122_pppp / k_122_gen and their tasks
   int* d_ppbase = nullptr;   // per block: first pp pair
   int* d_ppstart = nullptr;  // per pp pair: first term (one more entry at the end)
   int2* d_ppterm = nullptr;
-  int* d_phbase = nullptr;   // per block: first ph pair
-  int* d_phstart = nullptr;  // per ph pair: first term (one more entry at the end)
-  int4* d_phterm = nullptr;
-  int4* d_sptask = nullptr;  // C_pppp tile pairs, then C_ppph tiles
-  int nsp_pppp = 0, nsp_ppph = 0;
+  int* d_gbase = nullptr;    // 3 * nblock: first hh, ph, pp pair of each block
+  int* d_rstart = nullptr;   // k_122_gen row and column term starts, per slot at gen_rso / gen_cso
+  int* d_cstart = nullptr;
+  int4* d_rterm = nullptr;
+  int4* d_cterm = nullptr;
+  int gen_rso[6] = {0}, gen_cso[6] = {0};
+  int4* d_sptask = nullptr;  // C_pppp tile pairs, then the k_122_gen tiles
+  int nsp_pppp = 0, nsp_gen = 0;
 };
 std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
@@ -989,70 +1014,200 @@ static int plan_122(qd_layout* L, Plan122** out) {
       (rc = upload_vec(L, th, &p.d_tiles)) ||
       (rc = upload_vec(L, sbase, &p.d_sbase)))
     return rc;
-  // generator-like A: per block its pp and ph pairs' terms (see k_122_pppp)
+  // generator-like A: the pp pairs' W terms (k_122_pppp) and the row and
+  // column terms of the other five parts (k_122_gen), per block
   {
-    const int n = L->n;
-    std::vector<int> ppbase(L->nblock), phbase(L->nblock), ppstart(1, 0), phstart(1, 0);
+    const int n = L->n, mp = L->mp;
+    const int ofph = (int)L->o_fph, ofpp = (int)L->o_fpp, ofhh = (int)L->o_fhh;
+    std::vector<int> gbase(3 * L->nblock), ppstart(1, 0);
     std::vector<int2> ppterm;
-    std::vector<int4> phterm, sptask[2];
-    int npp_all = 0, nph_all = 0;
+    // per slot: its terms and, per pair of its classes (block order), their starts
+    std::vector<int> rst[6], cst[6];
+    std::vector<int4> rterm_s[6], cterm_s[6];
+    std::vector<int4> ptask, gtask;
+    int cnt[3] = {0, 0, 0};
+    enum { NEG = 1, MA = 2, MB = 4, CB = 8 };
+    auto fA = [&](int pt, int h) { return ofph + (pt - n) + h * mp; };  // A's or B's fph(p, h)
+    auto fpp = [&](int t, int b) { return ofpp + (t - n) + (b - n) * mp; };
+    auto fhh = [&](int k, int t) { return ofhh + k + t * n; };
+    auto src = [](int opd, int slot, int tr) { return (opd << 4) | (tr << 3) | slot; };
     for (int q = 0; q < L->nblock; ++q) {
       const int nh = L->blk[q].x, nb = L->blk[q].y, np = L->blk[q].z, pb = L->pbase[q];
-      ppbase[q] = npp_all;
-      phbase[q] = nph_all;
-      npp_all += np;
-      nph_all += nb;
+      for (int c = 0; c < 3; ++c) gbase[c * L->nblock + q] = cnt[c];
+      cnt[0] += nh;
+      cnt[1] += nb;
+      cnt[2] += np;
       std::map<std::pair<int, int>, int> ihh, iph, ipp;
       for (int k = 0; k < nh; ++k) ihh[{L->pairs[pb + k].x, L->pairs[pb + k].y}] = k;
       for (int k = 0; k < nb; ++k) iph[{L->pairs[pb + nh + k].x, L->pairs[pb + nh + k].y}] = k;
       for (int k = 0; k < np; ++k) ipp[{L->pairs[pb + nh + nb + k].x, L->pairs[pb + nh + nb + k].y}] = k;
-      auto code = [&](int hole, int part, bool neg) { return hole | ((part - n) << 8) | ((neg ? 1 : 0) << 20); };
-      auto members = [&](int x) { return std::make_pair(L->gstart[L->gid[x]], L->gstart[L->gid[x] + 1]); };
-      for (int k = 0; k < np; ++k) {  // pp pair (a, b): +fA(a,t) (t,b), -fA(b,t) (t,a), holes t
-        const int a = L->pairs[pb + nh + nb + k].x, b = L->pairs[pb + nh + nb + k].y;
+      auto grp = [&](int x) { return std::make_pair(L->gstart[L->gid[x]], L->gstart[L->gid[x] + 1]); };
+      // members t of G(x) that are holes (want_hole) or particles, excluding `skip`
+      auto each = [&](int x, bool want_hole, int skip, auto fn) {
+        const auto mr = grp(x);
+        for (int u = mr.first; u < mr.second; ++u) {
+          const int tt = L->gmem[u];
+          if ((tt < n) == want_hole && tt != skip) fn(tt);
+        }
+      };
+      // index and ordering sign of the pair {u, v} in a class map
+      auto srt = [](const std::map<std::pair<int, int>, int>& m, int u, int v, int* idx, int* sg) {
+        auto f = m.find({std::min(u, v), std::max(u, v)});
+        if (f == m.end()) return false;
+        *idx = f->second;
+        *sg = u < v ? 1 : -1;
+        return true;
+      };
+      const auto hhp = [&](int k) { return L->pairs[pb + k]; };
+      const auto php = [&](int k) { return L->pairs[pb + nh + k]; };
+      const auto ppp = [&](int k) { return L->pairs[pb + nh + nb + k]; };
+      int idx, sg;
+      // pp pairs (a, b): W terms +fA(a,t) B_ppph(., (t,b)), -fA(b,t) B_ppph(., (t,a)), holes t
+      for (int k = 0; k < np; ++k) {
+        const int x0 = ppp(k).x, y0 = ppp(k).y;
         for (int side = 0; side < 2; ++side) {
-          const int x = side == 0 ? a : b, y = side == 0 ? b : a;
-          const auto mr = members(x);
-          for (int u = mr.first; u < mr.second; ++u) {
-            const int tt = L->gmem[u];
-            if (tt >= n) continue;
-            auto f = iph.find({tt, y});
-            if (f != iph.end()) ppterm.push_back(int2{f->second, code(tt, x, side == 1)});
-          }
+          const int x = side ? y0 : x0, y = side ? x0 : y0;
+          each(x, true, -1, [&](int t) {
+            auto f = iph.find({t, y});
+            if (f != iph.end()) ppterm.push_back(int2{f->second, (t) | ((x - n) << 8) | ((side ? 1 : 0) << 20)});
+          });
         }
         ppstart.push_back((int)ppterm.size());
       }
-      for (int k = 0; k < nb; ++k) {  // ph pair (h, p)
-        const int hh = L->pairs[pb + nh + k].x, pp = L->pairs[pb + nh + k].y;
-        auto mr = members(hh);
-        for (int u = mr.first; u < mr.second; ++u) {  // particles t in G(h): B_pppp column (t, p)
-          const int tt = L->gmem[u];
-          if (tt < n || tt == pp) continue;
-          auto f = ipp.find({std::min(tt, pp), std::max(tt, pp)});
-          if (f != ipp.end()) phterm.push_back(int4{f->second, code(hh, tt, tt > pp), 0, 0});
+      // row terms, per slot over the pairs of its row class
+      auto rows_of = [&](int slot, int k) {
+        std::vector<int4>& T = rterm_s[slot];
+        if (slot == 4 || slot == 2) {  // rows pp (x, y)
+          const int x0 = ppp(k).x, y0 = ppp(k).y;
+          for (int side = 0; side < 2; ++side) {
+            const int x = side ? y0 : x0, y = side ? x0 : y0;
+            each(x, true, -1, [&](int t) {
+              auto f = iph.find({t, y});
+              if (f != iph.end()) T.push_back(int4{f->second, fA(x, t), side ? NEG : 0, src(1, slot == 4 ? 3 : 5, 0)});
+            });
+            if (slot == 2)  // -s hB fppB(t, x) A_pphh((t,y)) over particles t in G(x)
+              each(x, false, y, [&](int t) {
+                if (srt(ipp, side ? y : t, side ? t : y, &idx, &sg))
+                  T.push_back(int4{idx, fpp(t, x), MB | CB | (sg > 0 ? NEG : 0), src(0, 2, 0)});
+              });
+          }
+        } else if (slot == 5 || slot == 3) {  // rows ph (h, p)
+          const int h = php(k).x, pt = php(k).y;
+          each(h, false, pt, [&](int t) {
+            if (!srt(ipp, t, pt, &idx, &sg)) return;
+            if (slot == 5) {
+              T.push_back(int4{idx, fA(t, h), MA | (sg < 0 ? NEG : 0), src(1, 2, 0)});
+              T.push_back(int4{idx, fA(t, h), MB | CB | (sg > 0 ? NEG : 0), src(0, 2, 0)});
+            } else {
+              T.push_back(int4{idx, fA(t, h), MA | (sg < 0 ? NEG : 0), src(1, 4, 0)});
+            }
+          });
+          each(pt, true, h, [&](int t) {
+            if (!srt(ihh, h, t, &idx, &sg)) return;
+            if (slot == 5)
+              T.push_back(int4{idx, fA(pt, t), sg < 0 ? NEG : 0, src(1, 0, 0)});
+            else
+              T.push_back(int4{idx, fA(pt, t), MB | (sg < 0 ? NEG : 0), src(1, 5, 1)});
+          });
+        } else {  // slot 0, rows hh (b1, b2)
+          const int b1 = hhp(k).x, b2 = hhp(k).y;
+          each(b1, false, -1, [&](int t) {
+            auto f = iph.find({b2, t});
+            if (f != iph.end()) T.push_back(int4{f->second, fA(t, b1), MA | NEG, src(1, 5, 0)});
+          });
+          each(b2, false, -1, [&](int t) {
+            auto f = iph.find({b1, t});
+            if (f != iph.end()) T.push_back(int4{f->second, fA(t, b2), MA, src(1, 5, 0)});
+          });
         }
-        mr = members(pp);
-        for (int u = mr.first; u < mr.second; ++u) {  // holes t in G(p): hh column (h, t)
-          const int tt = L->gmem[u];
-          if (tt >= n || tt == hh) continue;
-          auto f = ihh.find({std::min(hh, tt), std::max(hh, tt)});
-          if (f != ihh.end()) phterm.push_back(int4{f->second, code(tt, pp, hh > tt), 1, 0});
+      };
+      auto cols_of = [&](int slot, int k) {
+        std::vector<int4>& T = cterm_s[slot];
+        if (slot == 4) {  // columns ph (h, p)
+          const int h = php(k).x, pt = php(k).y;
+          each(h, false, pt, [&](int t) {
+            if (srt(ipp, t, pt, &idx, &sg)) T.push_back(int4{idx, fA(t, h), sg > 0 ? NEG : 0, src(1, 1, 0)});
+          });
+          each(pt, true, h, [&](int t) {
+            if (!srt(ihh, h, t, &idx, &sg)) return;
+            T.push_back(int4{idx, fA(pt, t), MA | (sg > 0 ? NEG : 0), src(1, 2, 0)});
+            T.push_back(int4{idx, fA(pt, t), MB | CB | (sg < 0 ? NEG : 0), src(0, 2, 0)});
+          });
+        } else if (slot == 3) {  // columns ph (k1, k2)
+          const int k1 = php(k).x, k2 = php(k).y;
+          each(k1, false, k2, [&](int t) {
+            if (srt(ipp, t, k2, &idx, &sg)) T.push_back(int4{idx, fA(t, k1), MB | (sg > 0 ? NEG : 0), src(1, 4, 1)});
+          });
+          each(k2, true, k1, [&](int t) {
+            if (srt(ihh, k1, t, &idx, &sg)) T.push_back(int4{idx, fA(k2, t), MA | (sg > 0 ? NEG : 0), src(1, 5, 0)});
+          });
+        } else {  // columns hh (k1, k2): slots 2, 5, 0
+          const int k1 = hhp(k).x, k2 = hhp(k).y;
+          for (int side = 0; side < 2; ++side) {
+            const int kk = side ? k2 : k1, ko = side ? k1 : k2;
+            each(kk, false, -1, [&](int t) {
+              auto f = iph.find({ko, t});
+              if (f == iph.end()) return;
+              const int ng = side ? NEG : 0;
+              if (slot == 2) T.push_back(int4{f->second, fA(t, kk), ng, src(1, 4, 0)});
+              else if (slot == 5) T.push_back(int4{f->second, fA(t, kk), ng, src(1, 3, 0)});
+              else T.push_back(int4{f->second, fA(t, kk), MB | ng, src(1, 5, 1)});
+            });
+            if (slot == 2)  // +s hB fhhB(kk, t) A_pphh(., (t,ko)) over holes t in G(kk)
+              each(kk, true, ko, [&](int t) {
+                if (srt(ihh, side ? ko : t, side ? t : ko, &idx, &sg))
+                  T.push_back(int4{idx, fhh(kk, t), MB | CB | (sg < 0 ? NEG : 0), src(0, 2, 0)});
+              });
+          }
         }
-        phstart.push_back((int)phterm.size());
+      };
+      const int rows_n[6] = {nh, 0, np, nb, np, nb}, cols_n[6] = {nh, 0, nh, nb, nb, nh};
+      for (int slot : {0, 2, 3, 4, 5}) {
+        int cr, cc;
+        part_classes(P_HHHH + slot, cr, cc);
+        const int nr = cr == 0 ? nh : (cr == 1 ? nb : np), nc = cc == 0 ? nh : (cc == 1 ? nb : np);
+        for (int k = 0; k < nr; ++k) {
+          rows_of(slot, k);
+          rst[slot].push_back((int)rterm_s[slot].size());  // end of pair k's terms
+        }
+        for (int k = 0; k < nc; ++k) {
+          cols_of(slot, k);
+          cst[slot].push_back((int)cterm_s[slot].size());
+        }
+        if (rows_n[slot] > 0 && cols_n[slot] > 0)
+          for (int i = 0; i < (rows_n[slot] + SP_B - 1) / SP_B; ++i)
+            for (int j = 0; j < (cols_n[slot] + SP_B - 1) / SP_B; ++j) gtask.push_back(int4{q, slot, i, j});
       }
-      const int tr = (np + SP_B - 1) / SP_B, tc = (nb + SP_B - 1) / SP_B;
+      const int tr = (np + SP_B - 1) / SP_B;
       for (int i = 0; i < tr; ++i)
-        for (int j = i; j < tr; ++j) sptask[0].push_back(int4{q, i, j, 0});
-      for (int i = 0; i < tr; ++i)
-        for (int j = 0; j < tc; ++j) sptask[1].push_back(int4{q, i, j, 1});
+        for (int j = i; j < tr; ++j) ptask.push_back(int4{q, i, j, 0});
     }
-    p.nsp_pppp = (int)sptask[0].size();
-    p.nsp_ppph = (int)sptask[1].size();
-    std::vector<int4> all = sptask[0];
-    all.insert(all.end(), sptask[1].begin(), sptask[1].end());
+    // per slot start arrays: one entry per pair of its class (in block order) plus one
+    // concatenated: per slot a start 0 then the pairs' ends, shifted by the
+    // slot's first term in the joint term arrays
+    std::vector<int> rall, call;
+    std::vector<int4> rterm, cterm;
+    for (int slot = 0; slot < 6; ++slot) {
+      p.gen_rso[slot] = (int)rall.size();
+      p.gen_cso[slot] = (int)call.size();
+      const int r0 = (int)rterm.size(), c0 = (int)cterm.size();
+      rall.push_back(r0);
+      for (int e : rst[slot]) rall.push_back(r0 + e);
+      call.push_back(c0);
+      for (int e : cst[slot]) call.push_back(c0 + e);
+      rterm.insert(rterm.end(), rterm_s[slot].begin(), rterm_s[slot].end());
+      cterm.insert(cterm.end(), cterm_s[slot].begin(), cterm_s[slot].end());
+    }
+    p.nsp_pppp = (int)ptask.size();
+    p.nsp_gen = (int)gtask.size();
+    std::vector<int4> all = ptask;
+    all.insert(all.end(), gtask.begin(), gtask.end());
+    std::vector<int> ppbase(L->nblock);
+    for (int q = 0; q < L->nblock; ++q) ppbase[q] = gbase[2 * L->nblock + q];
     if ((rc = upload_vec(L, ppbase, &p.d_ppbase)) || (rc = upload_vec(L, ppstart, &p.d_ppstart)) ||
-        (rc = upload_vec(L, ppterm, &p.d_ppterm)) || (rc = upload_vec(L, phbase, &p.d_phbase)) ||
-        (rc = upload_vec(L, phstart, &p.d_phstart)) || (rc = upload_vec(L, phterm, &p.d_phterm)) ||
+        (rc = upload_vec(L, ppterm, &p.d_ppterm)) || (rc = upload_vec(L, gbase, &p.d_gbase)) ||
+        (rc = upload_vec(L, rall, &p.d_rstart)) || (rc = upload_vec(L, call, &p.d_cstart)) ||
+        (rc = upload_vec(L, rterm, &p.d_rterm)) || (rc = upload_vec(L, cterm, &p.d_cterm)) ||
         (rc = upload_vec(L, all, &p.d_sptask)))
       return rc;
   }
@@ -1201,10 +1356,10 @@ static int task_set(qd_layout* L, Plan122* p, unsigned zA, unsigned zB, TaskSet*
   const unsigned za2 = (zA >> P_HHHH) & 63u, zb2 = (zB >> P_HHHH) & 63u;
   // lists: 0 one operand (set), 1 both operands (set), 2 one operand (accumulate)
   std::vector<std::pair<size_t, int2>> lst[3];
-  const unsigned outmask = gen_like(zA) ? OUT_NO_PP : OUT_ALL;
+  const unsigned outmask = gen_like(zA) ? OUT_NONE : OUT_ALL;
   for (size_t i = 0; i < p->tiles.size(); ++i) {
     const TileInfo& t = p->tiles[i];
-    if (!(t.outs & outmask)) continue;  // every output of the tile comes from k_122_pppp / k_122_ppph
+    if (!(t.outs & outmask)) continue;  // every output of the tile comes from k_122_pppp / k_122_gen
     const bool nb = !fa0 && (t.parts & ~zb2) && !(spa && t.holefree);
     const bool na = !fb0 && (t.parts & ~za2) && !(spb && t.holefree);
     const int op = (nb ? 1 : 0) | (na ? 2 : 0);
@@ -1238,8 +1393,8 @@ void drop_122_plan(const qd_layout* L) {
   Plan122& p = it->second;
   for (void* ptr : {(void*)p.d_gpd, (void*)p.d_gpp, (void*)p.d_tiles, (void*)p.d_sbase,
                     (void*)p.d_ftab, (void*)p.d_gpg, (void*)p.d_zrow, (void*)p.d_ptask, (void*)p.d_ppbase,
-                    (void*)p.d_ppstart, (void*)p.d_ppterm, (void*)p.d_phbase, (void*)p.d_phstart,
-                    (void*)p.d_phterm, (void*)p.d_sptask})
+                    (void*)p.d_ppstart, (void*)p.d_ppterm, (void*)p.d_gbase, (void*)p.d_rstart,
+                    (void*)p.d_cstart, (void*)p.d_rterm, (void*)p.d_cterm, (void*)p.d_sptask})
     if (ptr) cudaFree(ptr);
   for (auto& kv : p.sets) {
     if (kv.second.d_task) cudaFree(kv.second.d_task);
@@ -1436,8 +1591,8 @@ int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B) {
   return QD_OK;
 }
 
-// C_pppp and C_ppph of every block for a generator-like A (k_122_pppp,
-// k_122_ppph) on stream st.
+// Every two-body part of C for a generator-like A (k_122_pppp, k_122_gen)
+// on stream st.
 static int launch_122_gen(qd_layout* L, const Plan122* p, const qd_op* A, const qd_op* B, double* C,
                           cudaStream_t st) {
   if (p->nsp_pppp > 0) {
@@ -1446,10 +1601,19 @@ static int launch_122_gen(qd_layout* L, const Plan122* p, const qd_op* A, const 
         B->zero_mask, C);
     ++L->nlaunch;
   }
-  if (p->nsp_ppph > 0) {
-    k_122_ppph<<<p->nsp_ppph, SP_T, 0, st>>>(L->dev, p->d_sptask + p->nsp_pppp, p->d_ppbase, p->d_ppstart,
-                                             p->d_ppterm, p->d_phbase, p->d_phstart, p->d_phterm, A->d,
-                                             (double)A->herm, A->zero_mask, B->d, (double)B->herm, B->zero_mask, C);
+  if (p->nsp_gen > 0) {
+    GenTables G;
+    G.gbase = p->d_gbase;
+    G.rstart = p->d_rstart;
+    G.cstart = p->d_cstart;
+    G.rterm = p->d_rterm;
+    G.cterm = p->d_cterm;
+    for (int k = 0; k < 6; ++k) {
+      G.rso[k] = p->gen_rso[k];
+      G.cso[k] = p->gen_cso[k];
+    }
+    k_122_gen<<<p->nsp_gen, SP_T, 0, st>>>(L->dev, p->d_sptask + p->nsp_pppp, G, A->d, (double)A->herm,
+                                           A->zero_mask, B->d, (double)B->herm, B->zero_mask, C);
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());
