@@ -448,13 +448,25 @@ __device__ __forceinline__ double sp_coef(const DevLayout& L, const double* __re
   return (code >> 20) & 1 ? -v : v;
 }
 
+// A term staged in shared memory: its coefficient, and the source element
+// off + fixed * (m & MULT_MASK) of operand B (bit 30 of m set) or A.
+struct StagedTerm {
+  double c;
+  int off, m;
+};
+constexpr int MULT_MASK = 0x3FFFFFFF;
+
 // One task = the tile pair (I, J), (J, I) of a block's C_pppp (64 x 64 each).
+// The W terms of the tile's columns (J, then I) are staged in shared memory
+// first, with their coefficients resolved; each W element then reads only
+// its B_ppph entries.
 __global__ void __launch_bounds__(SP_T) k_122_pppp(DevLayout L, const int4* __restrict__ tasks,
                                                   const int* __restrict__ ppbase, const int* __restrict__ ppstart,
                                                   const int2* __restrict__ ppterm, const double* __restrict__ A,
                                                   double hA, const double* __restrict__ B, double hB, unsigned zB,
                                                   double* __restrict__ C) {
-  extern __shared__ double spw[];  // W1[c][r] = W(I0 + r, J0 + c), W2[c][r] = W(J0 + r, I0 + c)
+  extern __shared__ __align__(16) double spw[];  // W1[c][r] = W(I0 + r, J0 + c), W2[c][r] = W(J0 + r, I0 + c), terms
+  __shared__ int sst[2][SP_B + 1];               // per pass: each column's first staged term
   const int4 t = tasks[blockIdx.x];
   const int q = t.x, I0 = t.y * SP_B, J0 = t.z * SP_B;
   const int4 bd = __ldg(&L.blk[q]);
@@ -465,20 +477,29 @@ __global__ void __launch_bounds__(SP_T) k_122_pppp(DevLayout L, const int4* __re
   const int pb = __ldg(&ppbase[q]);
   const int tid = threadIdx.x, r = tid & (SP_B - 1), cg = tid >> 6;
   const bool diag = t.y == t.z;
-  for (int pass = 0; pass < (diag ? 1 : 2); ++pass) {
-    const int R0 = pass == 0 ? I0 : J0, C0 = pass == 0 ? J0 : I0;
+  const int npass = diag ? 1 : 2;
+  StagedTerm* T = reinterpret_cast<StagedTerm*>(spw + 2 * SP_B * SP_LD);
+  int base = 0;
+  for (int pass = 0; pass < npass; ++pass) {
+    const int C0 = pass == 0 ? J0 : I0, nc = live ? min(SP_B, np - C0) : 0;
+    const int e0 = __ldg(&ppstart[pb + C0]);
+    for (int i = tid; i <= SP_B; i += SP_T) sst[pass][i] = base + (i <= nc ? __ldg(&ppstart[pb + C0 + i]) : __ldg(&ppstart[pb + C0 + nc])) - e0;
+    const int ne = nc > 0 ? __ldg(&ppstart[pb + C0 + nc]) - e0 : 0;
+    for (int i = tid; i < ne; i += SP_T) {
+      const int2 tm = __ldg(&ppterm[e0 + i]);
+      T[base + i] = StagedTerm{sp_coef(L, A, tm.y), tm.x * np, 0};
+    }
+    base += ne;
+  }
+  __syncthreads();
+  for (int pass = 0; pass < npass; ++pass) {
+    const int R0 = pass == 0 ? I0 : J0;
     double* W = spw + pass * SP_B * SP_LD;
     const int row = R0 + r;
     for (int cc = cg; cc < SP_B; cc += SP_T / SP_B) {
-      const int col = C0 + cc;
       double w = 0.0;
-      if (live && row < np && col < np) {
-        const int e1 = __ldg(&ppstart[pb + col + 1]);
-        for (int e = __ldg(&ppstart[pb + col]); e < e1; ++e) {
-          const int2 tm = __ldg(&ppterm[e]);
-          w += sp_coef(L, A, tm.y) * X[row + (i64)tm.x * np];
-        }
-      }
+      if (row < np)
+        for (int e = sst[pass][cc]; e < sst[pass][cc + 1]; ++e) w += T[e].c * X[row + (i64)T[e].off];
       W[cc * SP_LD + r] = w;
     }
   }
@@ -527,48 +548,76 @@ struct GenTables {
   int rso[6], cso[6];  // offset of each part's start array (slot order)
 };
 
-__device__ __forceinline__ double gen_term(const DevLayout& L, const int4& tm, const double* __restrict__ A,
-                                           double hA, unsigned zA, const double* __restrict__ B, double hB,
-                                           unsigned zB, int q, int4 bd, int fixed, bool row_term) {
+// Resolve a term for one tile: its coefficient and its source element as
+// off + fixed * m (row term: fixed = output column; column term: output row).
+__device__ __forceinline__ StagedTerm stage_term(const DevLayout& L, const int4& tm, int q, int4 bd, bool row_term,
+                                                 const double* __restrict__ A, double hA,
+                                                 const double* __restrict__ B, double hB) {
   const int opd = tm.w >> 4, slot = tm.w & 7;
   const bool tr = (tm.w >> 3) & 1;
-  if ((((opd ? zB : zA) >> (P_HHHH + slot)) & 1u)) return 0.0;
-  const double* M = (opd ? B : A) + __ldg(L.boff + 6 * q + slot);
-  const i64 ld = part_rows(P_HHHH + slot, bd);
+  const int ld = part_rows(P_HHHH + slot, bd);
+  const int bo = (int)__ldg(L.boff + 6 * q + slot);
+  StagedTerm st;
+  if (row_term != tr) {
+    st.off = bo + tm.x;
+    st.m = ld;
+  } else {
+    st.off = bo + tm.x * ld;
+    st.m = 1;
+  }
+  st.m |= opd << 30;
   double c = __ldg(&((tm.z >> 3) & 1 ? B : A)[tm.y]);
   if (tm.z & 2) c *= hA;
   if (tm.z & 4) c *= hB;
   if (tm.z & 1) c = -c;
-  // row term: fixed = output column; column term: fixed = output row
-  const i64 e = (row_term != tr) ? tm.x + (i64)fixed * ld : fixed + (i64)tm.x * ld;
-  return c * M[e];
+  st.c = c;
+  return st;
 }
 
+// The tile's column terms, then its row terms, are staged once per CTA in
+// shared memory (dynamic size: the most terms of any tile of the launch).
 __global__ void __launch_bounds__(SP_T) k_122_gen(DevLayout L, const int4* __restrict__ tasks, GenTables G,
-                                                 const double* __restrict__ A, double hA, unsigned zA,
-                                                 const double* __restrict__ B, double hB, unsigned zB,
+                                                 const double* __restrict__ A, double hA,
+                                                 const double* __restrict__ B, double hB,
                                                  double* __restrict__ C) {
+  extern __shared__ __align__(16) double sgt[];
+  StagedTerm* T = reinterpret_cast<StagedTerm*>(sgt);
+  __shared__ int scs[SP_B + 1], srs[SP_B + 1];
   const int4 t = tasks[blockIdx.x];
   const int q = t.x, slot = t.y, I0 = t.z * SP_B, J0 = t.w * SP_B;
   const int4 bd = __ldg(&L.blk[q]);
   int cr, cc;
   part_classes(P_HHHH + slot, cr, cc);
   const int nrow = part_rows(P_HHHH + slot, bd), ncol = cc == 0 ? bd.x : (cc == 1 ? bd.y : bd.z);
-  const int tid = threadIdx.x, r = tid & (SP_B - 1), cg = tid >> 6;
+  const int nrt = min(SP_B, nrow - I0), nct = min(SP_B, ncol - J0);
+  const int* rs = G.rstart + G.rso[slot] + __ldg(&G.gbase[cr * L.nblock + q]) + I0;
+  const int* cs = G.cstart + G.cso[slot] + __ldg(&G.gbase[cc * L.nblock + q]) + J0;
+  const int c0 = __ldg(&cs[0]), nce = __ldg(&cs[nct]) - c0;
+  const int r0 = __ldg(&rs[0]), nre = __ldg(&rs[nrt]) - r0;
+  const int tid = threadIdx.x;
+  for (int i = tid; i <= SP_B; i += SP_T) {
+    scs[i] = __ldg(&cs[min(i, nct)]) - c0;
+    srs[i] = nce + __ldg(&rs[min(i, nrt)]) - r0;
+  }
+  for (int i = tid; i < nce; i += SP_T) T[i] = stage_term(L, __ldg(&G.cterm[c0 + i]), q, bd, false, A, hA, B, hB);
+  for (int i = tid; i < nre; i += SP_T) T[nce + i] = stage_term(L, __ldg(&G.rterm[r0 + i]), q, bd, true, A, hA, B, hB);
+  __syncthreads();
+  const int r = tid & (SP_B - 1), cg = tid >> 6;
+  if (r >= nrt) return;  // after the only barrier
   const int row = I0 + r;
-  if (row >= nrow) return;  // no barrier below
-  const int* rs = G.rstart + G.rso[slot] + __ldg(&G.gbase[cr * L.nblock + q]);
-  const int* cs = G.cstart + G.cso[slot] + __ldg(&G.gbase[cc * L.nblock + q]);
-  const int er0 = __ldg(&rs[row]), er1 = __ldg(&rs[row + 1]);
+  const int er0 = srs[r], er1 = srs[r + 1];
   double* out = C + __ldg(L.boff + 6 * q + slot);
-  for (int k = cg; k < SP_B; k += SP_T / SP_B) {
+  for (int k = cg; k < nct; k += SP_T / SP_B) {
     const int col = J0 + k;
-    if (col >= ncol) break;
     double y = 0.0;
-    const int e1 = __ldg(&cs[col + 1]);
-    for (int e = __ldg(&cs[col]); e < e1; ++e)
-      y += gen_term(L, __ldg(&G.cterm[e]), A, hA, zA, B, hB, zB, q, bd, row, false);
-    for (int e = er0; e < er1; ++e) y += gen_term(L, __ldg(&G.rterm[e]), A, hA, zA, B, hB, zB, q, bd, col, true);
+    for (int e = scs[k]; e < scs[k + 1]; ++e) {
+      const StagedTerm s = T[e];
+      y += s.c * ((s.m >> 30) ? B : A)[s.off + (i64)row * (s.m & MULT_MASK)];
+    }
+    for (int e = er0; e < er1; ++e) {
+      const StagedTerm s = T[e];
+      y += s.c * ((s.m >> 30) ? B : A)[s.off + (i64)col * (s.m & MULT_MASK)];
+    }
     out[row + (i64)col * nrow] = y;
   }
 }
@@ -847,6 +896,7 @@ struct Plan122 {
   int gen_rso[6] = {0}, gen_cso[6] = {0};
   int4* d_sptask = nullptr;  // C_pppp tile pairs, then the k_122_gen tiles
   int nsp_pppp = 0, nsp_gen = 0;
+  int pppp_terms = 0, gen_terms = 0;  // the most terms one task of each kernel stages
 };
 std::map<const qd_layout*, Plan122>& plans() {
   static std::map<const qd_layout*, Plan122> m;
@@ -1200,6 +1250,34 @@ static int plan_122(qd_layout* L, Plan122** out) {
     }
     p.nsp_pppp = (int)ptask.size();
     p.nsp_gen = (int)gtask.size();
+    // the most terms one task stages (its shared memory)
+    p.pppp_terms = 0;
+    for (const int4& tk : ptask) {
+      const int q = tk.x, np = L->blk[q].z, pbq = gbase[2 * L->nblock + q];
+      int ne = 0;
+      for (int pass = 0; pass < (tk.y == tk.z ? 1 : 2); ++pass) {
+        const int c0 = (pass == 0 ? tk.z : tk.y) * SP_B, nc = std::min(SP_B, np - c0);
+        ne += ppstart[pbq + c0 + nc] - ppstart[pbq + c0];
+      }
+      p.pppp_terms = std::max(p.pppp_terms, ne);
+    }
+    p.gen_terms = 0;
+    for (const int4& tk : gtask) {
+      const int q = tk.x, slot = tk.y;
+      int cr, cc;
+      part_classes(P_HHHH + slot, cr, cc);
+      const int4 bd = L->blk[q];
+      const int nr = cr == 0 ? bd.x : (cr == 1 ? bd.y : bd.z), nc = cc == 0 ? bd.x : (cc == 1 ? bd.y : bd.z);
+      const int i0 = tk.z * SP_B, j0 = tk.w * SP_B, nrt = std::min(SP_B, nr - i0), nct = std::min(SP_B, nc - j0);
+      const int* rr = rall.data() + p.gen_rso[slot] + gbase[cr * L->nblock + q] + i0;
+      const int* cs = call.data() + p.gen_cso[slot] + gbase[cc * L->nblock + q] + j0;
+      p.gen_terms = std::max(p.gen_terms, (rr[nrt] - rr[0]) + (cs[nct] - cs[0]));
+    }
+    if (2 * SP_B * SP_LD * sizeof(double) + (size_t)p.pppp_terms * sizeof(StagedTerm) > SMEM_MAX_122 - 1024 ||
+        (size_t)p.gen_terms * sizeof(StagedTerm) > SMEM_MAX_122 - 1024) {
+      set_error("commutator_122: %d / %d terms of one tile exceed shared memory", p.pppp_terms, p.gen_terms);
+      return QD_ERR_ARG;
+    }
     std::vector<int4> all = ptask;
     all.insert(all.end(), gtask.begin(), gtask.end());
     std::vector<int> ppbase(L->nblock);
@@ -1272,7 +1350,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
                          (const void*)k_122_tile<1, 256, true>, (const void*)k_122_tile<2, 256, true>,
                          (const void*)k_pandya_tile<PD_ALL4>, (const void*)k_pandya_tile<PD_PAIRS>,
                          (const void*)k_pandya_tile<PD_SINGLE>, (const void*)k_pandya_tile<PD_DIRECT>,
-                         (const void*)k_122_pppp}) {
+                         (const void*)k_122_pppp, (const void*)k_122_gen}) {
     cudaFuncAttributes fa;
     QD_CUDA(cudaFuncGetAttributes(&fa, fn));
     QD_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1580,7 +1658,7 @@ int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B) {
   if (rc) return rc;
   TaskSet* ts;
   if ((rc = task_set(L, p, A->zero_mask, B->zero_mask, &ts))) return rc;
-  if (!ts->tuned && !L->prof.on && !capturing(L->stream)) {
+  if (!ts->tuned && !ts->buckets.empty() && !L->prof.on && !capturing(L->stream)) {
     // the F tables of these operands first: the timed launches read them
     const int nf = L->m * p->gmax;
     k_ftab<<<(nf + 127) / 128, 128, 0, L->stream>>>(L->dev, p->d_sbase, A->d, (double)A->herm, B->d,
@@ -1596,7 +1674,7 @@ int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B) {
 static int launch_122_gen(qd_layout* L, const Plan122* p, const qd_op* A, const qd_op* B, double* C,
                           cudaStream_t st) {
   if (p->nsp_pppp > 0) {
-    k_122_pppp<<<p->nsp_pppp, SP_T, 2 * SP_B * SP_LD * sizeof(double), st>>>(
+    k_122_pppp<<<p->nsp_pppp, SP_T, 2 * SP_B * SP_LD * sizeof(double) + p->pppp_terms * sizeof(StagedTerm), st>>>(
         L->dev, p->d_sptask, p->d_ppbase, p->d_ppstart, p->d_ppterm, A->d, (double)A->herm, B->d, (double)B->herm,
         B->zero_mask, C);
     ++L->nlaunch;
@@ -1612,8 +1690,8 @@ static int launch_122_gen(qd_layout* L, const Plan122* p, const qd_op* A, const 
       G.rso[k] = p->gen_rso[k];
       G.cso[k] = p->gen_cso[k];
     }
-    k_122_gen<<<p->nsp_gen, SP_T, 0, st>>>(L->dev, p->d_sptask + p->nsp_pppp, G, A->d, (double)A->herm,
-                                           A->zero_mask, B->d, (double)B->herm, B->zero_mask, C);
+    k_122_gen<<<p->nsp_gen, SP_T, p->gen_terms * sizeof(StagedTerm), st>>>(
+        L->dev, p->d_sptask + p->nsp_pppp, G, A->d, (double)A->herm, B->d, (double)B->herm, C);
     ++L->nlaunch;
   }
   QD_CUDA(cudaGetLastError());
@@ -1628,12 +1706,13 @@ int launch_122(qd_layout* L, const qd_op* A, const qd_op* B, double* C) {
   TaskSet* ts;
   if ((rc = task_set(L, p, A->zero_mask, B->zero_mask, &ts))) return rc;
   const int spA = spars(A), spB = spars(B);
+  if (ts->outmask != OUT_ALL) TRY(launch_122_gen(L, p, A, B, C, L->stream));
+  if (ts->buckets.empty()) return QD_OK;  // no group-pair tiles: their F tables are not needed
   const int nf = L->m * p->gmax;
   k_ftab<<<(nf + 127) / 128, 128, 0, L->stream>>>(L->dev, p->d_sbase, A->d, (double)A->herm, B->d,
                                                   (double)B->herm, p->d_ftab, p->gmax, p->nfent);
   ++L->nlaunch;
   if (!ts->tuned && !L->prof.on && !capturing(L->stream)) TRY(tune_122(L, p, ts, A, B, spA, spB));
-  if (ts->outmask != OUT_ALL) TRY(launch_122_gen(L, p, A, B, C, L->stream));
   for (const Bucket122& b : ts->buckets) TRY(launch_bucket(L, p, ts, b, b.threads, A, B, spA, spB, C));
   QD_CUDA(cudaGetLastError());
   return QD_OK;
@@ -1776,10 +1855,12 @@ int launch_122_batched(cudaStream_t st, const std::vector<Item122>& items) {
   for (size_t i = 0; i < n; ++i) {
     const Item122& it = items[i];
     const Plan122* p = pl[i];
-    const int nf = it.L->m * p->gmax;
-    k_ftab<<<(nf + 127) / 128, 128, 0, st>>>(it.L->dev, p->d_sbase, it.A->d, (double)it.A->herm, it.B->d,
-                                             (double)it.B->herm, p->d_ftab, p->gmax, p->nfent);
-    ++it.L->nlaunch;
+    if (!tsv[i]->buckets.empty()) {  // F tables for the group-pair tiles
+      const int nf = it.L->m * p->gmax;
+      k_ftab<<<(nf + 127) / 128, 128, 0, st>>>(it.L->dev, p->d_sbase, it.A->d, (double)it.A->herm, it.B->d,
+                                               (double)it.B->herm, p->d_ftab, p->gmax, p->nfent);
+      ++it.L->nlaunch;
+    }
     Inst122& I = m->h_inst[i];
     I.L = it.L->dev;
     I.tiles = p->d_tiles;
