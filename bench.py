@@ -244,12 +244,11 @@ def stage_roofline(prof: dict, flops: dict, neq2b: int, dgemm_peak: float, hbm_p
 NCU_NEQ = 19841598
 NCU_TRAFFIC = {"ladder_gemm": 794.761728e6 + 162.643712e6, "pandya_gemm": 200.469760e6 + 676.389888e6,
                "pandya_gather": 2126.409e6 + 154.573824e6}
-# commutator_122 of one flow commutator [Omega, X] (the two k_122_tile
-# launches: tiles needing X only, tiles needing Omega and X), from the N=20,
-# R=18 capture (29,618,726 entries per operator): scaled to the flow's basis
-# by entries per operator
+# commutator_122 of one flow commutator [Omega, X] (the k_122_pppp and
+# k_122_gen launches), from the N=20, R=18 capture (29,618,726 entries per
+# operator): scaled to the flow's basis by entries per operator
 NCU_FLOW_NEQ = 29618726
-NCU_FLOW_TRAFFIC = {"c122": 296.7e6 + 178.7e6}
+NCU_FLOW_TRAFFIC = {"c122": (29.3e6 + 139.6e6) + (179.3e6 + 51.9e6)}
 
 
 def _peaks_present() -> bool:
@@ -574,7 +573,7 @@ def run_flow(args, world, rank, local):
             "note": "stage with the most device time, per launch = per commutator; bytes = read A, B and "
                     "write C two-body parts once",
             "traffic": NCU_FLOW_TRAFFIC[name] * P.neq / NCU_FLOW_NEQ if name in NCU_FLOW_TRAFFIC else None,
-            "traffic_source": "ncu dram bytes of the k_122_tile launches of one commutator at N=20 R=18, "
+            "traffic_source": "ncu dram bytes of the k_122_pppp and k_122_gen launches of one commutator at N=20 R=18, "
                               "scaled by entries per operator" if name in NCU_FLOW_TRAFFIC else None}
     roof["frac"] = roof["achieved"] / roof["peak"]
     cpu = None
