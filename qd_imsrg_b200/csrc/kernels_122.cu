@@ -442,6 +442,8 @@ __host__ __device__ __forceinline__ bool gen_like(unsigned zmask) {
 }
 
 constexpr int SP_T = 256, SP_B = 64, SP_LD = SP_B + 1;
+// k_122_pppp tiles: 32 x 32 (two W tiles of 8.4 KB per CTA: seven CTAs per SM)
+constexpr int PP_B = 32, PP_LD = PP_B + 1;
 
 __device__ __forceinline__ double sp_coef(const DevLayout& L, const double* __restrict__ f, int code) {
   const double v = __ldg(&f[L.o_fph + ((code >> 8) & 0xFFF) + (i64)(code & 0xFF) * L.mp]);
@@ -456,7 +458,7 @@ struct StagedTerm {
 };
 constexpr int MULT_MASK = 0x3FFFFFFF;
 
-// One task = the tile pair (I, J), (J, I) of a block's C_pppp (64 x 64 each).
+// One task = the tile pair (I, J), (J, I) of a block's C_pppp (32 x 32 each).
 // The W terms of the tile's columns (J, then I) are staged in shared memory
 // first, with their coefficients resolved; each W element then reads only
 // its B_ppph entries.
@@ -466,24 +468,24 @@ __global__ void __launch_bounds__(SP_T) k_122_pppp(DevLayout L, const int4* __re
                                                   double hA, const double* __restrict__ B, double hB, unsigned zB,
                                                   double* __restrict__ C) {
   extern __shared__ __align__(16) double spw[];  // W1[c][r] = W(I0 + r, J0 + c), W2[c][r] = W(J0 + r, I0 + c), terms
-  __shared__ int sst[2][SP_B + 1];               // per pass: each column's first staged term
+  __shared__ int sst[2][PP_B + 1];               // per pass: each column's first staged term
   const int4 t = tasks[blockIdx.x];
-  const int q = t.x, I0 = t.y * SP_B, J0 = t.z * SP_B;
+  const int q = t.x, I0 = t.y * PP_B, J0 = t.z * PP_B;
   const int4 bd = __ldg(&L.blk[q]);
   const int np = bd.z;
   const i64* boff = L.boff + 6 * q;
   const bool live = !((zB >> P_PPPH) & 1u);
   const double* X = B + __ldg(boff + 4);  // B_ppph, np x nph
   const int pb = __ldg(&ppbase[q]);
-  const int tid = threadIdx.x, r = tid & (SP_B - 1), cg = tid >> 6;
+  const int tid = threadIdx.x, r = tid & (PP_B - 1), cg = tid >> 5;
   const bool diag = t.y == t.z;
   const int npass = diag ? 1 : 2;
-  StagedTerm* T = reinterpret_cast<StagedTerm*>(spw + 2 * SP_B * SP_LD);
+  StagedTerm* T = reinterpret_cast<StagedTerm*>(spw + 2 * PP_B * PP_LD);
   int base = 0;
   for (int pass = 0; pass < npass; ++pass) {
-    const int C0 = pass == 0 ? J0 : I0, nc = live ? min(SP_B, np - C0) : 0;
+    const int C0 = pass == 0 ? J0 : I0, nc = live ? min(PP_B, np - C0) : 0;
     const int e0 = __ldg(&ppstart[pb + C0]);
-    for (int i = tid; i <= SP_B; i += SP_T) sst[pass][i] = base + (i <= nc ? __ldg(&ppstart[pb + C0 + i]) : __ldg(&ppstart[pb + C0 + nc])) - e0;
+    for (int i = tid; i <= PP_B; i += SP_T) sst[pass][i] = base + (i <= nc ? __ldg(&ppstart[pb + C0 + i]) : __ldg(&ppstart[pb + C0 + nc])) - e0;
     const int ne = nc > 0 ? __ldg(&ppstart[pb + C0 + nc]) - e0 : 0;
     for (int i = tid; i < ne; i += SP_T) {
       const int2 tm = __ldg(&ppterm[e0 + i]);
@@ -494,29 +496,29 @@ __global__ void __launch_bounds__(SP_T) k_122_pppp(DevLayout L, const int4* __re
   __syncthreads();
   for (int pass = 0; pass < npass; ++pass) {
     const int R0 = pass == 0 ? I0 : J0;
-    double* W = spw + pass * SP_B * SP_LD;
+    double* W = spw + pass * PP_B * PP_LD;
     const int row = R0 + r;
-    for (int cc = cg; cc < SP_B; cc += SP_T / SP_B) {
+    for (int cc = cg; cc < PP_B; cc += SP_T / PP_B) {
       double w = 0.0;
       if (row < np)
         for (int e = sst[pass][cc]; e < sst[pass][cc + 1]; ++e) w += T[e].c * X[row + (i64)T[e].off];
-      W[cc * SP_LD + r] = w;
+      W[cc * PP_LD + r] = w;
     }
   }
   __syncthreads();
   const double* W1 = spw;
-  const double* W2 = diag ? spw : spw + SP_B * SP_LD;
+  const double* W2 = diag ? spw : spw + PP_B * PP_LD;
   double* out = C + __ldg(boff + 1);
-  for (int idx = tid; idx < SP_B * SP_B; idx += SP_T) {
-    const int rr = idx & (SP_B - 1), c = idx >> 6;
+  for (int idx = tid; idx < PP_B * PP_B; idx += SP_T) {
+    const int rr = idx & (PP_B - 1), c = idx >> 5;
     if (I0 + rr < np && J0 + c < np)  // C(I0 + rr, J0 + c) = hB W(J0 + c, I0 + rr) - hA W(I0 + rr, J0 + c)
-      out[(I0 + rr) + (i64)(J0 + c) * np] = hB * W2[rr * SP_LD + c] - hA * W1[c * SP_LD + rr];
+      out[(I0 + rr) + (i64)(J0 + c) * np] = hB * W2[rr * PP_LD + c] - hA * W1[c * PP_LD + rr];
   }
   if (diag) return;
-  for (int idx = tid; idx < SP_B * SP_B; idx += SP_T) {
-    const int rr = idx & (SP_B - 1), c = idx >> 6;
+  for (int idx = tid; idx < PP_B * PP_B; idx += SP_T) {
+    const int rr = idx & (PP_B - 1), c = idx >> 5;
     if (J0 + rr < np && I0 + c < np)  // C(J0 + rr, I0 + c) = hB W(I0 + c, J0 + rr) - hA W(J0 + rr, I0 + c)
-      out[(J0 + rr) + (i64)(I0 + c) * np] = hB * W1[rr * SP_LD + c] - hA * W2[c * SP_LD + rr];
+      out[(J0 + rr) + (i64)(I0 + c) * np] = hB * W1[rr * PP_LD + c] - hA * W2[c * PP_LD + rr];
   }
 }
 
@@ -1228,7 +1230,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
           for (int i = 0; i < (rows_n[slot] + SP_B - 1) / SP_B; ++i)
             for (int j = 0; j < (cols_n[slot] + SP_B - 1) / SP_B; ++j) gtask.push_back(int4{q, slot, i, j});
       }
-      const int tr = (np + SP_B - 1) / SP_B;
+      const int tr = (np + PP_B - 1) / PP_B;
       for (int i = 0; i < tr; ++i)
         for (int j = i; j < tr; ++j) ptask.push_back(int4{q, i, j, 0});
     }
@@ -1256,7 +1258,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
       const int q = tk.x, np = L->blk[q].z, pbq = gbase[2 * L->nblock + q];
       int ne = 0;
       for (int pass = 0; pass < (tk.y == tk.z ? 1 : 2); ++pass) {
-        const int c0 = (pass == 0 ? tk.z : tk.y) * SP_B, nc = std::min(SP_B, np - c0);
+        const int c0 = (pass == 0 ? tk.z : tk.y) * PP_B, nc = std::min(PP_B, np - c0);
         ne += ppstart[pbq + c0 + nc] - ppstart[pbq + c0];
       }
       p.pppp_terms = std::max(p.pppp_terms, ne);
@@ -1273,7 +1275,7 @@ static int plan_122(qd_layout* L, Plan122** out) {
       const int* cs = call.data() + p.gen_cso[slot] + gbase[cc * L->nblock + q] + j0;
       p.gen_terms = std::max(p.gen_terms, (rr[nrt] - rr[0]) + (cs[nct] - cs[0]));
     }
-    if (2 * SP_B * SP_LD * sizeof(double) + (size_t)p.pppp_terms * sizeof(StagedTerm) > SMEM_MAX_122 - 1024 ||
+    if (2 * PP_B * PP_LD * sizeof(double) + (size_t)p.pppp_terms * sizeof(StagedTerm) > SMEM_MAX_122 - 1024 ||
         (size_t)p.gen_terms * sizeof(StagedTerm) > SMEM_MAX_122 - 1024) {
       set_error("commutator_122: %d / %d terms of one tile exceed shared memory", p.pppp_terms, p.gen_terms);
       return QD_ERR_ARG;
@@ -1674,7 +1676,7 @@ int prepare_122(qd_layout* L, const qd_op* A, const qd_op* B) {
 static int launch_122_gen(qd_layout* L, const Plan122* p, const qd_op* A, const qd_op* B, double* C,
                           cudaStream_t st) {
   if (p->nsp_pppp > 0) {
-    k_122_pppp<<<p->nsp_pppp, SP_T, 2 * SP_B * SP_LD * sizeof(double) + p->pppp_terms * sizeof(StagedTerm), st>>>(
+    k_122_pppp<<<p->nsp_pppp, SP_T, 2 * PP_B * PP_LD * sizeof(double) + p->pppp_terms * sizeof(StagedTerm), st>>>(
         L->dev, p->d_sptask, p->d_ppbase, p->d_ppstart, p->d_ppterm, A->d, (double)A->herm, B->d, (double)B->herm,
         B->zero_mask, C);
     ++L->nlaunch;
